@@ -1,0 +1,160 @@
+"""ctypes bindings of libbt_gpu.so (include/bt_gpu.h).
+
+The library is built in-tree by ``beamtrace2007_b200.build``; loading fails
+loudly when it is missing -- there is no CPU path behind these calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libbt_gpu.so")
+
+BT_OK = 0
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "capacity exceeded",
+          -5: "round limit", -6: "no CUDA device", -7: "busy", -8: "size over limit"}
+
+
+class BtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Camera(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("fwd", C.c_float * 3), ("right", C.c_float * 3), ("down", C.c_float * 3),
+                ("half_w", C.c_float), ("half_h", C.c_float), ("W", C.c_int32), ("H", C.c_int32)]
+
+    def as_array(self) -> np.ndarray:
+        """eye fwd right down half_w half_h as 14 doubles (the oracle's camera form)."""
+        return np.array(list(self.eye) + list(self.fwd) + list(self.right) + list(self.down) +
+                        [self.half_w, self.half_h], np.float64)
+
+
+class AreaLight(C.Structure):
+    _fields_ = [("c", C.c_float * 3), ("U", C.c_float * 3), ("V", C.c_float * 3)]
+
+    @staticmethod
+    def from_array(a) -> "AreaLight":
+        a = np.asarray(a, np.float32).ravel()
+        L = AreaLight()
+        for i in range(3):
+            L.c[i], L.U[i], L.V[i] = a[i], a[3 + i], a[6 + i]
+        return L
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("num_verts", C.c_int64), ("tris", C.c_void_p), ("tri_normals", C.c_void_p),
+                ("num_tris", C.c_int64), ("bounds", C.c_float * 6)]
+
+
+class KdDesc(C.Structure):
+    _fields_ = [("split", C.c_void_p), ("data", C.c_void_p), ("offset", C.c_void_p), ("parent", C.c_void_p),
+                ("node_box", C.c_void_p), ("num_nodes", C.c_int64), ("tri_indices", C.c_void_p),
+                ("num_refs", C.c_int64), ("bounds", C.c_float * 6)]
+
+
+class KdParams(C.Structure):
+    _fields_ = [("cost_traverse", C.c_float), ("cost_intersect", C.c_float), ("empty_bonus", C.c_float),
+                ("max_depth", C.c_int32), ("bin_threshold", C.c_int32), ("bins", C.c_int32),
+                ("clip_bounds", C.c_int32), ("single_leaf", C.c_int32)]
+
+
+class GpuInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("sm_count", C.c_int32), ("mem_gb", C.c_double), ("cc_major", C.c_int32),
+                ("cc_minor", C.c_int32)]
+
+
+class GpuConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("budget", C.c_int32), ("primary_budget", C.c_int32),
+                ("capacity", C.c_int64), ("blocks_per_sm", C.c_int32), ("split_batch", C.c_int32),
+                ("max_retries", C.c_int32)]
+
+
+class SoftOpts(C.Structure):
+    _fields_ = [("exact", C.c_int32), ("offset", C.c_float)]
+
+
+class RunInfo(C.Structure):
+    _fields_ = [("kd_steps", C.c_uint64), ("leaf_visits", C.c_uint64), ("tri_tests", C.c_uint64),
+                ("hits", C.c_uint64), ("splits", C.c_uint64), ("beams", C.c_uint64), ("root_beams", C.c_uint64),
+                ("presplit_beams", C.c_uint64), ("five_splits", C.c_uint64), ("climbs", C.c_uint64),
+                ("dropped_area", C.c_double), ("eps_band_corners", C.c_uint64), ("eps_fp64_flips", C.c_uint64),
+                ("ms_primary", C.c_double), ("ms_trace", C.c_double), ("ms_total", C.c_double),
+                ("ms_round", C.c_double), ("launches", C.c_int32), ("round_launches", C.c_int32),
+                ("passes", C.c_int32), ("retried_roots", C.c_int32), ("max_spill", C.c_int32),
+                ("roots", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Polys(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("n", C.c_void_p), ("tri", C.c_void_p), ("area", C.c_void_p),
+                ("root", C.c_void_p), ("cap", C.c_int64)]
+
+
+_P = C.c_void_p
+_I = C.c_int
+_I64 = C.c_int64
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "bt_gpu_last_error": (C.c_char_p, []),
+    "bt_gpu_config_default": (None, [C.POINTER(GpuConfig)]),
+    "bt_scene_finalize": (_I64, [_P, _I64, _P, _I64, _P, _P, _P, _P]),
+    "bt_kd_params_default": (None, [C.POINTER(KdParams)]),
+    "bt_kd_build": (_I, [_P, _P, _P, _I64, _P, C.POINTER(KdParams), C.POINTER(_P)]),
+    "bt_kd_sizes": (None, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "bt_kd_view": (None, [_P, C.POINTER(KdDesc)]),
+    "bt_kd_free": (None, [_P]),
+    "bt_camera_make": (None, [_P, _P, C.c_float, _P, C.c_int32, C.c_int32, C.POINTER(Camera)]),
+    "bt_gpu_available": (_I, [C.POINTER(GpuInfo)]),
+    "bt_gpu_create": (_I, [C.POINTER(SceneDesc), C.POINTER(KdDesc), C.POINTER(GpuConfig), C.POINTER(_P)]),
+    "bt_gpu_destroy": (_I, [_P]),
+    "bt_gpu_soft": (_I, [_P, C.POINTER(Camera), C.POINTER(AreaLight), C.POINTER(SoftOpts), _P, _P, _P, _P,
+                         C.POINTER(RunInfo)]),
+    "bt_gpu_soft_points": (_I, [_P, C.POINTER(AreaLight), C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P, _P,
+                                C.POINTER(RunInfo)]),
+    "bt_gpu_soft_points_device": (_I, [_P, C.POINTER(AreaLight), C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P,
+                                       _P, C.POINTER(RunInfo)]),
+    "bt_gpu_soft_device": (_I, [_P, C.POINTER(Camera), C.POINTER(AreaLight), C.POINTER(SoftOpts), _P, _P, _P, _P,
+                                C.POINTER(RunInfo)]),
+    "bt_gpu_primary_rays": (_I, [_P, C.POINTER(Camera), _P, _P, _P]),
+    "bt_gpu_primary_rays_device": (_I, [_P, C.POINTER(Camera), _P, _P, _P]),
+    "bt_gpu_primary": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, C.POINTER(Polys), C.POINTER(_I64),
+                            C.POINTER(RunInfo)]),
+    "bt_gpu_point": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, _P, C.POINTER(Polys), C.POINTER(_I64),
+                          C.POINTER(RunInfo)]),
+    "bt_gpu_raster": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, C.POINTER(Polys), _I64, _P, _P]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libbt_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m beamtrace2007_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int):
+    if code != BT_OK:
+        raise BtError(code, lib().bt_gpu_last_error().decode(errors="replace"))
+    return code
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

@@ -1,0 +1,1624 @@
+// The B200 beam engine: persistent warps over sub-beam records, and the
+// C-ABI entry points (include/bt_gpu.h).
+//
+// Work hierarchy, innermost first:
+//   lane registers   one sub-beam per lane, traced leaf by leaf;
+//   warp stack       a LIFO of records in shared memory (kStack per warp):
+//                    pieces of a clip and of a root's pre-split stay with the
+//                    warp that made them, so a beam tree is traced depth-first
+//                    by one warp with its kd cells hot in L1;
+//   spill queues     two global queues of 64-byte records; a warp whose stack
+//                    is full appends to the "next" queue, which the following
+//                    launch consumes.
+// A launch ("round") admits new roots as lanes fall idle, as long as their
+// budget of live sub-beams fits in the free queue slots, so the spill queue
+// can never overflow.  A root that would exceed its budget is abandoned and
+// traced again, on the GPU, in a retry pass with a 16x budget (the reference
+// recomputed such roots on the CPU, cuda/gpu_render.cu:651-672).
+//
+// Lanes that need a clip park until `split_batch` lanes of the warp wait (or
+// no lane can trace), then clip together: trace and clip each run with most
+// lanes converged.  Both phases work on the same per-lane record, so a lane
+// never holds two beams in registers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bt_gpu.h"
+#include "engine_core.cuh"
+
+using namespace btg;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void setErr(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+#define CK(x)                                                                         \
+  do {                                                                                \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess) {                                                          \
+      setErr("%s: %s (%s:%d)", #x, cudaGetErrorString(e_), __FILE__, __LINE__);     \
+      return BT_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 4;
+constexpr int kThreads = 32 * kWarps;
+constexpr int kStack = 40;
+constexpr double kFixVis = 1099511627776.0;         // 2^40: visible fraction, fixed point
+constexpr double kFixG = 1152921504606846976.0;     // 2^60: Lambert integral, fixed point
+constexpr int kMaxLaunches = 20000;  // launches per call before BT_ERR_TIMEOUT
+
+enum App { kAppSoft = 0, kAppPrimary = 1, kAppPoint = 2 };
+enum RootState { kRootNone = 0, kRootTraced = 1, kRootKilled = 2 };
+enum Phase { kIdle = 0, kLoaded = 1, kTrace = 2, kSplit = 3 };
+
+// Engine state shared by all warps of a pass.
+struct Counters {
+  int count[2];      // records in spill queue 0 / 1
+  int head;          // fetch cursor in the queue being consumed
+  int rootNext;      // next entry of the root list to admit
+  int inflight;      // admitted roots not finished
+  int killed;        // roots abandoned in this pass
+  unsigned long long reserved;  // spill slots reserved by roots in flight
+  int maxSpill;
+  int overflow;      // a spill found no slot (impossible by the reservation rule)
+  int outCount;      // output polygons
+  int done;
+  int launches;
+  int pad;
+};
+
+// Per-root query: plane, tolerances, mode (WfRoot, cuda/wavefront.cu:80-86).
+struct __align__(16) RootRec {
+  float4 a, b, c, d, e, f;  // O.xyz ext | p0.xyz exclude | u.xyz lightArea | v.xyz flags | n.xyz attempt | d.xyz -
+};
+
+struct OutPolyDev {
+  float* x;
+  float* y;
+  int32_t* n;
+  int32_t* tri;
+  float* area;
+  int32_t* root;
+  int32_t* attempt;
+  int cap;
+};
+
+struct AppParams {
+  // image / camera
+  int W, H, tilesX, tile, tilesW, cull, tiled;
+  Plane camPlane;
+  V3 eye, fwd, right, down;
+  float halfW, halfH;
+  // soft shadows
+  V3 Lc, LU, LV;
+  float offset;
+  int exact;
+  const int32_t* pixTri;
+  const float* pixX;
+  const float* pixN;
+  float *vis, *E, *Eu;
+  unsigned long long* missFx;
+  unsigned long long* gFx;
+  float4* shade;  // x, ns per root
+  // point shadows
+  V3 pointLight;
+  const float* hx;
+  const float* hy;
+  const int32_t* hn;
+  const int32_t* htri;
+  OutPolyDev out;
+};
+
+struct RoundParams {
+  SceneDev s;
+  SubBeam* q[2];
+  int cur;
+  int capacity;
+  int budget;
+  int numRoots;
+  const int32_t* rootList;
+  RootRec* roots;
+  int32_t* live;
+  int32_t* state;
+  int32_t* attempt;
+  Counters* ctr;
+  unsigned long long* stats;
+  int splitBatch;
+  AppParams app;
+};
+
+__device__ __forceinline__ int laneId() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ float asF(int i) { return __int_as_float(i); }
+__device__ __forceinline__ int asI(float f) { return __float_as_int(f); }
+
+__device__ void storeRoot(RootRec* R, const Query& q, float lightArea, int attempt) {
+  RootRec r;
+  r.a = make_float4(q.P.O.x, q.P.O.y, q.P.O.z, q.ext);
+  r.b = make_float4(q.P.p0.x, q.P.p0.y, q.P.p0.z, asF(q.exclude));
+  r.c = make_float4(q.P.u.x, q.P.u.y, q.P.u.z, lightArea);
+  r.d = make_float4(q.P.v.x, q.P.v.y, q.P.v.z, asF(q.mode | (q.farIsPlane << 1) | (q.cull << 2)));
+  r.e = make_float4(q.P.n.x, q.P.n.y, q.P.n.z, asF(attempt));
+  r.f = make_float4(q.P.d.x, q.P.d.y, q.P.d.z, 0.f);
+  *R = r;
+}
+
+__device__ void loadRoot(const RootRec* R, Query& q, float& lightArea) {
+  const float4 a = R->a, b = R->b, c = R->c, d = R->d, e = R->e, f = R->f;
+  q.P.O = mk(a.x, a.y, a.z);
+  q.P.p0 = mk(b.x, b.y, b.z);
+  q.P.u = mk(c.x, c.y, c.z);
+  q.P.v = mk(d.x, d.y, d.z);
+  q.P.n = mk(e.x, e.y, e.z);
+  q.P.d = mk(f.x, f.y, f.z);
+  q.exclude = asI(b.w);
+  const int fl = asI(d.w);
+  q.mode = fl & 1;
+  q.farIsPlane = (fl >> 1) & 1;
+  q.cull = (fl >> 2) & 1;
+  lightArea = c.w;
+  querySetup(q, a.w);
+}
+
+__device__ void rootDone(const RoundParams& p) {
+  atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)p.budget));
+  atomicSub(&p.ctr->inflight, 1);
+}
+
+__device__ void liveSub(const RoundParams& p, int root, int n) {
+  if (n > 0 && atomicSub(&p.live[root], n) == n) rootDone(p);
+}
+
+__device__ void killRoot(const RoundParams& p, int root) {
+  if (atomicExch(&p.state[root], int(kRootKilled)) != int(kRootKilled)) atomicAdd(&p.ctr->killed, 1);
+}
+
+__device__ void appendPoly(const RoundParams& p, int root, const float* x, const float* y, int n, int tri,
+                           float area) {
+  const int k = atomicAdd(&p.ctr->outCount, 1);
+  if (k >= p.app.out.cap) return;  // counted: the host retries with a larger buffer
+  const OutPolyDev& o = p.app.out;
+  for (int i = 0; i < 4; ++i) {
+    const int j = i < n ? i : n - 1;
+    o.x[4 * k + i] = x[j];
+    o.y[4 * k + i] = y[j];
+  }
+  o.n[k] = n;
+  o.tri[k] = tri;
+  o.area[k] = area;
+  o.root[k] = root;
+  o.attempt[k] = p.attempt[root];
+}
+
+// Finished pieces.  Soft: unoccluded area (fixed point) and, with exact, the
+// FP64 Lambert integral; primary: visible polygons; point shadows: occluded
+// pieces projected back into the image (WfOut, cuda/wavefront.cu:193-227).
+template <int App>
+__device__ void outputPiece(const RoundParams& p, const Query& q, float lightArea, int root, const Beam& b, int tri,
+                            Stats& st) {
+  Poly<4> poly;
+  const float area = beamPoly(b, poly);
+  if (tri >= 0) st.hits++;
+  st.beams++;
+  if (App == kAppSoft) {
+    if (tri >= 0) return;
+    const double f = double(area) / double(lightArea) * kFixVis;
+    if (f > 0) atomicAdd(&p.app.missFx[root], (unsigned long long)llrint(f));
+    if (p.app.exact) {
+      V3 P[4];
+      for (int i = 0; i < poly.n; ++i) P[i] = planePoint(q.P, poly.x[i], poly.y[i]);
+      const float4 xs = p.app.shade[2 * root], ns = p.app.shade[2 * root + 1];
+      const double G = formFactorFP64(mk(xs.x, xs.y, xs.z), mk(ns.x, ns.y, ns.z), P, poly.n);
+      const double g = G * kFixG;
+      if (g > 0) atomicAdd(&p.app.gFx[root], (unsigned long long)llrint(g));
+    }
+    return;
+  }
+  if (tri < 0) return;
+  if (App == kAppPrimary) {
+    appendPoly(p, root, poly.x, poly.y, poly.n, tri, area);
+  } else {
+    float ox[4], oy[4];
+    const int T = q.exclude;
+    if (pointShadowToImage(p.app.camPlane, q.P, poly.x, poly.y, poly.n, ox, oy)) appendPoly(p, root, ox, oy, poly.n, T, 0.f);
+  }
+}
+
+// Per-lane environment for admission and clip emission: the first queued
+// piece stays in the lane, the rest go to the warp stack (or spill).
+template <int App>
+struct LaneEnv {
+  const RoundParams* p;
+  const Query* q;
+  float lightArea;
+  int root;
+  SubBeam* stack;
+  int* top;
+  Stats* st;
+  SubBeam first;
+  int haveFirst;
+  int queued;
+  __device__ bool queue(const SubBeam& r) {
+    ++queued;
+    if (!haveFirst) {
+      first = r;
+      haveFirst = 1;
+      return true;
+    }
+    const int slot = atomicAdd(top, 1);
+    if (slot < kStack) {
+      stack[slot] = r;
+      return true;
+    }
+    const int nxt = p->cur ^ 1;
+    const int g = atomicAdd(&p->ctr->count[nxt], 1);
+    if (g < p->capacity) {
+      p->q[nxt][g] = r;
+      return true;
+    }
+    atomicExch(&p->ctr->overflow, 1);
+    return false;
+  }
+  __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
+  __device__ void missed(const Beam& b) { outputPiece<App>(*p, *q, lightArea, root, b, -1, *st); }
+  __device__ void dropped(float) {}
+};
+
+// Root k of an 8x4-pixel tile per warp (cuda/wavefront.cu:245-252).
+__device__ __forceinline__ bool softPixel(const AppParams& a, int k, int& pix) {
+  if (!a.tiled) {
+    pix = k;
+    return true;
+  }
+  const int tile = k >> 5, l = k & 31;
+  const int x = (tile % a.tilesX) * 8 + (l & 7), y = (tile / a.tilesX) * 4 + (l >> 3);
+  pix = y * a.W + x;
+  return x < a.W && y < a.H;
+}
+
+// Sets up root k and queues its pre-split pieces (admitRoot,
+// cuda/wavefront.cu:255-325).  Returns true if the lane took a piece.
+template <int App>
+__device__ bool admit(const RoundParams& p, int k, SubBeam* stack, int* top, Stats& st, SubBeam& first, Query& q,
+                      float& lightArea) {
+  p.live[k] = 0;
+  p.state[k] = kRootNone;
+  const int att = p.attempt[k] + 1;
+  p.attempt[k] = att;
+  Poly<8> poly;
+  poly.clear();
+  lightArea = 0;
+  if (App == kAppSoft) {
+    p.app.missFx[k] = 0;
+    p.app.gFx[k] = 0;
+    int pix;
+    if (!softPixel(p.app, k, pix)) {
+      rootDone(p);
+      return false;
+    }
+    const int T = p.app.pixTri[pix];
+    if (T < 0) {
+      if (p.app.vis) p.app.vis[pix] = -1;
+      if (p.app.E) p.app.E[pix] = 0;
+      if (p.app.Eu) p.app.Eu[pix] = 0;
+      rootDone(p);
+      return false;
+    }
+    const V3 x = mk(p.app.pixX[3 * pix], p.app.pixX[3 * pix + 1], p.app.pixX[3 * pix + 2]);
+    const V3 ns = mk(p.app.pixN[3 * pix], p.app.pixN[3 * pix + 1], p.app.pixN[3 * pix + 2]);
+    const float A = length(cross(p.app.LU, p.app.LV));
+    if (p.app.Eu) p.app.Eu[pix] = A * lightCenterG(p.app.Lc, p.app.LU, p.app.LV, x, ns);
+    if (!lightBeamSetup(p.app.Lc, p.app.LU, p.app.LV, x, ns, T, p.app.offset, q, poly, lightArea)) {
+      if (p.app.vis) p.app.vis[pix] = 0;
+      if (p.app.E) p.app.E[pix] = 0;
+      rootDone(p);
+      return false;
+    }
+    p.app.shade[2 * k] = make_float4(x.x, x.y, x.z, 0.f);
+    p.app.shade[2 * k + 1] = make_float4(ns.x, ns.y, ns.z, 0.f);
+  } else if (App == kAppPrimary) {
+    const int tx = k % p.app.tilesW, ty = k / p.app.tilesW;
+    const int x0 = tx * p.app.tile, y0 = ty * p.app.tile;
+    const int x1 = min(p.app.W, x0 + p.app.tile), y1 = min(p.app.H, y0 + p.app.tile);
+    const float qx0 = (2 * float(x0) / float(p.app.W) - 1) * p.app.halfW;
+    const float qx1 = (2 * float(x1) / float(p.app.W) - 1) * p.app.halfW;
+    const float qy0 = (2 * float(y0) / float(p.app.H) - 1) * p.app.halfH;
+    const float qy1 = (2 * float(y1) / float(p.app.H) - 1) * p.app.halfH;
+    poly.push(qx0, qy0);
+    poly.push(qx1, qy0);
+    poly.push(qx1, qy1);
+    poly.push(qx0, qy1);
+    q.P = p.app.camPlane;
+    q.mode = kModeNearest;
+    q.farIsPlane = 0;
+    q.exclude = -1;
+    q.cull = p.app.cull;
+  } else {
+    const int T = p.app.htri[k];
+    float px[4], py[4];
+    const int n = p.app.hn[k];
+    for (int i = 0; i < 4; ++i) {
+      px[i] = p.app.hx[4 * k + i];
+      py[i] = p.app.hy[4 * k + i];
+    }
+    if (T < 0) {
+      rootDone(p);
+      return false;
+    }
+    V3 nT, v0;
+    triNV(p.s, T, nT, v0);
+    if (!pointShadowSetup(p.app.eye, p.app.fwd, p.app.right, p.app.down, nT, v0, T, p.app.pointLight, px, py, n, q,
+                          poly)) {
+      appendPoly(p, k, px, py, n, T, 0.f);  // receiver faces away from the light: all in shadow
+      p.state[k] = kRootTraced;
+      rootDone(p);
+      return false;
+    }
+  }
+  querySetup(q, poly.extent());
+  storeRoot(&p.roots[k], q, lightArea, att);
+  p.state[k] = kRootTraced;
+  LaneEnv<App> env{&p, &q, lightArea, k, stack, top, &st, SubBeam(), 0, 0};
+  const bool ok = admitRoot(p.s, q, poly, k, env, st);
+  p.live[k] = env.queued;
+  if (!ok || env.queued > p.budget) killRoot(p, k);
+  if (env.queued == 0) {
+    rootDone(p);
+    return false;
+  }
+  if (env.haveFirst) first = env.first;
+  return env.haveFirst != 0;
+}
+
+__device__ void flushStats(const RoundParams& p, const Stats& st) {
+  unsigned long long v[kStDropped] = {st.kdSteps, st.leafVisits, st.triTests, st.hits, st.splits,
+                                      st.beams, st.rootBeams, st.presplitBeams, st.fiveSplits, st.climbs};
+  for (int f = 0; f < kStDropped; ++f) {
+    unsigned long long s = v[f];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+    if (laneId() == 0 && s) atomicAdd(&p.stats[f], s);
+  }
+  double d = st.dropped;
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(kFull, d, o);
+  if (laneId() == 0 && d != 0) atomicAdd(reinterpret_cast<double*>(&p.stats[kStDropped]), d);
+}
+
+template <int App>
+__global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
+  __shared__ SubBeam sStack[kWarps][kStack];
+  __shared__ int sTop[kWarps];
+  const int lane = laneId(), wid = threadIdx.x >> 5;
+  const unsigned ltMask = (1u << lane) - 1u;
+  SubBeam* stack = sStack[wid];
+  int* top = &sTop[wid];
+  if (lane == 0) *top = 0;
+  __syncwarp();
+  const int nCur = min(p.ctr->count[p.cur], p.capacity);
+  const SubBeam* qCur = p.q[p.cur];
+  bool queueDone = nCur == 0, rootsDone = false;
+  int phase = kIdle;
+  SubBeam r;
+  Beam b;
+  Query q;
+  Walk w;
+  float lightArea = 0;
+  int qRoot = -1;
+  Stats st;
+  st.clear();
+  for (;;) {
+    // ---- refill idle lanes: warp stack, then spill queue, then new roots
+    unsigned idle = __ballot_sync(kFull, phase == kIdle);
+    if (idle) {
+      const int t0 = *top;
+      const int take = min(__popc(idle), t0);
+      const int rank = __popc(idle & ltMask);
+      if (phase == kIdle && rank < take) {
+        r = stack[t0 - 1 - rank];
+        phase = kLoaded;
+      }
+      __syncwarp();
+      if (lane == 0) *top = t0 - take;
+      __syncwarp();
+      idle = __ballot_sync(kFull, phase == kIdle);
+      if (idle && !queueDone) {
+        const int ni = __popc(idle);
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&p.ctr->head, ni);
+        base = __shfl_sync(kFull, base, 0);
+        if (base + ni >= nCur) queueDone = true;
+        const int i = base + __popc(idle & ltMask);
+        if (phase == kIdle && i < nCur) {
+          r = qCur[i];
+          phase = kLoaded;
+        }
+        idle = __ballot_sync(kFull, phase == kIdle);
+      }
+      if (idle && !rootsDone) {
+        const int ni = __popc(idle);
+        int base = -1;
+        if (lane == 0) {
+          const unsigned long long need = (unsigned long long)ni * (unsigned long long)p.budget;
+          const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
+          if (old + need > (unsigned long long)p.capacity) {
+            atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)need));
+          } else {
+            base = atomicAdd(&p.ctr->rootNext, ni);
+            const int got = max(0, min(ni, p.numRoots - base));
+            if (got < ni)
+              atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - got)) * (unsigned long long)p.budget);
+            if (got > 0) atomicAdd(&p.ctr->inflight, got);
+          }
+        }
+        base = __shfl_sync(kFull, base, 0);
+        if (base < 0 || base + ni >= p.numRoots) rootsDone = true;
+        const int j = base + __popc(idle & ltMask);
+        if (base >= 0 && phase == kIdle && j < p.numRoots) {
+          const int k = p.rootList ? p.rootList[j] : j;
+          if (admit<App>(p, k, stack, top, st, r, q, lightArea)) {
+            qRoot = k;
+            phase = kLoaded;
+          } else {
+            qRoot = -1;
+          }
+        }
+        __syncwarp();
+        if (lane == 0 && *top > kStack) *top = kStack;
+      }
+    }
+    __syncwarp();
+    // ---- expand newly loaded records
+    if (phase == kLoaded) {
+      if (r.n == 0 || p.state[r.root] == kRootKilled) {
+        liveSub(p, r.root, 1);
+        phase = kIdle;
+      } else {
+        if (r.root != qRoot) {
+          loadRoot(&p.roots[r.root], q, lightArea);
+          qRoot = r.root;
+        }
+        expand(p.s, q, r, b);
+        walkBegin(p.s, r, w);
+        phase = kTrace;
+      }
+    }
+    const unsigned tr = __ballot_sync(kFull, phase == kTrace);
+    const unsigned sp = __ballot_sync(kFull, phase == kSplit);
+    const unsigned idleNow = __ballot_sync(kFull, phase == kIdle);
+    if (!tr && !sp) {
+      if (queueDone && rootsDone && *top == 0) break;
+      continue;
+    }
+    const bool doSplit = sp && (__popc(sp) >= p.splitBatch || !tr || idleNow);
+    if (doSplit) {
+      if (phase == kSplit) {
+        TriInfo ti;
+        Line L[5];
+        int nl = 0;
+        bool commit = false;
+        const int slots = splitPass1<LaneEnv<App>>(p.s, q, r, b, st, ti, L, nl, commit);
+        if (slots < 0) {
+          killRoot(p, r.root);
+          liveSub(p, r.root, 1);
+          phase = kIdle;
+        } else if (!commit) {
+          r.cursor += 1;
+          w.phase = kPhTest;
+          phase = kTrace;
+        } else {
+          const int root = r.root;
+          const int old = atomicAdd(&p.live[root], slots - 1);
+          if (old + slots - 1 > p.budget) {
+            killRoot(p, root);
+            liveSub(p, root, slots);
+            phase = kIdle;
+          } else {
+            LaneEnv<App> env{&p, &q, lightArea, root, stack, top, &st, SubBeam(), 0, 0};
+            splitPass2(q, r, b, ti, L, nl, env, st);
+            if (env.queued < slots) liveSub(p, root, slots - env.queued);
+            if (env.haveFirst) {
+              r = env.first;
+              expand(p.s, q, r, b);
+              walkBegin(p.s, r, w);
+              phase = kTrace;
+            } else {
+              phase = kIdle;
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && *top > kStack) *top = kStack;
+      __syncwarp();
+    } else if (phase == kTrace) {
+      // one leaf: climb / descend to it, then test its triangles
+      int res = advance(p.s, q, b, r, w, st);
+      int occ = -1;
+      if (res == kStepContinue) {
+        for (;;) {
+          res = testOne(p.s, q, r, b, st, occ);
+          if (res != kStepContinue || !moreInLeaf(p.s, q, r)) break;
+        }
+      }
+      if (res == kStepFinished) {
+        outputPiece<App>(p, q, lightArea, r.root, b, occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1), st);
+        liveSub(p, r.root, 1);
+        phase = kIdle;
+      } else if (res == kStepSplit) {
+        phase = kSplit;
+      }
+    }
+  }
+  flushStats(p, st);
+}
+
+// Between launches: the consumed queue is emptied, completion is decided
+// (scheduleKernel's bookkeeping, cuda/wavefront.cu:327-345).
+__global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
+  const int nxt = cur ^ 1;
+  if (c->count[nxt] > c->maxSpill) c->maxSpill = c->count[nxt];
+  c->count[cur] = 0;
+  c->head = 0;
+  c->launches++;
+  c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
+}
+
+// Roots abandoned in a pass, compacted for the retry pass.
+__global__ void collectKilledKernel(const int32_t* state, const int32_t* list, int n, int32_t* out, int* count) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int k = list ? list[j] : j;
+  if (state[k] == kRootKilled) out[atomicAdd(count, 1)] = k;
+}
+
+// vis = missFx / 2^40 (clamped), E = Lambert integral or A G0 V
+// (finalizeSoftKernel, cuda/wavefront.cu:539-561).
+__global__ void softFinalizeKernel(AppParams a, const int32_t* state, int R) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= R) return;
+  int pix;
+  if (!softPixel(a, k, pix)) return;
+  if (state[k] != kRootTraced) return;
+  double V = double(a.missFx[k]) / kFixVis;
+  V = V < 0 ? 0 : (V > 1 ? 1 : V);
+  const float Vf = float(V);
+  if (a.vis) a.vis[pix] = Vf;
+  if (a.E) {
+    if (a.exact) {
+      a.E[pix] = float(double(a.gFx[k]) / kFixG);
+    } else {
+      const V3 x = mk(a.pixX[3 * pix], a.pixX[3 * pix + 1], a.pixX[3 * pix + 2]);
+      const V3 ns = mk(a.pixN[3 * pix], a.pixN[3 * pix + 1], a.pixN[3 * pix + 2]);
+      const float A = length(cross(a.LU, a.LV));
+      a.E[pix] = A * lightCenterG(a.Lc, a.LU, a.LV, x, ns) * Vf;
+    }
+  }
+}
+
+// ------------------------------------------------------------ primary rays
+
+// Moller-Trumbore (rayHitTri, src/ray/ray_core.h:22-37).
+__device__ __forceinline__ float rayHit(V3 o, V3 d, V3 v0, V3 v1, V3 v2) {
+  V3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+  V3 pv = cross(d, e2);
+  float det = dot(e1, pv);
+  if (det == 0) return kInf;
+  float inv = 1 / det;
+  V3 tv = sub(o, v0);
+  float u = dot(tv, pv) * inv;
+  if (u < 0 || u > 1) return kInf;
+  V3 qv = cross(tv, e1);
+  float v = dot(d, qv) * inv;
+  if (v < 0 || u + v > 1) return kInf;
+  return dot(e2, qv) * inv;
+}
+
+// One ray per pixel centre, nearest hit with coplanar ties to the lower id
+// (primaryKernel + rayTraverse<false>, cuda/gpu_render.cu:222-244,
+// src/ray/ray_core.h:42-132): tri, X, N (normal facing the eye).
+__global__ void __launch_bounds__(128) primaryRaysKernel(SceneDev s, bt_camera cam, int32_t* triOut, float* Xout,
+                                                         float* Nout) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cam.W || y >= cam.H) return;
+  const size_t k = size_t(y) * size_t(cam.W) + size_t(x);
+  const float qx = (2 * (float(x) + 0.5f) / float(cam.W) - 1) * cam.half_w;
+  const float qy = (2 * (float(y) + 0.5f) / float(cam.H) - 1) * cam.half_h;
+  const V3 o = mk(cam.eye[0], cam.eye[1], cam.eye[2]);
+  const V3 fwd = mk(cam.fwd[0], cam.fwd[1], cam.fwd[2]), right = mk(cam.right[0], cam.right[1], cam.right[2]),
+           down = mk(cam.down[0], cam.down[1], cam.down[2]);
+  const V3 d = add(add(fwd, mul(right, qx)), mul(down, qy));
+  triOut[k] = -1;
+  Xout[3 * k] = Xout[3 * k + 1] = Xout[3 * k + 2] = 0;
+  Nout[3 * k] = Nout[3 * k + 1] = Nout[3 * k + 2] = 0;
+  float t0 = 0, t1 = kInf;
+  float inv[3];
+  for (int a = 0; a < 3; ++a) {
+    const float da = comp(d, a), oa = comp(o, a);
+    inv[a] = 1 / da;
+    if (da == 0) {
+      if (oa < s.bounds.lo[a] || oa > s.bounds.hi[a]) return;
+      continue;
+    }
+    float ta = (s.bounds.lo[a] - oa) * inv[a];
+    float tb = (s.bounds.hi[a] - oa) * inv[a];
+    if (ta > tb) {
+      float tt = ta;
+      ta = tb;
+      tb = tt;
+    }
+    t0 = t0 > ta ? t0 : ta;
+    t1 = t1 < tb ? t1 : tb;
+  }
+  if (t0 > t1) return;
+  struct Entry {
+    uint32_t node;
+    float t0, t1;
+  };
+  Entry stk[64];
+  int sp = 0;
+  uint32_t node = 0;
+  float best = kInf;
+  int bestTri = -1;
+  const float tieEps = 4 * 1.1920928955078125e-07f;
+  for (;;) {
+    const uint2 nd = s.node[node];
+    if (!isLeaf(nd)) {
+      const int a = int(nd.y & 3u);
+      const float sp_ = splitOf(nd);
+      const float oa = comp(o, a), da = comp(d, a);
+      const bool belowFirst = oa < sp_ || (oa == sp_ && da <= 0);
+      const uint32_t first = belowFirst ? node + 1 : (nd.y >> 2);
+      const uint32_t second = belowFirst ? (nd.y >> 2) : node + 1;
+      if (da == 0) {
+        node = first;
+        continue;
+      }
+      const float tp = (sp_ - oa) * inv[a];
+      if (tp > t1 || tp <= 0) {
+        node = first;
+      } else if (tp < t0) {
+        node = second;
+      } else {
+        if (sp < 64) stk[sp++] = Entry{second, tp, t1};
+        node = first;
+        t1 = tp;
+      }
+      continue;
+    }
+    const uint32_t cnt = nd.y >> 2;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      const TriRec t = loadRef(s, nd.x + i);
+      const float th = rayHit(o, d, t.v0, t.v1, t.v2);
+      if (!(th > 0 && th < kInf)) continue;
+      const float tol = bestTri < 0 ? 0.f : best * tieEps;
+      if (bestTri < 0 || th < best - tol || (th <= best + tol && t.tri < bestTri)) {
+        best = th;
+        bestTri = t.tri;
+      }
+    }
+    if (bestTri >= 0 && best <= t1) break;
+    if (sp == 0) break;
+    --sp;
+    node = stk[sp].node;
+    t0 = stk[sp].t0;
+    t1 = stk[sp].t1;
+  }
+  if (bestTri < 0) return;
+  triOut[k] = bestTri;
+  const V3 X = add(o, mul(d, best));
+  V3 nT, v0;
+  triNV(s, bestTri, nT, v0);
+  if (dot(nT, d) > 0) nT = neg(nT);
+  Xout[3 * k] = X.x;
+  Xout[3 * k + 1] = X.y;
+  Xout[3 * k + 2] = X.z;
+  Nout[3 * k] = nT.x;
+  Nout[3 * k + 1] = nT.y;
+  Nout[3 * k + 2] = nT.z;
+}
+
+// ---------------------------------------------------------------- raster
+
+// Covers pixel centres with convex image-plane polygons (rasterize,
+// src/render/render.cpp:49-95, one sample at the pixel centre): one thread
+// per polygon; among polygons covering a centre (shared edges) the higher
+// triangle id wins, so the result does not depend on polygon order.
+__global__ void rasterKernel(bt_camera cam, const float* px_, const float* py_, const int32_t* pn, const int32_t* ptri,
+                             int64_t np, int shadow, int32_t* triBuf, uint8_t* flagBuf) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int n = pn[i], tri = ptri[i];
+  if (!shadow && tri < 0) return;
+  if (n < 3 || n > 4) return;
+  double px[4], py[4], A[4], B[4], C[4];
+  double ly = 1e300, hy = -1e300;
+  for (int k = 0; k < n; ++k) {
+    const float x = (px_[4 * i + k] / cam.half_w + 1) * 0.5f * float(cam.W);
+    const float y = (py_[4 * i + k] / cam.half_h + 1) * 0.5f * float(cam.H);
+    px[k] = double(x);
+    py[k] = double(y);
+    ly = ly < py[k] ? ly : py[k];
+    hy = hy > py[k] ? hy : py[k];
+  }
+  for (int k = 0; k < n; ++k) {
+    const int j = k + 1 == n ? 0 : k + 1;
+    A[k] = -(py[j] - py[k]);
+    B[k] = px[j] - px[k];
+    C[k] = -(A[k] * px[k] + B[k] * py[k]);
+  }
+  const double o = 0.5;
+  const int y0 = max(0, int(ceil(ly - o))), y1 = min(cam.H - 1, int(floor(hy - o)));
+  for (int y = y0; y <= y1; ++y) {
+    const double sy = y + o;
+    double xl = -1e300, xr = 1e300;
+    bool empty = false;
+    for (int k = 0; k < n && !empty; ++k) {
+      const double rr = B[k] * sy + C[k];
+      if (A[k] > 0)
+        xl = xl > -rr / A[k] ? xl : -rr / A[k];
+      else if (A[k] < 0)
+        xr = xr < -rr / A[k] ? xr : -rr / A[k];
+      else if (rr < 0)
+        empty = true;
+    }
+    if (empty || xl > xr) continue;
+    const int x0 = max(0, int(ceil(xl - o))), x1 = min(cam.W - 1, int(floor(xr - o)));
+    for (int x = x0; x <= x1; ++x) {
+      const size_t k = size_t(y) * size_t(cam.W) + size_t(x);
+      if (shadow)
+        flagBuf[k] = 1;
+      else
+        atomicMax(&triBuf[k], tri);
+    }
+  }
+}
+
+__global__ void fillKernel(int32_t* p, int64_t n, int32_t v) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+template <class T>
+int devAlloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  if (e != cudaSuccess) {
+    setErr("cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  return BT_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ context
+
+struct bt_gpu_ctx {
+  int device = 0;
+  int sms = 1;
+  bt_gpu_config cfg;
+  cudaStream_t stream = nullptr;
+  // scene
+  uint2* dNode = nullptr;
+  float4* dBox = nullptr;
+  uint32_t* dParent = nullptr;
+  float4* dRef = nullptr;
+  float4* dTriNV = nullptr;
+  SceneDev s;
+  float offset = 0;  // |scene diagonal| * kEpsRel
+  int64_t numTris = 0;
+  // engine
+  SubBeam* dQ[2] = {nullptr, nullptr};
+  int capacity = 0;
+  Counters* dCtr = nullptr;
+  unsigned long long* dStats = nullptr;
+  size_t rootCap = 0;
+  RootRec* dRoots = nullptr;
+  int32_t *dLive = nullptr, *dState = nullptr, *dAttempt = nullptr, *dList[2] = {nullptr, nullptr};
+  unsigned long long *dMiss = nullptr, *dG = nullptr;
+  float4* dShade = nullptr;
+  int* dKillCount = nullptr;
+  // outputs
+  int64_t outCap = 0;
+  float *dOx = nullptr, *dOy = nullptr, *dOarea = nullptr;
+  int32_t *dOn = nullptr, *dOtri = nullptr, *dOroot = nullptr, *dOatt = nullptr;
+  // per-image scratch
+  int64_t pixCap = 0;
+  int32_t* dPixTri = nullptr;
+  float *dPixX = nullptr, *dPixN = nullptr, *dVis = nullptr, *dE = nullptr, *dEu = nullptr;
+  int blocksSoft = 0, blocksPrimary = 0, blocksPoint = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t rev[2] = {nullptr, nullptr};
+};
+
+extern "C" {
+
+const char* bt_gpu_last_error(void) { return g_err; }
+
+void bt_gpu_config_default(bt_gpu_config* c) {
+  c->device = 0;
+  c->budget = 128;
+  c->primary_budget = 4096;
+  c->capacity = 0;
+  c->blocks_per_sm = 0;
+  c->split_batch = 12;
+  c->max_retries = 4;
+}
+
+int bt_gpu_available(bt_gpu_info* info) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    setErr("no CUDA device");
+    return BT_ERR_NODEVICE;
+  }
+  if (info) {
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, 0) != cudaSuccess) return BT_ERR_NODEVICE;
+    snprintf(info->name, sizeof info->name, "%s", pr.name);
+    info->sm_count = pr.multiProcessorCount;
+    info->mem_gb = double(pr.totalGlobalMem) / double(1 << 30);
+    info->cc_major = pr.major;
+    info->cc_minor = pr.minor;
+  }
+  return BT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int ensureRoots(bt_gpu_ctx* c, size_t R) {
+  if (c->rootCap >= R) return BT_OK;
+  cudaFree(c->dRoots);
+  cudaFree(c->dLive);
+  cudaFree(c->dState);
+  cudaFree(c->dAttempt);
+  cudaFree(c->dList[0]);
+  cudaFree(c->dList[1]);
+  cudaFree(c->dMiss);
+  cudaFree(c->dG);
+  cudaFree(c->dShade);
+  c->rootCap = 0;
+  int e;
+  if ((e = devAlloc(&c->dRoots, R)) || (e = devAlloc(&c->dLive, R)) || (e = devAlloc(&c->dState, R)) ||
+      (e = devAlloc(&c->dAttempt, R)) || (e = devAlloc(&c->dList[0], R)) || (e = devAlloc(&c->dList[1], R)) ||
+      (e = devAlloc(&c->dMiss, R)) || (e = devAlloc(&c->dG, R)) || (e = devAlloc(&c->dShade, 2 * R)))
+    return e;
+  c->rootCap = R;
+  return BT_OK;
+}
+
+int ensureOut(bt_gpu_ctx* c, int64_t cap) {
+  if (c->outCap >= cap) return BT_OK;
+  cudaFree(c->dOx);
+  cudaFree(c->dOy);
+  cudaFree(c->dOarea);
+  cudaFree(c->dOn);
+  cudaFree(c->dOtri);
+  cudaFree(c->dOroot);
+  cudaFree(c->dOatt);
+  c->outCap = 0;
+  int e;
+  if ((e = devAlloc(&c->dOx, size_t(4 * cap))) || (e = devAlloc(&c->dOy, size_t(4 * cap))) ||
+      (e = devAlloc(&c->dOarea, size_t(cap))) || (e = devAlloc(&c->dOn, size_t(cap))) ||
+      (e = devAlloc(&c->dOtri, size_t(cap))) || (e = devAlloc(&c->dOroot, size_t(cap))) ||
+      (e = devAlloc(&c->dOatt, size_t(cap))))
+    return e;
+  c->outCap = cap;
+  return BT_OK;
+}
+
+int ensurePix(bt_gpu_ctx* c, int64_t n) {
+  if (c->pixCap >= n) return BT_OK;
+  cudaFree(c->dPixTri);
+  cudaFree(c->dPixX);
+  cudaFree(c->dPixN);
+  cudaFree(c->dVis);
+  cudaFree(c->dE);
+  cudaFree(c->dEu);
+  c->pixCap = 0;
+  int e;
+  if ((e = devAlloc(&c->dPixTri, size_t(n))) || (e = devAlloc(&c->dPixX, size_t(3 * n))) ||
+      (e = devAlloc(&c->dPixN, size_t(3 * n))) || (e = devAlloc(&c->dVis, size_t(n))) ||
+      (e = devAlloc(&c->dE, size_t(n))) || (e = devAlloc(&c->dEu, size_t(n))))
+    return e;
+  c->pixCap = n;
+  return BT_OK;
+}
+
+template <int App>
+int gridFor(bt_gpu_ctx* c) {
+  int perSM = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, roundKernel<App>, kThreads, 0);
+  if (c->cfg.blocks_per_sm > 0) perSM = c->cfg.blocks_per_sm;
+  return c->sms * std::max(1, perSM);
+}
+
+void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
+  if (!info) return;
+  unsigned long long st[kNumStats];
+  cudaMemcpy(st, c->dStats, sizeof st, cudaMemcpyDeviceToHost);
+  info->kd_steps = st[kStKd];
+  info->leaf_visits = st[kStLeaf];
+  info->tri_tests = st[kStTests];
+  info->hits = st[kStHits];
+  info->splits = st[kStSplits];
+  info->beams = st[kStBeams];
+  info->root_beams = st[kStRoots];
+  info->presplit_beams = st[kStPresplit];
+  info->five_splits = st[kStFive];
+  info->climbs = st[kStClimbs];
+  double d;
+  memcpy(&d, &st[kStDropped], sizeof d);
+  info->dropped_area = d;
+  info->eps_band_corners = st[kStEpsBand];
+  info->eps_fp64_flips = st[kStEpsFlip];
+  info->max_spill = std::max(info->max_spill, hc.maxSpill);
+}
+
+// Runs every root of `R` through the engine: passes of launches until all
+// roots are done; roots abandoned over budget are retried with 16x budget.
+template <int App>
+int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info) {
+  int e = ensureRoots(c, size_t(R));
+  if (e) return e;
+  CK(cudaMemsetAsync(c->dAttempt, 0, sizeof(int32_t) * size_t(R), c->stream));
+  CK(cudaMemsetAsync(c->dStats, 0, sizeof(unsigned long long) * kNumStats, c->stream));
+  app.missFx = c->dMiss;
+  app.gFx = c->dG;
+  app.shade = c->dShade;
+  RoundParams p;
+  p.s = c->s;
+  p.q[0] = c->dQ[0];
+  p.q[1] = c->dQ[1];
+  p.capacity = c->capacity;
+  p.roots = c->dRoots;
+  p.live = c->dLive;
+  p.state = c->dState;
+  p.attempt = c->dAttempt;
+  p.ctr = c->dCtr;
+  p.stats = c->dStats;
+  p.splitBatch = std::max(1, std::min(32, c->cfg.split_batch));
+  p.app = app;
+  const int grid = gridFor<App>(c);
+  int launches = 0, passes = 0, retried = 0;
+  const int32_t* list = nullptr;
+  int n = R;
+  Counters hc;
+  memset(&hc, 0, sizeof hc);
+  for (int pass = 0;; ++pass) {
+    p.budget = budget;
+    if (int64_t(budget) > c->capacity) {
+      setErr("a root needs more than %d live sub-beams (capacity %d)", budget / 16, c->capacity);
+      return BT_ERR_CAPACITY;
+    }
+    p.numRoots = n;
+    p.rootList = list;
+    CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
+    ++passes;
+    for (int cur = 0;; cur ^= 1) {
+      p.cur = cur;
+      CK(cudaEventRecord(c->rev[0], c->stream));
+      roundKernel<App><<<grid, kThreads, 0, c->stream>>>(p);
+      CK(cudaEventRecord(c->rev[1], c->stream));
+      roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, cur, n);
+      launches += 2;
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (info) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
+        info->ms_round += ms;
+        info->round_launches++;
+      }
+      if (hc.overflow) {
+        setErr("spill queue overflow (capacity %d)", c->capacity);
+        return BT_ERR_CAPACITY;
+      }
+      if (hc.done) break;
+      if (launches > kMaxLaunches) {
+        setErr("round limit reached");
+        return BT_ERR_TIMEOUT;
+      }
+    }
+    if (info) info->max_spill = std::max(info->max_spill, hc.maxSpill);
+    if (hc.killed == 0) break;
+    if (pass >= c->cfg.max_retries) {
+      setErr("%d roots still over budget %d after %d retries", hc.killed, budget, pass);
+      return BT_ERR_CAPACITY;
+    }
+    // retry the abandoned roots with a larger budget
+    int32_t* dst = c->dList[pass & 1];
+    CK(cudaMemsetAsync(c->dKillCount, 0, sizeof(int), c->stream));
+    collectKilledKernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->dState, list, n, dst, c->dKillCount);
+    launches++;
+    int nk = 0;
+    CK(cudaMemcpyAsync(&nk, c->dKillCount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    retried += nk;
+    list = dst;
+    n = nk;
+    budget *= 16;
+  }
+  if (info) {
+    info->launches += launches;
+    info->passes += passes;
+    info->retried_roots += retried;
+    info->roots += R;
+    fillInfo(c, hc, info);
+  }
+  return BT_OK;
+}
+
+int uploadScene(bt_gpu_ctx* c, const bt_scene_desc* sc, const bt_kd_desc* kd) {
+  const int64_t nn = kd->num_nodes, nr = kd->num_refs, nt = sc->num_tris;
+  std::vector<uint2> node(static_cast<size_t>(nn));
+  std::vector<float4> box(static_cast<size_t>(2 * nn));
+  for (int64_t i = 0; i < nn; ++i) {
+    const uint32_t d = kd->data[i];
+    uint32_t x;
+    if ((d & 3u) == 3u) {
+      x = kd->offset[i];
+      if (int64_t(x) + int64_t(d >> 2) > nr) {
+        setErr("kd leaf %lld points past the reference list", (long long)i);
+        return BT_ERR_INVALID;
+      }
+    } else {
+      memcpy(&x, &kd->split[i], 4);
+      if (int64_t(d >> 2) >= nn) {
+        setErr("kd node %lld has an invalid child", (long long)i);
+        return BT_ERR_INVALID;
+      }
+    }
+    node[size_t(i)] = make_uint2(x, d);
+    const float* b = kd->node_box + 6 * i;
+    box[size_t(2 * i)] = make_float4(b[0], b[1], b[2], b[3]);
+    box[size_t(2 * i + 1)] = make_float4(b[4], b[5], 0.f, 0.f);
+  }
+  std::vector<float4> ref(static_cast<size_t>(4 * nr));
+  for (int64_t k = 0; k < nr; ++k) {
+    const uint32_t t = kd->tri_indices[k];
+    if (int64_t(t) >= nt) {
+      setErr("kd reference %lld names triangle %u of %lld", (long long)k, t, (long long)nt);
+      return BT_ERR_INVALID;
+    }
+    const uint32_t* vi = sc->tris + 3 * size_t(t);
+    const float* p0 = sc->pos + 3 * size_t(vi[0]);
+    const float* p1 = sc->pos + 3 * size_t(vi[1]);
+    const float* p2 = sc->pos + 3 * size_t(vi[2]);
+    const float* n = sc->tri_normals + 3 * size_t(t);
+    float w[4];
+    uint32_t u[4] = {vi[0], vi[1], vi[2], t};
+    memcpy(w, u, 16);
+    ref[size_t(4 * k)] = make_float4(p0[0], p0[1], p0[2], p1[0]);
+    ref[size_t(4 * k + 1)] = make_float4(p1[1], p1[2], p2[0], p2[1]);
+    ref[size_t(4 * k + 2)] = make_float4(p2[2], n[0], n[1], n[2]);
+    ref[size_t(4 * k + 3)] = make_float4(w[0], w[1], w[2], w[3]);
+  }
+  std::vector<float4> tnv(static_cast<size_t>(2 * nt));
+  for (int64_t t = 0; t < nt; ++t) {
+    const float* n = sc->tri_normals + 3 * t;
+    const float* p0 = sc->pos + 3 * size_t(sc->tris[3 * t]);
+    tnv[size_t(2 * t)] = make_float4(n[0], n[1], n[2], 0.f);
+    tnv[size_t(2 * t + 1)] = make_float4(p0[0], p0[1], p0[2], 0.f);
+  }
+  int e;
+  if ((e = devAlloc(&c->dNode, size_t(nn))) || (e = devAlloc(&c->dBox, size_t(2 * nn))) ||
+      (e = devAlloc(&c->dParent, size_t(nn))) || (e = devAlloc(&c->dRef, size_t(4 * nr))) ||
+      (e = devAlloc(&c->dTriNV, size_t(2 * nt))))
+    return e;
+  CK(cudaMemcpy(c->dNode, node.data(), sizeof(uint2) * node.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dBox, box.data(), sizeof(float4) * box.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dParent, kd->parent, sizeof(uint32_t) * size_t(nn), cudaMemcpyHostToDevice));
+  if (nr) CK(cudaMemcpy(c->dRef, ref.data(), sizeof(float4) * ref.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dTriNV, tnv.data(), sizeof(float4) * tnv.size(), cudaMemcpyHostToDevice));
+  c->s.node = c->dNode;
+  c->s.box = c->dBox;
+  c->s.parent = c->dParent;
+  c->s.ref = c->dRef;
+  c->s.triNV = c->dTriNV;
+  for (int a = 0; a < 3; ++a) {
+    c->s.bounds.lo[a] = kd->bounds[a];
+    c->s.bounds.hi[a] = kd->bounds[3 + a];
+  }
+  c->s.numTris = int(nt);
+  c->numTris = nt;
+  // offset = length(scene.bounds.diag()) * kEpsRel (render.cpp:348)
+  V3 dg = mk(sc->bounds[3] - sc->bounds[0], sc->bounds[4] - sc->bounds[1], sc->bounds[5] - sc->bounds[2]);
+  c->offset = length(dg) * kEpsRel;
+  return BT_OK;
+}
+
+AppParams baseApp(const bt_gpu_ctx* c, const bt_camera* cam) {
+  AppParams a;
+  memset(&a, 0, sizeof a);
+  if (cam) {
+    a.W = cam->W;
+    a.H = cam->H;
+    a.eye = mk(cam->eye[0], cam->eye[1], cam->eye[2]);
+    a.fwd = mk(cam->fwd[0], cam->fwd[1], cam->fwd[2]);
+    a.right = mk(cam->right[0], cam->right[1], cam->right[2]);
+    a.down = mk(cam->down[0], cam->down[1], cam->down[2]);
+    a.halfW = cam->half_w;
+    a.halfH = cam->half_h;
+    // Camera::plane (render_types.h:21)
+    a.camPlane = makePlane(a.eye, add(a.eye, a.fwd), a.right, a.down);
+  }
+  a.out.x = c->dOx;
+  a.out.y = c->dOy;
+  a.out.n = c->dOn;
+  a.out.tri = c->dOtri;
+  a.out.area = c->dOarea;
+  a.out.root = c->dOroot;
+  a.out.attempt = c->dOatt;
+  a.out.cap = int(std::min<int64_t>(c->outCap, 0x7fffffff));
+  return a;
+}
+
+bool camOk(const bt_camera* cam) { return cam && cam->W > 0 && cam->H > 0 && cam->W <= 65536 && cam->H <= 65536; }
+
+int softCore(bt_gpu_ctx* c, const bt_area_light* L, const bt_soft_opts* o, int64_t n, const bt_camera* cam,
+             const int32_t* dTri, const float* dX, const float* dN, float* dVis, float* dE, float* dEu,
+             bt_run_info* info) {
+  AppParams a = baseApp(c, cam);
+  a.Lc = mk(L->c[0], L->c[1], L->c[2]);
+  a.LU = mk(L->U[0], L->U[1], L->U[2]);
+  a.LV = mk(L->V[0], L->V[1], L->V[2]);
+  a.offset = (o && o->offset > 0) ? o->offset : c->offset;
+  a.exact = o ? o->exact : 0;
+  a.pixTri = dTri;
+  a.pixX = dX;
+  a.pixN = dN;
+  a.vis = dVis;
+  a.E = dE;
+  a.Eu = dEu;
+  int R;
+  if (cam) {
+    a.tiled = 1;
+    a.tilesX = (cam->W + 7) / 8;
+    R = a.tilesX * ((cam->H + 3) / 4) * 32;
+  } else {
+    a.tiled = 0;
+    a.W = int(n);
+    a.H = 1;
+    R = int(n);
+  }
+  if (R == 0) return BT_OK;
+  int e = runRoots<kAppSoft>(c, a, R, c->cfg.budget, info);
+  if (e) return e;
+  a.missFx = c->dMiss;
+  a.gFx = c->dG;
+  softFinalizeKernel<<<(R + 255) / 256, 256, 0, c->stream>>>(a, c->dState, R);
+  if (info) info->launches++;
+  CK(cudaGetLastError());
+  return BT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu_config* cfg, bt_gpu_ctx** out) {
+  if (!scene || !kd || !out || scene->num_tris <= 0 || kd->num_nodes <= 0) {
+    setErr("bt_gpu_create: empty scene or tree");
+    return BT_ERR_INVALID;
+  }
+  *out = nullptr;
+  bt_gpu_ctx* c = new bt_gpu_ctx();
+  if (cfg)
+    c->cfg = *cfg;
+  else
+    bt_gpu_config_default(&c->cfg);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || c->cfg.device < 0 || c->cfg.device >= ndev) {
+    cudaGetLastError();
+    delete c;
+    setErr("no CUDA device %d", cfg ? cfg->device : 0);
+    return BT_ERR_NODEVICE;
+  }
+  c->device = c->cfg.device;
+  int e = BT_OK;
+  auto fail = [&](int code) {
+    bt_gpu_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(BT_ERR_CUDA);
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(BT_ERR_CUDA);
+  for (auto& ev : c->ev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
+  for (auto& ev : c->rev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
+  if ((e = uploadScene(c, scene, kd))) return fail(e);
+  // Spill queues: two of `capacity` 64-byte records.  Default: 2^25 records
+  // (2 GiB per queue), at most 10% of the free memory.
+  int64_t cap = c->cfg.capacity;
+  if (cap <= 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    cap = std::min<int64_t>(int64_t(1) << 25, int64_t(fr / 10 / (2 * sizeof(SubBeam))));
+  }
+  cap = std::max<int64_t>(cap, 1024);
+  cap = std::min<int64_t>(cap, int64_t(1) << 30);
+  c->capacity = int(cap);
+  if ((e = devAlloc(&c->dQ[0], size_t(cap))) || (e = devAlloc(&c->dQ[1], size_t(cap))) ||
+      (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) || (e = devAlloc(&c->dKillCount, 1)))
+    return fail(e);
+  *out = c;
+  return BT_OK;
+}
+
+int bt_gpu_destroy(bt_gpu_ctx* c) {
+  if (!c) return BT_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dCtr, c->dStats,
+                  c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
+                  c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
+                  c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  for (auto& ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->rev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return BT_OK;
+}
+
+int bt_gpu_primary_rays_device(bt_gpu_ctx* c, const bt_camera* cam, int32_t* dTri, float* dX, float* dN) {
+  if (!c || !camOk(cam) || !dTri || !dX || !dN) return BT_ERR_INVALID;
+  CK(cudaSetDevice(c->device));
+  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, dTri, dX, dN);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+int bt_gpu_soft(bt_gpu_ctx* c, const bt_camera* cam, const bt_area_light* L, const bt_soft_opts* o, int32_t* tri,
+                float* vis, float* E, float* Eu, bt_run_info* info) {
+  if (!c || !camOk(cam) || !L) {
+    setErr("bt_gpu_soft: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t np = int64_t(cam->W) * cam->H;
+  int e = ensurePix(c, np);
+  if (e) return e;
+  if (info) memset(info, 0, sizeof *info);
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, c->dPixTri, c->dPixX, c->dPixN);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  if (info) info->launches++;
+  e = softCore(c, L, o, np, cam, c->dPixTri, c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, info);
+  if (e) return e;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  if (tri) CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, c->stream));
+  if (vis) CK(cudaMemcpyAsync(vis, c->dVis, sizeof(float) * np, cudaMemcpyDeviceToHost, c->stream));
+  if (E) CK(cudaMemcpyAsync(E, c->dE, sizeof(float) * np, cudaMemcpyDeviceToHost, c->stream));
+  if (Eu) CK(cudaMemcpyAsync(Eu, c->dEu, sizeof(float) * np, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float a = 0, b = 0, t = 0;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[3]);
+    info->ms_primary = a;
+    info->ms_trace = b;
+    info->ms_total = t;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_soft_device(bt_gpu_ctx* c, const bt_camera* cam, const bt_area_light* L, const bt_soft_opts* o,
+                       int32_t* dTri, float* dVis, float* dE, float* dEu, bt_run_info* info) {
+  if (!c || !camOk(cam) || !L || !dTri) {
+    setErr("bt_gpu_soft_device: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t np = int64_t(cam->W) * cam->H;
+  int e = ensurePix(c, np);
+  if (e) return e;
+  if (info) memset(info, 0, sizeof *info);
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, dTri, c->dPixX, c->dPixN);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  if (info) info->launches++;
+  e = softCore(c, L, o, np, cam, dTri, c->dPixX, c->dPixN, dVis, dE, dEu, info);
+  if (e) return e;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    info->ms_primary = a;
+    info->ms_trace = b;
+    info->ms_total = a + b;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_primary_rays(bt_gpu_ctx* c, const bt_camera* cam, int32_t* tri, float* X, float* N) {
+  if (!c || !camOk(cam) || !tri || !X || !N) {
+    setErr("bt_gpu_primary_rays: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t np = int64_t(cam->W) * cam->H;
+  int e = ensurePix(c, np);
+  if (e) return e;
+  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, c->dPixTri, c->dPixX, c->dPixN);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(X, c->dPixX, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(N, c->dPixN, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+int bt_gpu_soft_points_device(bt_gpu_ctx* c, const bt_area_light* L, const bt_soft_opts* o, int64_t n,
+                              const int32_t* dTri, const float* dX, const float* dN, float* dVis, float* dE, float* dEu,
+                              bt_run_info* info) {
+  if (!c || !L || n < 0 || n > 0x7fffffff || (n > 0 && (!dTri || !dX || !dN))) {
+    setErr("bt_gpu_soft_points_device: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  int e = softCore(c, L, o, n, nullptr, dTri, dX, dN, dVis, dE, dEu, info);
+  if (e) return e;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float b = 0;
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    info->ms_trace = b;
+    info->ms_total = b;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_soft_points(bt_gpu_ctx* c, const bt_area_light* L, const bt_soft_opts* o, int64_t n, const int32_t* tri,
+                       const float* X, const float* N, float* vis, float* E, float* Eu, bt_run_info* info) {
+  if (!c || !L || n < 0 || (n > 0 && (!tri || !X || !N))) {
+    setErr("bt_gpu_soft_points: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  int e = ensurePix(c, std::max<int64_t>(n, 1));
+  if (e) return e;
+  if (n > 0) {
+    CK(cudaMemcpyAsync(c->dPixTri, tri, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->dPixX, X, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->dPixN, N, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  }
+  e = bt_gpu_soft_points_device(c, L, o, n, c->dPixTri, c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, info);
+  if (e) return e;
+  if (n > 0) {
+    if (vis) CK(cudaMemcpyAsync(vis, c->dVis, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (E) CK(cudaMemcpyAsync(E, c->dE, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    if (Eu) CK(cudaMemcpyAsync(Eu, c->dEu, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Copies the polygons of roots that finished in their last attempt to the
+// host (downloadPolys, cuda/wavefront.cu:766-783).
+int downloadPolys(bt_gpu_ctx* c, int64_t produced, int R, bt_polys* out, int64_t* count) {
+  const int64_t n = std::min<int64_t>(produced, c->outCap);
+  std::vector<float> x(static_cast<size_t>(4 * n)), y(static_cast<size_t>(4 * n)), area(static_cast<size_t>(n));
+  std::vector<int32_t> nn(static_cast<size_t>(n)), tri(static_cast<size_t>(n)), root(static_cast<size_t>(n)), att(static_cast<size_t>(n)), state(static_cast<size_t>(R)),
+      attempt(static_cast<size_t>(R));
+  if (n > 0) {
+    CK(cudaMemcpy(x.data(), c->dOx, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(y.data(), c->dOy, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(area.data(), c->dOarea, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nn.data(), c->dOn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tri.data(), c->dOtri, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(root.data(), c->dOroot, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(att.data(), c->dOatt, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+  }
+  CK(cudaMemcpy(state.data(), c->dState, sizeof(int32_t) * R, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(attempt.data(), c->dAttempt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost));
+  int64_t k = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int r = root[size_t(i)];
+    if (state[size_t(r)] != kRootTraced || att[size_t(i)] != attempt[size_t(r)]) continue;
+    if (k < out->cap) {
+      for (int j = 0; j < 4; ++j) {
+        out->x[4 * k + j] = x[size_t(4 * i + j)];
+        out->y[4 * k + j] = y[size_t(4 * i + j)];
+      }
+      out->n[k] = nn[size_t(i)];
+      out->tri[k] = tri[size_t(i)];
+      out->area[k] = area[size_t(i)];
+      if (out->root) out->root[k] = r;
+    }
+    ++k;
+  }
+  *count = k;
+  return BT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_gpu_primary(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t tile, bt_polys* out, int64_t* count,
+                   bt_run_info* info) {
+  if (!c || !camOk(cam) || tile <= 0 || !out || !count) {
+    setErr("bt_gpu_primary: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  const int tilesW = (cam->W + tile - 1) / tile, tilesH = (cam->H + tile - 1) / tile;
+  const int R = tilesW * tilesH;
+  int64_t cap = std::max<int64_t>(int64_t(1) << 16, int64_t(cam->W) * cam->H * 2);
+  for (;;) {
+    int e = ensureOut(c, cap);
+    if (e) return e;
+    AppParams a = baseApp(c, cam);
+    a.tile = tile;
+    a.tilesW = tilesW;
+    a.cull = cull ? 1 : 0;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    e = runRoots<kAppPrimary>(c, a, R, c->cfg.primary_budget, info);
+    if (e) return e;
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    Counters hc;
+    CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hc.outCount > c->outCap) {
+      cap = int64_t(hc.outCount) + hc.outCount / 4;
+      continue;
+    }
+    if (info) {
+      float b = 0;
+      cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+      info->ms_trace = b;
+      info->ms_total = b;
+    }
+    return downloadPolys(c, hc.outCount, R, out, count);
+  }
+}
+
+int bt_gpu_point(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* hits, int64_t nh, const float* light,
+                 bt_polys* out, int64_t* count, bt_run_info* info) {
+  if (!c || !camOk(cam) || !hits || nh < 0 || nh > 0x7fffffff || !light || !out || !count) {
+    setErr("bt_gpu_point: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  *count = 0;
+  if (nh == 0) return BT_OK;
+  for (int64_t i = 0; i < nh; ++i)
+    if (hits->tri[i] >= c->numTris || hits->n[i] < 3 || hits->n[i] > 4) {
+      setErr("bt_gpu_point: hit polygon %lld is invalid", (long long)i);
+      return BT_ERR_INVALID;
+    }
+  float *dhx, *dhy;
+  int32_t *dhn, *dht;
+  int e;
+  if ((e = devAlloc(&dhx, size_t(4 * nh))) || (e = devAlloc(&dhy, size_t(4 * nh))) ||
+      (e = devAlloc(&dhn, size_t(nh))) || (e = devAlloc(&dht, size_t(nh))))
+    return e;
+  struct Free {
+    void* p[4];
+    ~Free() {
+      for (void* q : p) cudaFree(q);
+    }
+  } guard{{dhx, dhy, dhn, dht}};
+  CK(cudaMemcpy(dhx, hits->x, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dhy, hits->y, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dhn, hits->n, sizeof(int32_t) * nh, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dht, hits->tri, sizeof(int32_t) * nh, cudaMemcpyHostToDevice));
+  int64_t cap = std::max<int64_t>(int64_t(1) << 16, nh * 4);
+  for (;;) {
+    if ((e = ensureOut(c, cap))) return e;
+    AppParams a = baseApp(c, cam);
+    a.pointLight = mk(light[0], light[1], light[2]);
+    a.hx = dhx;
+    a.hy = dhy;
+    a.hn = dhn;
+    a.htri = dht;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    e = runRoots<kAppPoint>(c, a, int(nh), c->cfg.budget, info);
+    if (e) return e;
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    Counters hc;
+    CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hc.outCount > c->outCap) {
+      cap = int64_t(hc.outCount) + hc.outCount / 4;
+      continue;
+    }
+    if (info) {
+      float b = 0;
+      cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+      info->ms_trace = b;
+      info->ms_total = b;
+    }
+    return downloadPolys(c, hc.outCount, int(nh), out, count);
+  }
+}
+
+int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int64_t np, const bt_polys* shadow,
+                  int64_t ns, int32_t* tri, uint8_t* flag) {
+  if (!c || !camOk(cam) || np < 0 || ns < 0 || (np > 0 && !prim) || (ns > 0 && !shadow)) {
+    setErr("bt_gpu_raster: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t npix = int64_t(cam->W) * cam->H;
+  const int64_t m = std::max(np, ns);
+  float *dx, *dy;
+  int32_t *dn, *dt, *dtri;
+  uint8_t* dflag;
+  int e;
+  if ((e = devAlloc(&dx, size_t(4 * std::max<int64_t>(m, 1)))) || (e = devAlloc(&dy, size_t(4 * std::max<int64_t>(m, 1)))) ||
+      (e = devAlloc(&dn, size_t(std::max<int64_t>(m, 1)))) || (e = devAlloc(&dt, size_t(std::max<int64_t>(m, 1)))) ||
+      (e = devAlloc(&dtri, size_t(npix))) || (e = devAlloc(&dflag, size_t(npix))))
+    return e;
+  struct Free {
+    void* p[6];
+    ~Free() {
+      for (void* q : p) cudaFree(q);
+    }
+  } guard{{dx, dy, dn, dt, dtri, dflag}};
+  fillKernel<<<(npix + 255) / 256, 256, 0, c->stream>>>(dtri, npix, -1);
+  CK(cudaMemsetAsync(dflag, 0, size_t(npix), c->stream));
+  for (int pass = 0; pass < 2; ++pass) {
+    const bt_polys* P = pass == 0 ? prim : shadow;
+    const int64_t n = pass == 0 ? np : ns;
+    if (n == 0) continue;
+    CK(cudaMemcpyAsync(dx, P->x, sizeof(float) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dy, P->y, sizeof(float) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dn, P->n, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dt, P->tri, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream));
+    rasterKernel<<<int((n + 127) / 128), 128, 0, c->stream>>>(*cam, dx, dy, dn, dt, n, pass, dtri, dflag);
+    CK(cudaGetLastError());
+  }
+  if (tri) CK(cudaMemcpyAsync(tri, dtri, sizeof(int32_t) * npix, cudaMemcpyDeviceToHost, c->stream));
+  if (flag) CK(cudaMemcpyAsync(flag, dflag, size_t(npix), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+}  // extern "C"

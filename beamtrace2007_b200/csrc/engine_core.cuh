@@ -1,0 +1,501 @@
+// Per-sub-beam steps of the engine: expand a queued record, advance it
+// through the kd-tree to its next triangle, test triangles, clip and emit
+// pieces, admit a root.  Host/device code: the CUDA kernels (engine.cu) run
+// these per lane; a host emulator in the tests runs them one record at a time.
+//
+// A sub-beam visits the same kd cells and triangles in the same order as the
+// reference's BeamCore with the restart trail and no mailboxing
+// (src/beam/wavefront_core.h:17-19), so its pieces are bitwise the same.
+//
+// Scene layout in device memory (SceneView of beam_types.h:86-97, re-laid
+// for 128-bit loads):
+//   node[i]    uint2  {split bits | leaf offset, data}: low 2 bits of data are
+//              the axis (3 = leaf), the high bits the right child / count
+//   box[i]     2 x float4 {lo.xyz, hi.x}, {hi.yz, -, -}: node boxes for the
+//              restart-trail climb
+//   parent[i]  uint32
+//   ref[k]     4 x float4 per leaf reference, in leaf order (area-sorted):
+//              {v0.xyz, v1.x} {v1.yz, v2.xy} {v2.z, n.xyz} {vi0, vi1, vi2, tri}
+//   triNV[t]   2 x float4 {n.xyz, -}, {v0.xyz, -}: hit planes by triangle id
+#pragma once
+
+#include <string.h>
+
+#if !defined(__CUDACC__)
+#include <vector_functions.h>
+#include <vector_types.h>
+#endif
+
+#include "beam_math.cuh"
+
+namespace btg {
+
+struct SceneDev {
+  const uint2* node;
+  const float4* box;
+  const uint32_t* parent;
+  const float4* ref;
+  const float4* triNV;
+  Box bounds;
+  int numTris;
+};
+
+// A queued sub-beam: 64 bytes, self-contained (corners on the root's plane,
+// restart trail, kd position, root, hit, cursor in the leaf).
+struct __align__(16) SubBeam {
+  float qx[4], qy[4];
+  unsigned long long trail;
+  uint32_t node;
+  int32_t root;
+  int32_t hit;
+  int32_t cursor;  // next triangle in the leaf; -1: descend from `node`
+  int16_t depth;
+  int8_t n;
+  int8_t neg;
+};
+
+// Per-lane counters (TraceStats, src/util/stats.h:8-42).
+struct Stats {
+  uint32_t kdSteps, leafVisits, triTests, hits, splits, beams, rootBeams, presplitBeams, fiveSplits, climbs;
+  double dropped;
+  BT_HD void clear() {
+    kdSteps = leafVisits = triTests = hits = splits = beams = rootBeams = presplitBeams = fiveSplits = climbs = 0;
+    dropped = 0;
+  }
+};
+enum { kStKd, kStLeaf, kStTests, kStHits, kStSplits, kStBeams, kStRoots, kStPresplit, kStFive, kStClimbs,
+       kStDropped, kStEpsBand, kStEpsFlip, kNumStats };
+
+BT_HD bool isLeaf(uint2 nd) { return (nd.y & 3u) == 3u; }
+
+BT_HD Box loadBox(const SceneDev& s, uint32_t i) {
+  float4 a = s.box[2 * i], b = s.box[2 * i + 1];
+  Box B;
+  B.lo[0] = a.x;
+  B.lo[1] = a.y;
+  B.lo[2] = a.z;
+  B.hi[0] = a.w;
+  B.hi[1] = b.x;
+  B.hi[2] = b.y;
+  return B;
+}
+
+struct TriRec {
+  V3 v0, v1, v2, n;
+  uint32_t vi[3];
+  int tri;
+};
+
+BT_HD TriRec loadRef(const SceneDev& s, uint32_t k) {
+#if defined(__CUDA_ARCH__)
+  const float4 a = __ldg(&s.ref[4 * k]), b = __ldg(&s.ref[4 * k + 1]), c = __ldg(&s.ref[4 * k + 2]),
+               d = __ldg(&s.ref[4 * k + 3]);
+#else
+  const float4 a = s.ref[4 * k], b = s.ref[4 * k + 1], c = s.ref[4 * k + 2], d = s.ref[4 * k + 3];
+#endif
+  TriRec t;
+  t.v0 = mk(a.x, a.y, a.z);
+  t.v1 = mk(a.w, b.x, b.y);
+  t.v2 = mk(b.z, b.w, c.x);
+  t.n = mk(c.y, c.z, c.w);
+  float fv[4] = {d.x, d.y, d.z, d.w};
+  uint32_t u[4];
+  for (int i = 0; i < 4; ++i) memcpy(&u[i], &fv[i], 4);
+  t.vi[0] = u[0];
+  t.vi[1] = u[1];
+  t.vi[2] = u[2];
+  t.tri = int(u[3]);
+  return t;
+}
+
+BT_HD int refTri(const SceneDev& s, uint32_t k) {
+#if defined(__CUDA_ARCH__)
+  return __float_as_int(__ldg(&s.ref[4 * k + 3].w));
+#else
+  float f = s.ref[4 * k + 3].w;
+  int t;
+  memcpy(&t, &f, 4);
+  return t;
+#endif
+}
+
+BT_HD void triNV(const SceneDev& s, int t, V3& n, V3& v0) {
+  float4 a = s.triNV[2 * t], b = s.triNV[2 * t + 1];
+  n = mk(a.x, a.y, a.z);
+  v0 = mk(b.x, b.y, b.z);
+}
+
+BT_HD float splitOf(uint2 nd) {
+  float f;
+  memcpy(&f, &nd.x, 4);
+  return f;
+}
+
+// Record -> working beam (wfExpand, wavefront_core.h:92-112).
+BT_HD void expand(const SceneDev& s, const Query& q, const SubBeam& r, Beam& b) {
+  const int n = r.n, l3 = n > 3 ? 3 : 2;
+  for (int i = 0; i < 3; ++i) {
+    b.qx[i] = r.qx[i];
+    b.qy[i] = r.qy[i];
+  }
+  b.qx[3] = r.qx[l3];
+  b.qy[3] = r.qy[l3];
+  b.n = n;
+  b.neg = r.neg;
+  beamAxes(q, b);
+  if (r.hit >= 0) {
+    V3 nT, v0;
+    triNV(s, r.hit, nT, v0);
+    hitPlane(q, nT, v0, b.hitA, b.hitC);
+    b.hitN = nT;
+    setStatus(q, b, r.hit, b.hitA, b.hitC);
+  } else {
+    b.hitA[0] = b.hitA[1] = b.hitA[2] = b.hitC = 0;
+    b.hitN = mk(0, 0, 0);
+    setStatus(q, b, -1, nullptr, 0);
+  }
+}
+
+BT_HD void storeGeom(const Beam& b, SubBeam& r) {
+  r.n = int8_t(b.n);
+  for (int i = 0; i < 4; ++i) {
+    r.qx[i] = b.qx[i];
+    r.qy[i] = b.qy[i];
+  }
+  r.neg = int8_t(b.neg);
+}
+
+enum { kStepFinished = 0, kStepSplit = 1, kStepContinue = 2 };
+enum { kPhDescend = 0, kPhTest = 1, kPhClimb = 2 };
+
+// Where a record is in the per-lane state machine (WfStepState).
+struct Walk {
+  int phase;
+  Box box;
+};
+
+BT_HD void walkBegin(const SceneDev& s, const SubBeam& r, Walk& w) {
+  if (r.cursor < 0) {
+    w.phase = kPhDescend;
+    w.box = loadBox(s, r.node);
+  } else {
+    w.phase = kPhTest;
+  }
+}
+
+BT_HD int highestBit64(unsigned long long x) {
+#if defined(__CUDA_ARCH__)
+  return 63 - __clzll((long long)x);
+#else
+  return 63 - __builtin_clzll(x);
+#endif
+}
+
+// Descends to the next leaf / climbs to the next pending far child until a
+// triangle is pending (kStepContinue, phase kPhTest) or no cell is left
+// (kStepFinished: the caller outputs the beam) (wfAdvance,
+// wavefront_core.h:157-231).
+BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st) {
+  for (;;) {
+    if (w.phase == kPhDescend) {
+      for (;;) {
+        const uint2 nd = s.node[r.node];
+        if (isLeaf(nd)) break;
+        st.kdSteps++;
+        const int d = r.depth++;
+        const int a = int(nd.y & 3u);
+        const float sp = splitOf(nd);
+        const bool pos = !((B.neg >> a) & 1);
+        const float Ns = (pos ? 1.f : -1.f) * (sp - comp(q.P.O, a));
+        const uint32_t left = r.node + 1, right = nd.y >> 2;
+        Box lbox = w.box, rbox = w.box;
+        lbox.hi[a] = sp;
+        rbox.lo[a] = sp;
+        const uint32_t cs = pos ? right : left, co = pos ? left : right;
+        int dec = kFar;
+        if (Ns > 0) dec = decide(q, B, a, Ns, w.box);
+        if (dec == kFar) {
+          r.node = cs;
+          w.box = pos ? rbox : lbox;
+        } else {
+          if (dec == kBoth) r.trail |= 1ull << d;
+          r.node = co;
+          w.box = pos ? lbox : rbox;
+        }
+      }
+      r.cursor = 0;
+      st.leafVisits++;
+      w.phase = kPhTest;
+    }
+    if (w.phase == kPhTest) {
+      const uint2 leaf = s.node[r.node];
+      const uint32_t cnt = leaf.y >> 2;
+      uint32_t i = uint32_t(r.cursor);
+      while (i < cnt && refTri(s, leaf.x + i) == q.exclude) ++i;
+      r.cursor = int32_t(i);
+      if (i < cnt) return kStepContinue;
+      w.phase = kPhClimb;
+    }
+    for (;;) {
+      if (r.trail == 0) return kStepFinished;
+      const int d = highestBit64(r.trail);
+      uint32_t node = r.node;
+      for (int depth = r.depth; depth > d; --depth) {
+        node = s.parent[node];
+        st.climbs++;
+      }
+      r.trail &= (1ull << d) - 1;
+      const uint2 nd = s.node[node];
+      const uint32_t cs = ((B.neg >> (nd.y & 3u)) & 1) ? node + 1 : (nd.y >> 2);
+      r.node = node;
+      r.depth = int16_t(d);
+      const Box cb = loadBox(s, cs);
+      if (overlaps(q, B, cb)) {
+        r.node = cs;
+        r.depth = int16_t(d + 1);
+        r.cursor = -1;
+        w.phase = kPhDescend;
+        w.box = cb;
+        break;
+      }
+    }
+  }
+}
+
+// True if the leaf has another triangle to test (skipping the excluded one)
+// (wfMoreInLeaf, wavefront_core.h:272-279).
+BT_HD bool moreInLeaf(const SceneDev& s, const Query& q, SubBeam& r) {
+  const uint2 leaf = s.node[r.node];
+  const uint32_t cnt = leaf.y >> 2;
+  uint32_t i = uint32_t(r.cursor);
+  while (i < cnt && refTri(s, leaf.x + i) == q.exclude) ++i;
+  r.cursor = int32_t(i);
+  return i < cnt;
+}
+
+BT_HD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
+  TriRec t = loadRef(s, k);
+  triSetup(q, t.v0, t.v1, t.v2, t.n, t.vi, t.tri, ti);
+}
+
+// Tests the pending triangle (wfTestOne, wavefront_core.h:236-268).
+// kStepFinished: AnyHit beam fully occluded by `occluder` (caller outputs
+// it); kStepSplit: triangle `cursor` needs a clip.
+BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats& st, int& occluder) {
+  const uint2 leaf = s.node[r.node];
+  const uint32_t i = uint32_t(r.cursor);
+  r.cursor = int32_t(i + 1);
+  TriInfo ti;
+  setupRef(s, q, leaf.x + i, ti);
+  if (!ti.ok) return kStepContinue;
+  st.triTests++;
+  const int t = ti.tri;
+  if (B.hit == t) return kStepContinue;
+  Line L[5];
+  int nl;
+  const int res = classifyTri(q, B, ti, L, nl);
+  if (res == kTriKeep) return kStepContinue;
+  if (res == kTriAllIn) {
+    if (q.mode == kModeAnyHit) {
+      occluder = t;
+      return kStepFinished;
+    }
+    setStatus(q, B, t, ti.A, ti.C);
+    B.hitA[0] = ti.A[0];
+    B.hitA[1] = ti.A[1];
+    B.hitA[2] = ti.A[2];
+    B.hitC = ti.C;
+    B.hitN = ti.n;
+    r.hit = t;
+    return kStepContinue;
+  }
+  r.cursor = int32_t(i);
+  return kStepSplit;
+}
+
+// Sink of clipTri's first pass: the area of the pieces that take the new
+// status (wfSplitClip's commit rule, wavefront_core.h:350-363), and the
+// number of queue slots the pieces would take.
+struct AreaSink {
+  float newArea;
+  int slots0, slots1;
+  template <int N>
+  BT_HD bool push(int l, const Poly<N>& p) {
+    if (p.n > 5) return false;
+    if (l == 1)
+      newArea += p.area();
+    if (l == 0)
+      slots0 += p.n == 5 ? 2 : 1;
+    else
+      slots1 += p.n == 5 ? 2 : 1;
+    return true;
+  }
+};
+
+// Sink of the second pass: each piece (pentagons split into quad and
+// triangle) becomes a beam; queued pieces continue at the next triangle of
+// the leaf with their new status, AnyHit occluded pieces are output
+// (wfSplitEmit, wavefront_core.h:370-422).  Env provides
+//   queue(const SubBeam&)                a continuing piece
+//   occluded(const Beam&, int tri)       an AnyHit piece hidden by tri
+//   dropped(float area)                  a sliver below minArea
+template <class Env>
+struct EmitSink {
+  const Query* q;
+  const SubBeam* base;
+  const Beam* parent;
+  int t;
+  Env* env;
+  Stats* st;
+  template <int N>
+  BT_HD bool push(int l, const Poly<N>& p0) {
+    const bool hitNow = l == 1;
+    const bool queued = !(hitNow && q->mode == kModeAnyHit);
+    Poly<5> sub[2];
+    int ns = 1;
+    if (p0.n == 5) {
+      splitFive(p0, sub[0], sub[1]);
+      st->fiveSplits++;
+      ns = 2;
+    } else {
+      sub[0].copyFrom(p0);
+    }
+    for (int j = 0; j < ns; ++j) {
+      Beam nb;
+      float dropped = 0;
+      if (!beamGeom(*q, sub[j], parent->neg, nb, dropped)) {
+        st->dropped += double(dropped);
+        env->dropped(dropped);
+        continue;
+      }
+      if (!queued) {
+        env->occluded(nb, t);
+        continue;
+      }
+      SubBeam pr = *base;
+      storeGeom(nb, pr);
+      pr.hit = hitNow ? t : parent->hit;
+      env->queue(pr);
+    }
+    return true;
+  }
+};
+
+// Clip of a record whose pending triangle needs it (after testOne returned
+// kStepSplit).  Pass 1 decides whether any piece measurably changes status
+// and counts queue slots; pass 2 (only if it does) replays the same clip and
+// streams the pieces to env.  Returns -1 if the clip overflowed its fixed
+// lists (the root must be abandoned), else the slots pass 2 will use
+// (0 if nothing changes: the record continues unchanged at cursor + 1).
+template <class Env>
+BT_HD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
+                     Line* L, int& nl, bool& commit) {
+  const uint2 leaf = s.node[r.node];
+  setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
+  classifyTri(q, B, ti, L, nl);
+  Line Lc[5];
+  for (int i = 0; i < nl; ++i) Lc[i] = L[i];
+  AreaSink a{0.f, 0, 0};
+  uint32_t five = 0;
+  if (!clipTri<6>(q, B, Lc, nl, a, five)) return -1;
+  st.fiveSplits += five;
+  commit = a.newArea >= q.minArea;
+  if (!commit) return 0;
+  return a.slots0 + (q.mode == kModeAnyHit ? 0 : a.slots1);
+}
+
+template <class Env>
+BT_HD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
+                      Stats& st) {
+  st.splits++;
+  SubBeam base = r;
+  base.cursor = r.cursor + 1;
+  EmitSink<Env> sink{&q, &base, &B, ti.tri, &env, &st};
+  uint32_t five = 0;  // counted in pass 1
+  clipTri<6>(q, B, L, nl, sink, five);
+}
+
+// Root admission: pre-split pieces become records at the kd root; pieces
+// missing the scene box are output at once (wfAdmit, wavefront_core.h:428-471).
+// Env provides queue / missed(const Beam&) / dropped.
+template <class Env>
+struct AdmitEmit {
+  const SceneDev* s;
+  const Query* q;
+  int root;
+  Env* env;
+  Stats* st;
+  BT_HD bool piece(const Poly<8>& p, int negBits) {
+    Beam b;
+    float dropped = 0;
+    if (!beamGeom(*q, p, negBits, b, dropped)) {
+      st->dropped += double(dropped);
+      env->dropped(dropped);
+      return true;
+    }
+    b.hitA[0] = b.hitA[1] = b.hitA[2] = b.hitC = 0;
+    b.hitN = mk(0, 0, 0);
+    setStatus(*q, b, -1, nullptr, 0);
+    st->rootBeams++;
+    if (!overlaps(*q, b, s->bounds)) {
+      env->missed(b);
+      return true;
+    }
+    SubBeam r;
+    storeGeom(b, r);
+    r.trail = 0;
+    r.node = 0;
+    r.root = root;
+    r.hit = -1;
+    r.cursor = -1;
+    r.depth = 0;
+    return env->queue(r);
+  }
+  BT_HD void presplit() { st->presplitBeams++; }
+  BT_HD void dropped(float a) {
+    st->dropped += double(a);
+    env->dropped(a);
+  }
+};
+
+template <class Env>
+BT_HD bool admitRoot(const SceneDev& s, const Query& q, const Poly<8>& rootPoly, int root, Env& env, Stats& st) {
+  Poly<8> p = rootPoly;
+  if (p.n < 3) return true;
+  if (p.area() < 0) p.reverse();
+  AdmitEmit<Env> e{&s, &q, root, &env, &st};
+  return presplit(q, p, e);
+}
+
+// Final piece polygon and area (wfOutput, wavefront_core.h:125-132).
+BT_HD float beamPoly(const Beam& b, Poly<4>& p) {
+  p.n = b.n;
+  for (int i = 0; i < b.n; ++i) {
+    p.x[i] = b.qx[i];
+    p.y[i] = b.qy[i];
+  }
+  return p.area();
+}
+
+// Lambert's formula over a visible light piece, in FP64 from the piece's
+// float corners on the light plane (the exact term of soft_core.h:18-33).
+BT_HD double formFactorFP64(V3 x, V3 n, const V3* P, int count) {
+  double sum = 0;
+  for (int i = 0; i < count; ++i) {
+    V3 pa = P[i], pb = P[i + 1 == count ? 0 : i + 1];
+    double ax = double(pa.x) - double(x.x), ay = double(pa.y) - double(x.y), az = double(pa.z) - double(x.z);
+    double bx = double(pb.x) - double(x.x), by = double(pb.y) - double(x.y), bz = double(pb.z) - double(x.z);
+    double la = sqrt(ax * ax + ay * ay + az * az), lb = sqrt(bx * bx + by * by + bz * bz);
+    if (la == 0 || lb == 0) continue;
+    double c = (ax * bx + ay * by + az * bz) / (la * lb);
+    c = c < -1 ? -1 : (c > 1 ? 1 : c);
+    double theta = acos(c);
+    double gx = ay * bz - az * by, gy = az * bx - ax * bz, gz = ax * by - ay * bx;
+    double lg = sqrt(gx * gx + gy * gy + gz * gz);
+    if (lg == 0) continue;
+    sum += theta * (gx * double(n.x) + gy * double(n.y) + gz * double(n.z)) / lg;
+  }
+  return (sum < 0 ? -sum : sum) * 0.5;
+}
+
+}  // namespace btg

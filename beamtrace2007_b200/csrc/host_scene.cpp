@@ -1,0 +1,472 @@
+// Host side of the scene: triangle finalisation, the SAH kd-tree and the
+// camera, exported through the C-ABI (include/bt_gpu.h).
+//
+// The beam tracer's output depends on the kd-tree (cells are visited in tree
+// order) and on the per-triangle normals, so these reproduce the reference's
+// host code exactly: Scene::finalize (src/scene/scene.cpp:89-118),
+// KdTree::build with perfect splits and area-sorted leaves
+// (src/accel/kdtree.cpp:77-338) and Camera::make (src/render/render.cpp:14-25).
+// Compiled with -ffp-contract=off like the reference (CMakeLists.txt:21).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <vector>
+
+#include "bt_gpu.h"
+
+namespace {
+
+struct F3 {
+  float x, y, z;
+  float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+  float& operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+};
+F3 f3(float x, float y, float z) { return F3{x, y, z}; }
+F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+F3 operator*(F3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+F3 cross(F3 a, F3 b) { return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+F3 normalize(F3 a) {
+  float l = std::sqrt(dot(a, a));
+  return l > 0 ? f3(a.x / l, a.y / l, a.z / l) : a;
+}
+
+struct Aabb {
+  F3 lo{std::numeric_limits<float>::infinity(), std::numeric_limits<float>::infinity(),
+        std::numeric_limits<float>::infinity()};
+  F3 hi{-std::numeric_limits<float>::infinity(), -std::numeric_limits<float>::infinity(),
+        -std::numeric_limits<float>::infinity()};
+  void expand(F3 p) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = lo[a] < p[a] ? lo[a] : p[a];
+      hi[a] = hi[a] > p[a] ? hi[a] : p[a];
+    }
+  }
+  float surfaceArea() const {
+    F3 d = hi - lo;
+    return 2 * (d.x * d.y + d.y * d.z + d.z * d.x);
+  }
+};
+
+struct TriBox {
+  uint32_t tri;
+  Aabb b;
+};
+
+struct KdBuild {
+  const float* pos;
+  const uint32_t* tris;
+  const float* area;
+  float costTraverse, costIntersect, emptyBonus;
+  int binThreshold, bins;
+  bool clipBounds, singleLeaf;
+  int maxDepth;
+  std::vector<float> split;
+  std::vector<uint32_t> data, offset, triIndices;
+  int numLeaves = 0, maxDepthReached = 0;
+
+  F3 v(uint32_t t, int k) const {
+    const float* p = pos + 3 * size_t(tris[3 * size_t(t) + size_t(k)]);
+    return f3(p[0], p[1], p[2]);
+  }
+
+  // Bounds of triangle t clipped to `box` in double, rounded outward, never
+  // beyond `box` or `fallback` (clippedTriangleBounds, kdtree.cpp:77-134).
+  Aabb clipped(uint32_t t, const Aabb& box, const Aabb& fallback) const {
+    double poly[2][12][3];
+    int n = 3;
+    for (int k = 0; k < 3; ++k) {
+      F3 p = v(t, k);
+      poly[0][k][0] = p.x;
+      poly[0][k][1] = p.y;
+      poly[0][k][2] = p.z;
+    }
+    int cur = 0;
+    for (int axis = 0; axis < 3 && n > 0; ++axis) {
+      for (int side = 0; side < 2 && n > 0; ++side) {
+        double plane = side == 0 ? double(box.lo[axis]) : double(box.hi[axis]);
+        double sign = side == 0 ? 1.0 : -1.0;
+        int m = 0;
+        for (int i = 0; i < n; ++i) {
+          const double* a = poly[cur][i];
+          const double* b = poly[cur][(i + 1) % n];
+          double da = sign * (a[axis] - plane), db = sign * (b[axis] - plane);
+          if (da >= 0) {
+            for (int c = 0; c < 3; ++c) poly[1 - cur][m][c] = a[c];
+            ++m;
+          }
+          if ((da >= 0) != (db >= 0)) {
+            double tt = da / (da - db);
+            for (int c = 0; c < 3; ++c) poly[1 - cur][m][c] = a[c] + tt * (b[c] - a[c]);
+            poly[1 - cur][m][axis] = plane;
+            ++m;
+          }
+        }
+        n = m;
+        cur = 1 - cur;
+      }
+    }
+    if (n == 0) return fallback;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = std::min(lo[c], poly[cur][i][c]);
+        hi[c] = std::max(hi[c], poly[cur][i][c]);
+      }
+    Aabb r;
+    const double ulp = double(std::numeric_limits<float>::epsilon());
+    for (int c = 0; c < 3; ++c) {
+      double pad = 4 * ulp * (std::fabs(lo[c]) + std::fabs(hi[c]) + double(box.hi[c] - box.lo[c]));
+      r.lo[c] = float(lo[c] - pad);
+      r.hi[c] = float(hi[c] + pad);
+    }
+    for (int a = 0; a < 3; ++a) {
+      float blo = box.lo[a] > fallback.lo[a] ? box.lo[a] : fallback.lo[a];
+      float bhi = box.hi[a] < fallback.hi[a] ? box.hi[a] : fallback.hi[a];
+      r.lo[a] = r.lo[a] > blo ? r.lo[a] : blo;
+      r.hi[a] = r.hi[a] < bhi ? r.hi[a] : bhi;
+      if (r.lo[a] > r.hi[a]) r.lo[a] = r.hi[a];
+    }
+    return r;
+  }
+
+  float sahCost(const Aabb& box, int axis, float s, size_t nl, size_t nr) const {
+    Aabb l = box, r = box;
+    l.hi[axis] = s;
+    r.lo[axis] = s;
+    float inv = 1 / box.surfaceArea();
+    float cost = costTraverse + costIntersect * (l.surfaceArea() * inv * float(nl) + r.surfaceArea() * inv * float(nr));
+    if (nl == 0 || nr == 0) cost *= emptyBonus;
+    return cost;
+  }
+
+  // Binned SAH above binThreshold references, exact event sweep below
+  // (kdtree.cpp:215-285).
+  void findSplit(const std::vector<TriBox>& refs, const Aabb& box, int& bestAxis, float& bestSplit,
+                 float& bestCost) const {
+    const size_t N = refs.size();
+    if (!(box.surfaceArea() > 0)) return;
+    for (int axis = 0; axis < 3; ++axis) {
+      float lo = box.lo[axis], hi = box.hi[axis];
+      if (!(hi > lo)) continue;
+      if (N > size_t(binThreshold)) {
+        const int B = bins;
+        std::vector<size_t> starts(size_t(B), 0), ends(size_t(B), 0);
+        float scale = float(B) / (hi - lo);
+        for (const TriBox& r : refs) {
+          int bs = int((r.b.lo[axis] - lo) * scale);
+          int be = int((r.b.hi[axis] - lo) * scale);
+          bs = bs < 0 ? 0 : (bs > B - 1 ? B - 1 : bs);
+          be = be < 0 ? 0 : (be > B - 1 ? B - 1 : be);
+          starts[size_t(bs)]++;
+          ends[size_t(be)]++;
+        }
+        size_t nl = 0, nr = N;
+        for (int k = 1; k < B; ++k) {
+          nl += starts[size_t(k - 1)];
+          nr -= ends[size_t(k - 1)];
+          float s = lo + (hi - lo) * float(k) / float(B);
+          float c = sahCost(box, axis, s, nl, nr);
+          if (c < bestCost) {
+            bestCost = c;
+            bestAxis = axis;
+            bestSplit = s;
+          }
+        }
+      } else {
+        struct Ev {
+          float pos;
+          int type;  // 0 end, 1 planar, 2 start
+        };
+        std::vector<Ev> ev;
+        ev.reserve(2 * N);
+        for (const TriBox& r : refs) {
+          float a = r.b.lo[axis], b = r.b.hi[axis];
+          if (a == b) {
+            ev.push_back({a, 1});
+          } else {
+            ev.push_back({a, 2});
+            ev.push_back({b, 0});
+          }
+        }
+        std::sort(ev.begin(), ev.end(),
+                  [](const Ev& x, const Ev& y) { return x.pos != y.pos ? x.pos < y.pos : x.type < y.type; });
+        size_t nl = 0, nr = N;
+        for (size_t i = 0; i < ev.size();) {
+          float p = ev[i].pos;
+          size_t pe = 0, pp = 0, ps = 0;
+          while (i < ev.size() && ev[i].pos == p && ev[i].type == 0) {
+            ++pe;
+            ++i;
+          }
+          while (i < ev.size() && ev[i].pos == p && ev[i].type == 1) {
+            ++pp;
+            ++i;
+          }
+          while (i < ev.size() && ev[i].pos == p && ev[i].type == 2) {
+            ++ps;
+            ++i;
+          }
+          nr -= pe + pp;
+          if (p > lo && p < hi) {
+            float c = sahCost(box, axis, p, nl + pp, nr + pp);
+            if (c < bestCost) {
+              bestCost = c;
+              bestAxis = axis;
+              bestSplit = p;
+            }
+          }
+          nl += ps + pp;
+        }
+      }
+    }
+  }
+
+  void makeLeaf(size_t node, std::vector<TriBox>& refs) {
+    std::sort(refs.begin(), refs.end(), [&](const TriBox& a, const TriBox& b) {
+      float aa = area[a.tri], ab = area[b.tri];
+      return aa != ab ? aa > ab : a.tri < b.tri;
+    });
+    offset[node] = uint32_t(triIndices.size());
+    data[node] = (uint32_t(refs.size()) << 2) | 3u;
+    for (const TriBox& r : refs) triIndices.push_back(r.tri);
+    numLeaves++;
+  }
+
+  // Depth-first build: left subtree at node + 1, right child recorded in the
+  // node (kdtree.cpp:142-187).
+  void build(std::vector<TriBox>& refs, const Aabb& box, int depth) {
+    const size_t node = split.size();
+    split.push_back(0.f);
+    data.push_back(3u);
+    offset.push_back(0u);
+    maxDepthReached = std::max(maxDepthReached, depth);
+    const size_t N = refs.size();
+    int bestAxis = -1;
+    float bestSplit = 0, bestCost = std::numeric_limits<float>::infinity();
+    if (!singleLeaf && N > 1 && depth < maxDepth) findSplit(refs, box, bestAxis, bestSplit, bestCost);
+    const float leafCost = costIntersect * float(N);
+    if (bestAxis < 0 || !(bestCost < leafCost)) {
+      makeLeaf(node, refs);
+      return;
+    }
+    Aabb lbox = box, rbox = box;
+    lbox.hi[bestAxis] = bestSplit;
+    rbox.lo[bestAxis] = bestSplit;
+    std::vector<TriBox> left, right;
+    left.reserve(N / 2 + 1);
+    right.reserve(N / 2 + 1);
+    for (const TriBox& r : refs) {
+      float lo = r.b.lo[bestAxis], hi = r.b.hi[bestAxis];
+      bool planar = lo == hi && lo == bestSplit;
+      bool goLeft = planar || lo < bestSplit;
+      bool goRight = planar || hi > bestSplit;
+      if (!goLeft && !goRight) goLeft = goRight = true;
+      if (goLeft && goRight && !planar && clipBounds) {
+        left.push_back({r.tri, clipped(r.tri, lbox, r.b)});
+        right.push_back({r.tri, clipped(r.tri, rbox, r.b)});
+      } else {
+        if (goLeft) left.push_back(r);
+        if (goRight) right.push_back(r);
+      }
+    }
+    std::vector<TriBox>().swap(refs);
+    build(left, lbox, depth + 1);
+    std::vector<TriBox>().swap(left);
+    const size_t rightIndex = split.size();
+    build(right, rbox, depth + 1);
+    split[node] = bestSplit;
+    data[node] = (uint32_t(rightIndex) << 2) | uint32_t(bestAxis);
+  }
+};
+
+}  // namespace
+
+struct bt_kd_tree {
+  std::vector<float> split;
+  std::vector<uint32_t> data, offset, parent, triIndices;
+  std::vector<float> nodeBox;  // 6 per node: lo xyz, hi xyz
+  float bounds[6];
+  int numLeaves, maxDepth;
+};
+
+extern "C" {
+
+// Scene::finalize: drops degenerate triangles (tested in double), computes
+// unit normals, areas and bounds.  Returns the number of triangles kept.
+int64_t bt_scene_finalize(const float* pos, int64_t numVerts, const uint32_t* trisIn, int64_t numTrisIn,
+                          uint32_t* trisOut, float* triN, float* triArea, float* bounds) {
+  float lo[3] = {std::numeric_limits<float>::infinity(), std::numeric_limits<float>::infinity(),
+                 std::numeric_limits<float>::infinity()};
+  float hi[3] = {-lo[0], -lo[1], -lo[2]};
+  int64_t kept = 0;
+  for (int64_t i = 0; i < numTrisIn; ++i) {
+    const uint32_t* t = trisIn + 3 * i;
+    if (int64_t(t[0]) >= numVerts || int64_t(t[1]) >= numVerts || int64_t(t[2]) >= numVerts) return -1;
+    const float* a = pos + 3 * size_t(t[0]);
+    const float* b = pos + 3 * size_t(t[1]);
+    const float* c = pos + 3 * size_t(t[2]);
+    double e1x = double(b[0]) - a[0], e1y = double(b[1]) - a[1], e1z = double(b[2]) - a[2];
+    double e2x = double(c[0]) - a[0], e2y = double(c[1]) - a[1], e2z = double(c[2]) - a[2];
+    double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    double l = std::sqrt(nx * nx + ny * ny + nz * nz);
+    double scale = std::sqrt(e1x * e1x + e1y * e1y + e1z * e1z) * std::sqrt(e2x * e2x + e2y * e2y + e2z * e2z);
+    if (!(l > 1e-7 * scale) || t[0] == t[1] || t[1] == t[2] || t[0] == t[2]) continue;
+    for (int k = 0; k < 3; ++k) trisOut[3 * kept + k] = t[k];
+    triN[3 * kept] = float(nx / l);
+    triN[3 * kept + 1] = float(ny / l);
+    triN[3 * kept + 2] = float(nz / l);
+    triArea[kept] = float(0.5 * l);
+    for (const float* p : {a, b, c})
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = lo[k] < p[k] ? lo[k] : p[k];
+        hi[k] = hi[k] > p[k] ? hi[k] : p[k];
+      }
+    ++kept;
+  }
+  for (int k = 0; k < 3; ++k) {
+    bounds[k] = lo[k];
+    bounds[3 + k] = hi[k];
+  }
+  return kept;
+}
+
+int bt_kd_build(const float* pos, const uint32_t* tris, const float* triArea, int64_t numTris, const float* sceneBounds,
+                const bt_kd_params* params, bt_kd_tree** out) {
+  if (!out || !pos || !tris || !triArea || numTris < 0) return BT_ERR_INVALID;
+  bt_kd_params p;
+  if (params) {
+    p = *params;
+  } else {
+    bt_kd_params_default(&p);
+  }
+  KdBuild b;
+  b.pos = pos;
+  b.tris = tris;
+  b.area = triArea;
+  b.costTraverse = p.cost_traverse;
+  b.costIntersect = p.cost_intersect;
+  b.emptyBonus = p.empty_bonus;
+  b.binThreshold = p.bin_threshold;
+  b.bins = p.bins;
+  b.clipBounds = p.clip_bounds != 0;
+  b.singleLeaf = p.single_leaf != 0;
+  // Root box: scene bounds padded by 1e-4 of the diagonal + 1e-6 (kdtree.cpp:301-305).
+  Aabb root;
+  for (int a = 0; a < 3; ++a) {
+    root.lo[a] = sceneBounds[a];
+    root.hi[a] = sceneBounds[3 + a];
+  }
+  F3 pad = (root.hi - root.lo) * 1e-4f + f3(1e-6f, 1e-6f, 1e-6f);
+  root.lo = root.lo - pad;
+  root.hi = root.hi + pad;
+  std::vector<TriBox> refs(static_cast<size_t>(numTris));
+  for (int64_t t = 0; t < numTris; ++t) {
+    Aabb bb;
+    for (int k = 0; k < 3; ++k) bb.expand(b.v(uint32_t(t), k));
+    refs[size_t(t)] = {uint32_t(t), bb};
+  }
+  int N = numTris > 1 ? int(numTris) : 1;
+  b.maxDepth = p.max_depth >= 0 ? p.max_depth : int(8 + 1.3 * std::log2(double(N)));
+  b.maxDepth = std::min(b.maxDepth, 63);
+  try {
+    b.build(refs, root, 0);
+  } catch (const std::bad_alloc&) {
+    return BT_ERR_NOMEM;
+  }
+  bt_kd_tree* t = new (std::nothrow) bt_kd_tree();
+  if (!t) return BT_ERR_NOMEM;
+  const size_t nn = b.split.size();
+  t->split.swap(b.split);
+  t->data.swap(b.data);
+  t->offset.swap(b.offset);
+  t->triIndices.swap(b.triIndices);
+  t->numLeaves = b.numLeaves;
+  t->maxDepth = b.maxDepthReached;
+  for (int a = 0; a < 3; ++a) {
+    t->bounds[a] = root.lo[a];
+    t->bounds[3 + a] = root.hi[a];
+  }
+  // Parents and node boxes as a descent from the root computes them (kdtree.cpp:318-336).
+  t->parent.assign(nn, ~0u);
+  t->nodeBox.assign(6 * nn, 0.f);
+  for (int a = 0; a < 6; ++a) t->nodeBox[size_t(a)] = t->bounds[a];
+  std::vector<uint32_t> stack(1, 0u);
+  while (!stack.empty()) {
+    const uint32_t i = stack.back();
+    stack.pop_back();
+    const uint32_t d = t->data[i];
+    if ((d & 3u) == 3u) continue;
+    const int a = int(d & 3u);
+    const uint32_t l = i + 1, r = d >> 2;
+    for (int k = 0; k < 6; ++k) {
+      t->nodeBox[6 * size_t(l) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
+      t->nodeBox[6 * size_t(r) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
+    }
+    t->nodeBox[6 * size_t(l) + 3 + size_t(a)] = t->split[i];
+    t->nodeBox[6 * size_t(r) + size_t(a)] = t->split[i];
+    t->parent[l] = t->parent[r] = i;
+    stack.push_back(l);
+    stack.push_back(r);
+  }
+  *out = t;
+  return BT_OK;
+}
+
+void bt_kd_params_default(bt_kd_params* p) {
+  p->cost_traverse = 1.f;
+  p->cost_intersect = 0.4f;  // the beam setting of apps/bt_render.cpp:172
+  p->empty_bonus = 0.8f;
+  p->max_depth = -1;
+  p->bin_threshold = 2048;
+  p->bins = 64;
+  p->clip_bounds = 1;
+  p->single_leaf = 0;
+}
+
+void bt_kd_sizes(const bt_kd_tree* t, int64_t* numNodes, int64_t* numRefs, int32_t* numLeaves, int32_t* maxDepth) {
+  if (numNodes) *numNodes = int64_t(t->split.size());
+  if (numRefs) *numRefs = int64_t(t->triIndices.size());
+  if (numLeaves) *numLeaves = t->numLeaves;
+  if (maxDepth) *maxDepth = t->maxDepth;
+}
+
+void bt_kd_view(const bt_kd_tree* t, bt_kd_desc* d) {
+  d->split = t->split.data();
+  d->data = t->data.data();
+  d->offset = t->offset.data();
+  d->parent = t->parent.data();
+  d->node_box = t->nodeBox.data();
+  d->num_nodes = int64_t(t->split.size());
+  d->tri_indices = t->triIndices.data();
+  d->num_refs = int64_t(t->triIndices.size());
+  for (int a = 0; a < 6; ++a) d->bounds[a] = t->bounds[a];
+}
+
+void bt_kd_free(bt_kd_tree* t) { delete t; }
+
+// Camera::make: fwd, right, down and the half extents of the image plane at
+// distance 1.
+void bt_camera_make(const float* eye, const float* target, float fovY, const float* up, int32_t W, int32_t H,
+                    bt_camera* c) {
+  F3 e = f3(eye[0], eye[1], eye[2]), t = f3(target[0], target[1], target[2]), u = f3(up[0], up[1], up[2]);
+  F3 fwd = normalize(t - e);
+  F3 right = normalize(cross(fwd, u));
+  F3 down = cross(fwd, right);
+  for (int a = 0; a < 3; ++a) {
+    c->eye[a] = e[a];
+    c->fwd[a] = fwd[a];
+    c->right[a] = right[a];
+    c->down[a] = down[a];
+  }
+  c->W = W;
+  c->H = H;
+  c->half_h = float(std::tan(double(fovY) * M_PI / 360.0));
+  c->half_w = c->half_h * float(W) / float(H);
+}
+
+}  // extern "C"

@@ -1,0 +1,226 @@
+/* C-ABI of the B200 beam tracer (libbt_gpu.so).
+ *
+ * Plain C types only: host pointers and sizes, caller-owned buffers, int
+ * status codes (BT_OK = 0, negative = error; bt_gpu_last_error() describes
+ * the last failure on the calling thread).  No call aborts the process.
+ *
+ * The entry points replace the GPU port of joelsalzman/beamtrace2007:
+ *   bt_gpu_available        gpuAvailable            cuda/gpu_render.h:24
+ *   bt_gpu_create/destroy   GpuRenderer ctor/dtor   cuda/gpu_render.h:28-29,
+ *                                                   cuda/gpu_render.cu:489-541
+ *   bt_gpu_soft             GpuRenderer::softShadows  cuda/gpu_render.h:36
+ *   bt_gpu_soft_points      wfSoftShadows (shading points supplied)
+ *                                                   cuda/gpu_common.cuh:148-150
+ *   bt_gpu_primary          GpuRenderer::primary    cuda/gpu_render.h:41
+ *   bt_gpu_point            GpuRenderer::pointShadows cuda/gpu_render.h:45-46
+ *   bt_gpu_raster           rasterize (aa = 1)      src/render/render.h:29
+ * and the host-side preparation the GPU path needs:
+ *   bt_scene_finalize       Scene::finalize         src/scene/scene.cpp:89-118
+ *   bt_kd_build             KdTree::build           src/accel/kdtree.h:36
+ *   bt_camera_make          Camera::make            src/render/render_types.h:24
+ * Batching and serving (no counterpart in the reference): bt_gpu_batch_soft,
+ * bt_gpu_submit / bt_gpu_poll.
+ */
+#ifndef BT_GPU_H
+#define BT_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BT_API __attribute__((visibility("default")))
+#else
+#define BT_API
+#endif
+
+enum {
+  BT_OK = 0,
+  BT_ERR_INVALID = -1,     /* bad argument */
+  BT_ERR_CUDA = -2,        /* a CUDA call failed (message in bt_gpu_last_error) */
+  BT_ERR_NOMEM = -3,       /* host or device allocation failed */
+  BT_ERR_CAPACITY = -4,    /* a root needs more live sub-beams than the queues hold */
+  BT_ERR_TIMEOUT = -5,     /* the round limit was reached */
+  BT_ERR_NODEVICE = -6,    /* no usable CUDA device */
+  BT_ERR_BUSY = -7,        /* serving: no free slot / memory budget for the request */
+  BT_ERR_TOO_LARGE = -8    /* a size exceeds a fixed limit of the entry point */
+};
+
+/* Camera (render_types.h:15-39): image plane at distance 1 along fwd,
+ * q in [-half_w, half_w] x [-half_h, half_h], ray dir = fwd + right qx + down qy. */
+typedef struct {
+  float eye[3], fwd[3], right[3], down[3];
+  float half_w, half_h;
+  int32_t W, H;
+} bt_camera;
+
+/* Square/parallelogram area light (soft_core.h:10-14): centre and full edge
+ * vectors; emits along normalize(U x V). */
+typedef struct {
+  float c[3], U[3], V[3];
+} bt_area_light;
+
+/* Finalised scene (see bt_scene_finalize): vertex positions, triangles and
+ * unit normals; bounds = lo xyz, hi xyz of the triangles' vertices. */
+typedef struct {
+  const float* pos;
+  int64_t num_verts;
+  const uint32_t* tris;
+  const float* tri_normals;
+  int64_t num_tris;
+  float bounds[6];
+} bt_scene_desc;
+
+/* kd-tree in structure-of-arrays form (KdNode split/data/offset, parent
+ * links, node boxes lo xyz hi xyz, leaf triangle lists, root box). */
+typedef struct {
+  const float* split;
+  const uint32_t* data;
+  const uint32_t* offset;
+  const uint32_t* parent;
+  const float* node_box;
+  int64_t num_nodes;
+  const uint32_t* tri_indices;
+  int64_t num_refs;
+  float bounds[6];
+} bt_kd_desc;
+
+typedef struct {
+  float cost_traverse, cost_intersect, empty_bonus;
+  int32_t max_depth, bin_threshold, bins, clip_bounds, single_leaf;
+} bt_kd_params;
+
+typedef struct bt_kd_tree bt_kd_tree;
+
+typedef struct {
+  char name[256];
+  int32_t sm_count;
+  double mem_gb;
+  int32_t cc_major, cc_minor;
+} bt_gpu_info;
+
+/* Engine tunables (GpuRenderer public fields, gpu_render.h:50-58). */
+typedef struct {
+  int32_t device;           /* CUDA device ordinal */
+  int32_t budget;           /* live sub-beams per soft/point root before a retry (wfBudget) */
+  int32_t primary_budget;   /* live sub-beams per primary tile (wfPrimaryBudget) */
+  int64_t capacity;         /* sub-beam records per spill queue (wfCapacity); 0 = from free memory */
+  int32_t blocks_per_sm;    /* persistent CTAs per SM; 0 = occupancy */
+  int32_t split_batch;      /* lanes that must wait for a clip before a warp clips */
+  int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
+} bt_gpu_config;
+
+typedef struct {
+  int32_t exact;            /* Lambert's formula over the visible light (E) instead of eq. 2 */
+  float offset;             /* apex offset along the normal; <= 0: |scene diagonal| * 2e-5 */
+} bt_soft_opts;
+
+/* Counters (TraceStats, src/util/stats.h:8-42) and engine figures of the last call. */
+typedef struct {
+  uint64_t kd_steps, leaf_visits, tri_tests, hits, splits, beams, root_beams, presplit_beams, five_splits, climbs;
+  double dropped_area;
+  uint64_t eps_band_corners;  /* corner votes that fell inside the fuzzy band */
+  uint64_t eps_fp64_flips;    /* of those, votes whose FP64 re-evaluation lies outside the band */
+  double ms_primary, ms_trace, ms_total;
+  double ms_round;            /* summed device time of the persistent round kernels */
+  int32_t launches;           /* kernels launched by the call */
+  int32_t round_launches;     /* of those, persistent round kernels */
+  int32_t passes, retried_roots, max_spill;
+  int64_t roots;
+} bt_run_info;
+
+/* Beam cross-sections on a query plane (OutBeam, beam_types.h:68-73):
+ * x/y hold 4 corners per polygon (the last corner repeated when n = 3). */
+typedef struct {
+  float* x;
+  float* y;
+  int32_t* n;
+  int32_t* tri;
+  float* area;
+  int32_t* root;  /* index of the root (tile / hit beam) it came from; may be NULL */
+  int64_t cap;
+} bt_polys;
+
+typedef struct bt_gpu_ctx bt_gpu_ctx;
+
+BT_API const char* bt_gpu_last_error(void);
+BT_API void bt_gpu_config_default(bt_gpu_config* cfg);
+
+/* ---- host-side scene preparation ---- */
+BT_API int64_t bt_scene_finalize(const float* pos, int64_t num_verts, const uint32_t* tris_in, int64_t num_tris_in,
+                                 uint32_t* tris_out, float* tri_normals, float* tri_area, float* bounds);
+BT_API void bt_kd_params_default(bt_kd_params* p);
+BT_API int bt_kd_build(const float* pos, const uint32_t* tris, const float* tri_area, int64_t num_tris,
+                       const float* scene_bounds, const bt_kd_params* params, bt_kd_tree** out);
+BT_API void bt_kd_sizes(const bt_kd_tree* t, int64_t* num_nodes, int64_t* num_refs, int32_t* num_leaves,
+                        int32_t* max_depth);
+BT_API void bt_kd_view(const bt_kd_tree* t, bt_kd_desc* d);
+BT_API void bt_kd_free(bt_kd_tree* t);
+BT_API void bt_camera_make(const float* eye, const float* target, float fov_y, const float* up, int32_t W, int32_t H,
+                           bt_camera* cam);
+
+/* ---- device ---- */
+BT_API int bt_gpu_available(bt_gpu_info* info);
+BT_API int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu_config* cfg,
+                         bt_gpu_ctx** out);
+BT_API int bt_gpu_destroy(bt_gpu_ctx* ctx);
+
+/* Exact soft shadows of a W x H image: GPU primary rays (tri, shading point,
+ * normal per pixel centre), then one shadow-beam root per covered pixel.
+ * Outputs (host, W*H each, any may be NULL): tri (-1 background), vis
+ * (visible light fraction; -1 background, 0 below the horizon), E
+ * (exact: Lambert integral over the visible light; else A*G0*V), Eu (A*G0). */
+BT_API int bt_gpu_soft(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_area_light* light, const bt_soft_opts* opts,
+                       int32_t* tri, float* vis, float* E, float* Eu, bt_run_info* info);
+
+/* Soft shadows for n supplied shading points (host arrays: tri[n], X[3n],
+ * N[3n]; tri < 0 = nothing to shade). */
+BT_API int bt_gpu_soft_points(bt_gpu_ctx* ctx, const bt_area_light* light, const bt_soft_opts* opts, int64_t n,
+                              const int32_t* tri, const float* X, const float* N, float* vis, float* E, float* Eu,
+                              bt_run_info* info);
+
+/* The same on device-resident buffers (device pointers; the caller's
+ * stream is the legacy default stream).  For benchmarks and batching. */
+BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light, const bt_soft_opts* opts, int64_t n,
+                                     const int32_t* d_tri, const float* d_X, const float* d_N, float* d_vis,
+                                     float* d_E, float* d_Eu, bt_run_info* info);
+
+/* bt_gpu_soft on device buffers (W*H each; d_vis/d_E/d_Eu may be NULL):
+ * everything stays in device memory.  Runs on the context's stream and
+ * returns when the results are complete. */
+BT_API int bt_gpu_soft_device(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_area_light* light,
+                              const bt_soft_opts* opts, int32_t* d_tri, float* d_vis, float* d_E, float* d_Eu,
+                              bt_run_info* info);
+
+/* GPU primary rays only (primaryKernel, cuda/gpu_render.cu:222-244): per
+ * pixel centre the nearest triangle (-1 none), hit point X (3 floats) and
+ * normal N facing the eye.  Host buffers (_device: device buffers). */
+BT_API int bt_gpu_primary_rays(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t* tri, float* X, float* N);
+BT_API int bt_gpu_primary_rays_device(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t* d_tri, float* d_X, float* d_N);
+
+/* Primary visibility, one root per tile x tile pixels: the visible
+ * polygons (image plane) in `out`; *count = number produced (may exceed
+ * out->cap: then only cap were written and the call should be repeated
+ * with a larger buffer). */
+BT_API int bt_gpu_primary(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, int32_t tile, bt_polys* out,
+                          int64_t* count, bt_run_info* info);
+
+/* Point-light shadows for `hits` (primary hit polygons, image plane), one
+ * root per polygon: the shadowed image-plane polygons are written to out
+ * (root = index into hits). */
+BT_API int bt_gpu_point(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_polys* hits, int64_t num_hits,
+                        const float* light, bt_polys* out, int64_t* count, bt_run_info* info);
+
+/* Rasterises polygons at pixel centres (rasterize, render.cpp:49-95, aa = 1)
+ * on the GPU: prim polygons write tri ids (-1 elsewhere), shadow polygons
+ * set flag = 1.  tri and flag are host buffers of W*H. */
+BT_API int bt_gpu_raster(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_polys* prim, int64_t num_prim,
+                         const bt_polys* shadow, int64_t num_shadow, int32_t* tri, uint8_t* flag);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BT_GPU_H */
