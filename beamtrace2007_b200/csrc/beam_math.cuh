@@ -17,11 +17,19 @@
 
 #include <cmath>
 
+// BT_HD: small helpers, always inlined.  BT_COLD: clipping, pre-split,
+// set-up and output paths, kept out of line as one copy each: the hot
+// traversal loop then fits the instruction caches (inlining everything made
+// instruction fetch the dominant stall).
 #if defined(__CUDACC__)
 #define BT_HD __host__ __device__ __forceinline__
+#define BT_COLD __host__ __device__ __noinline__
 #else
 #define BT_HD inline
+#define BT_COLD __attribute__((noinline))
 #endif
+
+constexpr int kPolyMax = 8;  // vertices of a clip polygon (kMaxPoly, beam_geom.h:12)
 
 namespace btg {
 
@@ -176,7 +184,7 @@ BT_HD Line makeLine(float a, float b, float c, float ext) {
 // Fuzzy split of convex p by L; crossings computed from the
 // lexicographically smaller endpoint (beam_geom.h:83-114).
 template <int N>
-BT_HD bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out) {
+BT_COLD bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out) {
   in.clear();
   out.clear();
   float d[N];
@@ -212,7 +220,7 @@ BT_HD bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Po
 // Welds duplicate / collinear vertices within 1e-3 of the split epsilon
 // (beam_geom.h:122-150); n = 0 if the polygon collapses.
 template <int N>
-BT_HD void cleanPoly(Poly<N>& p, float epsSplit) {
+BT_COLD void cleanPoly(Poly<N>& p, float epsSplit) {
   const float eps = epsSplit * 1e-3f;
   bool changed = true;
   while (changed && p.n >= 3) {
@@ -354,7 +362,7 @@ BT_HD void beamCorners(const Poly<N>& c, Beam& b) {
 // Cleaned corners and axes of a piece; false (and `dropped` = |area|) for
 // slivers below minArea (BeamCtx::beamGeom, beam_core.h:200-221).
 template <int N>
-BT_HD bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped) {
+BT_COLD bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped) {
   Poly<N> c = p;
   cleanPoly(c, q.eps);
   float A = c.n >= 3 ? c.area() : 0.f;
@@ -571,7 +579,7 @@ BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, in
 // The cheap beam-triangle tests: trivial cases, depth line, far plane
 // (BeamCtx::classifyTri, beam_core.h:374-409).  The current hit's plane
 // comes from the beam (hitA, hitC, hitN).
-BT_HD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl) {
+BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl) {
   nl = 0;
   bool allIn = true;
   for (int k = 0; k < 3; ++k)
@@ -592,7 +600,7 @@ BT_HD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L,
 // outside some line go to sink.push(0, p), pieces inside every line to
 // sink.push(1, p) (BeamCtx::clipTri with orderEdges, beam_core.h:420-479).
 template <int N, class Sink>
-BT_HD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink, uint32_t& fiveSplits) {
+BT_COLD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink, uint32_t& fiveSplits) {
   {
     float score[3];
     for (int k = 0; k < 3; ++k) {
@@ -668,7 +676,7 @@ BT_HD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink, u
 // beam_core.h:488-546).  emit.piece(poly, negBits) per piece (false aborts),
 // emit.presplit() per extra split, emit.dropped(area) per sign-line sliver.
 template <class Emit>
-BT_HD bool presplit(const Query& q, const Poly<8>& root, Emit& emit) {
+BT_COLD bool presplit(const Query& q, const Poly<8>& root, Emit& emit) {
   struct Item {
     Poly<8> p;
     int axis;
@@ -735,7 +743,7 @@ BT_HD bool presplit(const Query& q, const Poly<8>& root, Emit& emit) {
 
 // Light-quad shadow beam from shading point x (normal ns), clipped by the
 // horizon (lightBeamSetup, src/render/soft_core.h:38-73).
-BT_HD bool lightBeamSetup(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns, int tri, float offset, Query& q, Poly<8>& root,
+BT_COLD bool lightBeamSetup(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns, int tri, float offset, Query& q, Poly<8>& root,
                           float& lightArea) {
   V3 nL = normalize(cross(LU, LV));
   if (!(dot(sub(x, Lc), nL) > 0)) return false;
@@ -773,7 +781,7 @@ BT_HD bool lightBeamSetup(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns, int tri, float offse
 }
 
 // Light-centre geometry term of eq. 2 (lightCenterG, soft_core.h:76-84).
-BT_HD float lightCenterG(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns) {
+BT_COLD float lightCenterG(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns) {
   V3 nL = normalize(cross(LU, LV));
   if (!(dot(sub(x, Lc), nL) > 0)) return 0;
   V3 w = sub(Lc, x);
@@ -786,7 +794,7 @@ BT_HD float lightCenterG(V3 Lc, V3 LU, V3 LV, V3 x, V3 ns) {
 // Shadow beam of a primary hit beam: corners back-projected onto the
 // receiver plane, traced from the light (pointShadowSetup,
 // src/render/point_core.h:15-36).  `cam` holds eye, fwd, right, down.
-BT_HD bool pointShadowSetup(V3 eye, V3 fwd, V3 right, V3 down, V3 nT, V3 P0, int T, V3 light, const float* px,
+BT_COLD bool pointShadowSetup(V3 eye, V3 fwd, V3 right, V3 down, V3 nT, V3 P0, int T, V3 light, const float* px,
                             const float* py, int n, Query& q, Poly<8>& root) {
   float sideCam = dot(nT, sub(eye, P0)), sideL = dot(nT, sub(light, P0));
   if (!(sideCam * sideL > 0)) return false;
@@ -809,7 +817,7 @@ BT_HD bool pointShadowSetup(V3 eye, V3 fwd, V3 right, V3 down, V3 nT, V3 P0, int
 
 // Occluded piece back to the image plane, counter-clockwise
 // (pointShadowToImage, point_core.h:41-64).
-BT_HD bool pointShadowToImage(const Plane& camPlane, const Plane& shadowPlane, const float* sx, const float* sy, int n,
+BT_COLD bool pointShadowToImage(const Plane& camPlane, const Plane& shadowPlane, const float* sx, const float* sy, int n,
                               float* ox, float* oy) {
   for (int i = 0; i < n; ++i)
     if (!planeProject(camPlane, planePoint(shadowPlane, sx[i], sy[i]), ox[i], oy[i])) return false;

@@ -1,25 +1,22 @@
 // The B200 beam engine: persistent warps over sub-beam records, and the
 // C-ABI entry points (include/bt_gpu.h).
 //
-// Work hierarchy, innermost first:
-//   lane registers   one sub-beam per lane, traced leaf by leaf;
-//   warp stack       a LIFO of records in shared memory (kStack per warp):
-//                    pieces of a clip and of a root's pre-split stay with the
-//                    warp that made them, so a beam tree is traced depth-first
-//                    by one warp with its kd cells hot in L1;
-//   spill queues     two global queues of 64-byte records; a warp whose stack
-//                    is full appends to the "next" queue, which the following
-//                    launch consumes.
-// A launch ("round") admits new roots as lanes fall idle, as long as their
-// budget of live sub-beams fits in the free queue slots, so the spill queue
-// can never overflow.  A root that would exceed its budget is abandoned and
-// traced again, on the GPU, in a retry pass with a 16x budget (the reference
-// recomputed such roots on the CPU, cuda/gpu_render.cu:651-672).
+// Sub-beams are 64-byte self-contained records in two global queues.  Each
+// launch ("round") is a persistent grid that drains the current queue: a lane
+// takes a record, traces it leaf by leaf until it finishes or a triangle
+// needs a clip, and takes the next record as soon as it is free (one atomic
+// per warp for all idle lanes, ballot/popc compaction).  When the queue is
+// empty, idle lanes admit new roots.  Lanes that need a clip park until
+// `split_batch` lanes of the warp wait (or no lane can trace), then clip
+// together, so tracing and clipping each run with most lanes converged; the
+// pieces of a clip go to the next round's queue in consecutive slots taken
+// with one atomic (siblings stay adjacent).  Every warp works on every root,
+// so no lane starves while work exists anywhere on the GPU.
 //
-// Lanes that need a clip park until `split_batch` lanes of the warp wait (or
-// no lane can trace), then clip together: trace and clip each run with most
-// lanes converged.  Both phases work on the same per-lane record, so a lane
-// never holds two beams in registers.
+// Memory is bounded without waiting: a root is admitted only if `budget`
+// queue slots are free for it, and a root that would exceed its budget is
+// abandoned and traced again, on the GPU, in a retry pass with a 16x budget
+// (the reference recomputed such roots on the CPU, cuda/gpu_render.cu:651-672).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,7 +56,6 @@ void setErr(const char* fmt, ...) {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;
 constexpr int kThreads = 32 * kWarps;
-constexpr int kStack = 40;
 constexpr double kFixVis = 1099511627776.0;         // 2^40: visible fraction, fixed point
 constexpr double kFixG = 1152921504606846976.0;     // 2^60: Lambert integral, fixed point
 constexpr int kMaxLaunches = 20000;  // launches per call before BT_ERR_TIMEOUT
@@ -241,16 +237,26 @@ __device__ void outputPiece(const RoundParams& p, const Query& q, float lightAre
   }
 }
 
-// Per-lane environment for admission and clip emission: the first queued
-// piece stays in the lane, the rest go to the warp stack (or spill).
+// Appends one record to the next round's queue (admission pieces).
+__device__ bool pushNext(const RoundParams& p, const SubBeam& r) {
+  const int nxt = p.cur ^ 1;
+  const int g = atomicAdd(&p.ctr->count[nxt], 1);
+  if (g < p.capacity) {
+    p.q[nxt][g] = r;
+    return true;
+  }
+  atomicExch(&p.ctr->overflow, 1);
+  return false;
+}
+
+// Admission: the root's first piece stays in the lane, the others go to the
+// next round's queue.
 template <int App>
-struct LaneEnv {
+struct AdmitEnv {
   const RoundParams* p;
   const Query* q;
   float lightArea;
   int root;
-  SubBeam* stack;
-  int* top;
   Stats* st;
   SubBeam first;
   int haveFirst;
@@ -262,19 +268,29 @@ struct LaneEnv {
       haveFirst = 1;
       return true;
     }
-    const int slot = atomicAdd(top, 1);
-    if (slot < kStack) {
-      stack[slot] = r;
-      return true;
-    }
-    const int nxt = p->cur ^ 1;
-    const int g = atomicAdd(&p->ctr->count[nxt], 1);
-    if (g < p->capacity) {
-      p->q[nxt][g] = r;
-      return true;
-    }
-    atomicExch(&p->ctr->overflow, 1);
-    return false;
+    return pushNext(*p, r);
+  }
+  __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
+  __device__ void missed(const Beam& b) { outputPiece<App>(*p, *q, lightArea, root, b, -1, *st); }
+  __device__ void dropped(float) {}
+};
+
+// Clip emission into `slots` consecutive slots of the next round's queue
+// reserved by one atomic; pieces dropped as slivers leave holes (n = 0) that
+// the next round skips, as the reference's split does
+// (wfSplitEmit, wavefront_core.h:367-422).
+template <int App>
+struct SplitEnv {
+  const RoundParams* p;
+  const Query* q;
+  float lightArea;
+  int root;
+  Stats* st;
+  SubBeam* dst;
+  int written;
+  __device__ bool queue(const SubBeam& r) {
+    dst[written++] = r;
+    return true;
   }
   __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
   __device__ void missed(const Beam& b) { outputPiece<App>(*p, *q, lightArea, root, b, -1, *st); }
@@ -296,8 +312,7 @@ __device__ __forceinline__ bool softPixel(const AppParams& a, int k, int& pix) {
 // Sets up root k and queues its pre-split pieces (admitRoot,
 // cuda/wavefront.cu:255-325).  Returns true if the lane took a piece.
 template <int App>
-__device__ bool admit(const RoundParams& p, int k, SubBeam* stack, int* top, Stats& st, SubBeam& first, Query& q,
-                      float& lightArea) {
+__device__ bool admit(const RoundParams& p, int k, Stats& st, SubBeam& first, Query& q, float& lightArea) {
   p.live[k] = 0;
   p.state[k] = kRootNone;
   const int att = p.attempt[k] + 1;
@@ -375,7 +390,7 @@ __device__ bool admit(const RoundParams& p, int k, SubBeam* stack, int* top, Sta
   querySetup(q, poly.extent());
   storeRoot(&p.roots[k], q, lightArea, att);
   p.state[k] = kRootTraced;
-  LaneEnv<App> env{&p, &q, lightArea, k, stack, top, &st, SubBeam(), 0, 0};
+  AdmitEnv<App> env{&p, &q, lightArea, k, &st, SubBeam(), 0, 0};
   const bool ok = admitRoot(p.s, q, poly, k, env, st);
   p.live[k] = env.queued;
   if (!ok || env.queued > p.budget) killRoot(p, k);
@@ -400,19 +415,19 @@ __device__ void flushStats(const RoundParams& p, const Stats& st) {
   if (laneId() == 0 && d != 0) atomicAdd(reinterpret_cast<double*>(&p.stats[kStDropped]), d);
 }
 
+// One round: every record of the current queue, then new roots, is traced
+// until it finishes or needs a clip; clips run warp-batched; all pieces go to
+// the next round's queue.  Lanes are refilled from the shared queue as soon
+// as they fall idle, so every warp works on every root.
 template <int App>
 __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
-  __shared__ SubBeam sStack[kWarps][kStack];
-  __shared__ int sTop[kWarps];
-  const int lane = laneId(), wid = threadIdx.x >> 5;
+  const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
-  SubBeam* stack = sStack[wid];
-  int* top = &sTop[wid];
-  if (lane == 0) *top = 0;
-  __syncwarp();
   const int nCur = min(p.ctr->count[p.cur], p.capacity);
   const SubBeam* qCur = p.q[p.cur];
+  const int nxt = p.cur ^ 1;
   bool queueDone = nCur == 0, rootsDone = false;
+  int admitWait = 0, blockedSleeps = 0;
   int phase = kIdle;
   SubBeam r;
   Beam b;
@@ -423,67 +438,71 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
   Stats st;
   st.clear();
   for (;;) {
-    // ---- refill idle lanes: warp stack, then spill queue, then new roots
+    // ---- refill idle lanes: the round's queue, then new roots
     unsigned idle = __ballot_sync(kFull, phase == kIdle);
-    if (idle) {
-      const int t0 = *top;
-      const int take = min(__popc(idle), t0);
-      const int rank = __popc(idle & ltMask);
-      if (phase == kIdle && rank < take) {
-        r = stack[t0 - 1 - rank];
+    if (idle && !queueDone) {
+      const int ni = __popc(idle);
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&p.ctr->head, ni);
+      base = __shfl_sync(kFull, base, 0);
+      if (base + ni >= nCur) queueDone = true;
+      const int i = base + __popc(idle & ltMask);
+      if (phase == kIdle && i < nCur) {
+        r = qCur[i];
         phase = kLoaded;
       }
-      __syncwarp();
-      if (lane == 0) *top = t0 - take;
-      __syncwarp();
       idle = __ballot_sync(kFull, phase == kIdle);
-      if (idle && !queueDone) {
-        const int ni = __popc(idle);
-        int base = 0;
-        if (lane == 0) base = atomicAdd(&p.ctr->head, ni);
-        base = __shfl_sync(kFull, base, 0);
-        if (base + ni >= nCur) queueDone = true;
-        const int i = base + __popc(idle & ltMask);
-        if (phase == kIdle && i < nCur) {
-          r = qCur[i];
-          phase = kLoaded;
+    }
+    if (idle && !rootsDone && admitWait > 0) {
+      --admitWait;
+    } else if (idle && !rootsDone) {
+      // Reserve `budget` queue slots for each root taken; take only as many
+      // roots as fit in the free slots.
+      const int ni = __popc(idle);
+      int base = -1, fit = 0;
+      if (lane == 0) {
+        const unsigned long long bud = (unsigned long long)p.budget, cap = (unsigned long long)p.capacity;
+        const unsigned long long need = (unsigned long long)ni * bud;
+        const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
+        fit = ni;
+        if (old + need > cap) {
+          fit = old >= cap ? 0 : int(min((unsigned long long)ni, (cap - old) / bud));
+          atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - fit)) * bud);
         }
-        idle = __ballot_sync(kFull, phase == kIdle);
+        if (fit > 0) {
+          base = atomicAdd(&p.ctr->rootNext, fit);
+          const int got = max(0, min(fit, p.numRoots - base));
+          if (got < fit) atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(fit - got)) * bud);
+          if (got > 0) atomicAdd(&p.ctr->inflight, got);
+        }
       }
-      if (idle && !rootsDone) {
-        const int ni = __popc(idle);
-        int base = -1;
-        if (lane == 0) {
-          const unsigned long long need = (unsigned long long)ni * (unsigned long long)p.budget;
-          const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
-          if (old + need > (unsigned long long)p.capacity) {
-            atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)need));
-          } else {
-            base = atomicAdd(&p.ctr->rootNext, ni);
-            const int got = max(0, min(ni, p.numRoots - base));
-            if (got < ni)
-              atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - got)) * (unsigned long long)p.budget);
-            if (got > 0) atomicAdd(&p.ctr->inflight, got);
-          }
+      base = __shfl_sync(kFull, base, 0);
+      fit = __shfl_sync(kFull, fit, 0);
+      if (fit == 0) {
+        // No free slots: roots in flight must finish first.  A warp with
+        // work carries on and retries later; an idle warp sleeps a bounded
+        // number of times, then leaves the rest to the next round.
+        admitWait = 8;
+        if (__popc(idle) == 32 && queueDone) {
+          if (++blockedSleeps > 64) rootsDone = true;
+          __nanosleep(2000);
         }
-        base = __shfl_sync(kFull, base, 0);
-        if (base < 0 || base + ni >= p.numRoots) rootsDone = true;
-        const int j = base + __popc(idle & ltMask);
-        if (base >= 0 && phase == kIdle && j < p.numRoots) {
-          const int k = p.rootList ? p.rootList[j] : j;
-          if (admit<App>(p, k, stack, top, st, r, q, lightArea)) {
-            qRoot = k;
-            phase = kLoaded;
-          } else {
-            qRoot = -1;
-          }
+      } else if (base + fit >= p.numRoots) {
+        rootsDone = true;
+      }
+      const int rank = __popc(idle & ltMask);
+      const int j = base + rank;
+      if (fit > 0 && rank < fit && phase == kIdle && j < p.numRoots) {
+        const int k = p.rootList ? p.rootList[j] : j;
+        if (admit<App>(p, k, st, r, q, lightArea)) {
+          qRoot = k;
+          phase = kLoaded;
+        } else {
+          qRoot = -1;
         }
-        __syncwarp();
-        if (lane == 0 && *top > kStack) *top = kStack;
       }
     }
-    __syncwarp();
-    // ---- expand newly loaded records
+    // ---- expand newly loaded records (holes and abandoned roots are dropped)
     if (phase == kLoaded) {
       if (r.n == 0 || p.state[r.root] == kRootKilled) {
         liveSub(p, r.root, 1);
@@ -502,7 +521,7 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
     const unsigned sp = __ballot_sync(kFull, phase == kSplit);
     const unsigned idleNow = __ballot_sync(kFull, phase == kIdle);
     if (!tr && !sp) {
-      if (queueDone && rootsDone && *top == 0) break;
+      if (queueDone && rootsDone) break;
       continue;
     }
     const bool doSplit = sp && (__popc(sp) >= p.splitBatch || !tr || idleNow);
@@ -512,40 +531,39 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
         Line L[5];
         int nl = 0;
         bool commit = false;
-        const int slots = splitPass1<LaneEnv<App>>(p.s, q, r, b, st, ti, L, nl, commit);
+        const int slots = splitPass1<SplitEnv<App>>(p.s, q, r, b, st, ti, L, nl, commit);
+        const int root = r.root;
         if (slots < 0) {
-          killRoot(p, r.root);
-          liveSub(p, r.root, 1);
+          killRoot(p, root);
+          liveSub(p, root, 1);
           phase = kIdle;
         } else if (!commit) {
-          r.cursor += 1;
+          r.cursor += 1;  // nothing measurable changes: continue at the next triangle
           w.phase = kPhTest;
           phase = kTrace;
         } else {
-          const int root = r.root;
           const int old = atomicAdd(&p.live[root], slots - 1);
           if (old + slots - 1 > p.budget) {
             killRoot(p, root);
             liveSub(p, root, slots);
-            phase = kIdle;
           } else {
-            LaneEnv<App> env{&p, &q, lightArea, root, stack, top, &st, SubBeam(), 0, 0};
-            splitPass2(q, r, b, ti, L, nl, env, st);
-            if (env.queued < slots) liveSub(p, root, slots - env.queued);
-            if (env.haveFirst) {
-              r = env.first;
-              expand(p.s, q, r, b);
-              walkBegin(p.s, r, w);
-              phase = kTrace;
+            if (old + slots - 1 == 0) rootDone(p);  // every piece occluded: the root is finished
+            const int base = slots > 0 ? atomicAdd(&p.ctr->count[nxt], slots) : 0;
+            if (base + slots > p.capacity) {
+              atomicExch(&p.ctr->overflow, 1);
             } else {
-              phase = kIdle;
+              SplitEnv<App> env{&p, &q, lightArea, root, &st, p.q[nxt] + base, 0};
+              splitPass2(q, r, b, ti, L, nl, env, st);
+              for (int k = env.written; k < slots; ++k) {
+                SubBeam hole = r;
+                hole.n = 0;
+                p.q[nxt][base + k] = hole;
+              }
             }
           }
+          phase = kIdle;
         }
       }
-      __syncwarp();
-      if (lane == 0 && *top > kStack) *top = kStack;
-      __syncwarp();
     } else if (phase == kTrace) {
       // one leaf: climb / descend to it, then test its triangles
       int res = advance(p.s, q, b, r, w, st);
@@ -570,6 +588,15 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
 
 // Between launches: the consumed queue is emptied, completion is decided
 // (scheduleKernel's bookkeeping, cuda/wavefront.cu:327-345).
+// Start of a retry pass: per-pass state is cleared; output counts and the
+// spill high-water mark of the call are kept.
+__global__ void passResetKernel(Counters* c) {
+  c->count[0] = c->count[1] = 0;
+  c->head = c->rootNext = c->inflight = c->killed = 0;
+  c->reserved = 0;
+  c->overflow = c->done = 0;
+}
+
 __global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
   const int nxt = cur ^ 1;
   if (c->count[nxt] > c->maxSpill) c->maxSpill = c->count[nxt];
@@ -999,6 +1026,8 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.splitBatch = std::max(1, std::min(32, c->cfg.split_batch));
   p.app = app;
   const int grid = gridFor<App>(c);
+  // BT_ROUND_LOG=1: one line per round on stderr (diagnostics).
+  FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
   int launches = 0, passes = 0, retried = 0;
   const int32_t* list = nullptr;
   int n = R;
@@ -1012,7 +1041,12 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     }
     p.numRoots = n;
     p.rootList = list;
-    CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
+    if (pass == 0) {
+      CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
+    } else {
+      passResetKernel<<<1, 1, 0, c->stream>>>(c->dCtr);
+      launches++;
+    }
     ++passes;
     for (int cur = 0;; cur ^= 1) {
       p.cur = cur;
@@ -1024,12 +1058,15 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
+      float roundMs = 0;
+      cudaEventElapsedTime(&roundMs, c->rev[0], c->rev[1]);
       if (info) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
-        info->ms_round += ms;
+        info->ms_round += roundMs;
         info->round_launches++;
       }
+      if (roundLog)
+        fprintf(roundLog, "pass %d round %d produced %d inflight %d rootNext %d ms %.3f\n", pass, launches / 2,
+                hc.count[cur ^ 1], hc.inflight, hc.rootNext, roundMs);
       if (hc.overflow) {
         setErr("spill queue overflow (capacity %d)", c->capacity);
         return BT_ERR_CAPACITY;

@@ -273,7 +273,7 @@ BT_HD bool moreInLeaf(const SceneDev& s, const Query& q, SubBeam& r) {
   return i < cnt;
 }
 
-BT_HD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
+BT_COLD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
   TriRec t = loadRef(s, k);
   triSetup(q, t.v0, t.v1, t.v2, t.n, t.vi, t.tri, ti);
 }
@@ -319,8 +319,7 @@ BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats&
 struct AreaSink {
   float newArea;
   int slots0, slots1;
-  template <int N>
-  BT_HD bool push(int l, const Poly<N>& p) {
+  BT_HD bool push(int l, const Poly<kPolyMax>& p) {
     if (p.n > 5) return false;
     if (l == 1)
       newArea += p.area();
@@ -347,18 +346,17 @@ struct EmitSink {
   int t;
   Env* env;
   Stats* st;
-  template <int N>
-  BT_HD bool push(int l, const Poly<N>& p0) {
+  BT_HD bool push(int l, const Poly<kPolyMax>& p0) {
     const bool hitNow = l == 1;
     const bool queued = !(hitNow && q->mode == kModeAnyHit);
-    Poly<5> sub[2];
+    Poly<kPolyMax> sub[2];
     int ns = 1;
     if (p0.n == 5) {
       splitFive(p0, sub[0], sub[1]);
       st->fiveSplits++;
       ns = 2;
     } else {
-      sub[0].copyFrom(p0);
+      sub[0] = p0;
     }
     for (int j = 0; j < ns; ++j) {
       Beam nb;
@@ -381,6 +379,15 @@ struct EmitSink {
   }
 };
 
+// One clipper instance per environment: measure (pass 1) or emit (pass 2).
+template <class Env>
+struct ClipSink {
+  int emitting;
+  AreaSink area;
+  EmitSink<Env> emit;
+  BT_HD bool push(int l, const Poly<kPolyMax>& p) { return emitting ? emit.push(l, p) : area.push(l, p); }
+};
+
 // Clip of a record whose pending triangle needs it (after testOne returned
 // kStepSplit).  Pass 1 decides whether any piece measurably changes status
 // and counts queue slots; pass 2 (only if it does) replays the same clip and
@@ -388,31 +395,35 @@ struct EmitSink {
 // lists (the root must be abandoned), else the slots pass 2 will use
 // (0 if nothing changes: the record continues unchanged at cursor + 1).
 template <class Env>
-BT_HD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
-                     Line* L, int& nl, bool& commit) {
+BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
+                       Line* L, int& nl, bool& commit) {
   const uint2 leaf = s.node[r.node];
   setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
   classifyTri(q, B, ti, L, nl);
   Line Lc[5];
   for (int i = 0; i < nl; ++i) Lc[i] = L[i];
-  AreaSink a{0.f, 0, 0};
+  ClipSink<Env> sink;
+  sink.emitting = 0;
+  sink.area = AreaSink{0.f, 0, 0};
   uint32_t five = 0;
-  if (!clipTri<6>(q, B, Lc, nl, a, five)) return -1;
+  if (!clipTri<kPolyMax>(q, B, Lc, nl, sink, five)) return -1;
   st.fiveSplits += five;
-  commit = a.newArea >= q.minArea;
+  commit = sink.area.newArea >= q.minArea;
   if (!commit) return 0;
-  return a.slots0 + (q.mode == kModeAnyHit ? 0 : a.slots1);
+  return sink.area.slots0 + (q.mode == kModeAnyHit ? 0 : sink.area.slots1);
 }
 
 template <class Env>
-BT_HD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
-                      Stats& st) {
+BT_COLD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
+                        Stats& st) {
   st.splits++;
   SubBeam base = r;
   base.cursor = r.cursor + 1;
-  EmitSink<Env> sink{&q, &base, &B, ti.tri, &env, &st};
+  ClipSink<Env> sink;
+  sink.emitting = 1;
+  sink.emit = EmitSink<Env>{&q, &base, &B, ti.tri, &env, &st};
   uint32_t five = 0;  // counted in pass 1
-  clipTri<6>(q, B, L, nl, sink, five);
+  clipTri<kPolyMax>(q, B, L, nl, sink, five);
 }
 
 // Root admission: pre-split pieces become records at the kd root; pieces
@@ -459,7 +470,7 @@ struct AdmitEmit {
 };
 
 template <class Env>
-BT_HD bool admitRoot(const SceneDev& s, const Query& q, const Poly<8>& rootPoly, int root, Env& env, Stats& st) {
+BT_COLD bool admitRoot(const SceneDev& s, const Query& q, const Poly<8>& rootPoly, int root, Env& env, Stats& st) {
   Poly<8> p = rootPoly;
   if (p.n < 3) return true;
   if (p.area() < 0) p.reverse();
@@ -479,7 +490,7 @@ BT_HD float beamPoly(const Beam& b, Poly<4>& p) {
 
 // Lambert's formula over a visible light piece, in FP64 from the piece's
 // float corners on the light plane (the exact term of soft_core.h:18-33).
-BT_HD double formFactorFP64(V3 x, V3 n, const V3* P, int count) {
+BT_COLD double formFactorFP64(V3 x, V3 n, const V3* P, int count) {
   double sum = 0;
   for (int i = 0; i < count; ++i) {
     V3 pa = P[i], pb = P[i + 1 == count ? 0 : i + 1];

@@ -337,3 +337,103 @@ EMU_API int64_t emu_point(void* h, const bt_camera* cam, const float* light, int
   c.add(stats);
   return k;
 }
+
+// Round structure of the wavefront for soft-shadow points: records of round
+// r run until they finish or need a clip; pieces form round r + 1.  For each
+// round: records, summed work and the largest single-record work, in units of
+// (kd steps + leaf visits + climbs + 4 * triangle tests).  Returns rounds.
+EMU_API int emu_soft_rounds(void* h, const float* light, float offset, int64_t n, const int32_t* tri, const float* X,
+                            const float* N, int maxRounds, int64_t* recs, double* work, double* maxWork,
+                            double* chain) {
+  Emu& e = *static_cast<Emu*>(h);
+  V3 Lc = mk(light[0], light[1], light[2]), LU = mk(light[3], light[4], light[5]), LV = mk(light[6], light[7], light[8]);
+  struct Rec {
+    SubBeam r;
+    Query q;
+    double pathWork;
+  };
+  std::vector<Rec> cur, nxt;
+  std::vector<Piece> sink;
+  double longest = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    if (tri[k] < 0) continue;
+    V3 x = mk(X[3 * k], X[3 * k + 1], X[3 * k + 2]), ns = mk(N[3 * k], N[3 * k + 1], N[3 * k + 2]);
+    Query q;
+    Poly<8> root;
+    float la;
+    if (!lightBeamSetup(Lc, LU, LV, x, ns, tri[k], offset, q, root, la)) continue;
+    querySetup(q, root.extent());
+    std::deque<SubBeam> fifo;
+    Stats st;
+    st.clear();
+    RootEnv env;
+    env.q = &fifo;
+    env.out = &sink;
+    env.qq = &q;
+    env.st = &st;
+    admitRoot(e.s, q, root, int(k), env, st);
+    for (const SubBeam& r : fifo) cur.push_back(Rec{r, q, 0});
+  }
+  int round = 0;
+  while (!cur.empty() && round < maxRounds) {
+    nxt.clear();
+    double tot = 0, mx = 0;
+    for (Rec& rc : cur) {
+      SubBeam r = rc.r;
+      const Query& q = rc.q;
+      Beam b;
+      expand(e.s, q, r, b);
+      Walk w;
+      walkBegin(e.s, r, w);
+      Stats st;
+      st.clear();
+      std::deque<SubBeam> fifo;
+      RootEnv env;
+      env.q = &fifo;
+      env.out = &sink;
+      env.qq = &q;
+      env.st = &st;
+      bool split = false;
+      for (;;) {
+        int res = advance(e.s, q, b, r, w, st);
+        int occ = -1;
+        if (res == kStepContinue) {
+          for (;;) {
+            res = testOne(e.s, q, r, b, st, occ);
+            if (res != kStepContinue || !moreInLeaf(e.s, q, r)) break;
+          }
+        }
+        if (res == kStepFinished) break;
+        if (res == kStepSplit) {
+          TriInfo ti;
+          Line L[5];
+          int nl = 0;
+          bool commit = false;
+          splitPass1<RootEnv>(e.s, q, r, b, st, ti, L, nl, commit);
+          if (!commit) {
+            r.cursor += 1;
+            w.phase = kPhTest;
+            continue;
+          }
+          splitPass2(q, r, b, ti, L, nl, env, st);
+          split = true;
+          break;
+        }
+      }
+      double wk = double(st.kdSteps + st.leafVisits + st.climbs) + 4.0 * st.triTests + (split ? 20.0 : 0.0);
+      tot += wk;
+      mx = wk > mx ? wk : mx;
+      const double pw = rc.pathWork + wk;
+      longest = pw > longest ? pw : longest;
+      for (const SubBeam& c : fifo) nxt.push_back(Rec{c, q, pw});
+      sink.clear();
+    }
+    recs[round] = int64_t(cur.size());
+    work[round] = tot;
+    maxWork[round] = mx;
+    ++round;
+    cur.swap(nxt);
+  }
+  *chain = longest;
+  return round;
+}

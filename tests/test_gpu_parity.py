@@ -5,7 +5,8 @@ to the reference float build per root; per-pixel ids and shadow flags
 identical outside the band of pixel centres covered by two polygons (shared
 edges, where the reference's own result depends on polygon order); soft
 visibility within 1e-4 of the FP64 build (bt_render_d) on identical shading
-points, exact E within 1e-6; primary rays (tri, X, N) bitwise."""
+points, exact E within 1e-5 of the image's largest E; primary rays (tri, X,
+N) bitwise."""
 import numpy as np
 import pytest
 
@@ -14,7 +15,7 @@ from conftest import piece_keys, scene, to_f32
 pytestmark = pytest.mark.gpu
 
 VIS_TOL = 1e-4   # |vis - vis_fp64|
-E_TOL = 1e-6     # |E_exact - E_fp64|
+E_REL = 1e-5     # |E_exact - E_fp64| relative to the image's largest E
 
 
 def _renderer(ps, **kw):
@@ -64,7 +65,10 @@ def test_soft_shadows_vs_fp64(name, W, H, scale, gpu, oracle_ready):
     err = np.abs(res.vis.astype(np.float64) - vd)[m]
     assert err.max() <= VIS_TOL, f"max |vis - fp64| {err.max():.3g}"
     assert np.abs(res.vis - vf.astype(np.float32))[m].max() <= 1e-6
-    assert np.abs(res.E.astype(np.float64) - Ed)[m].max() <= E_TOL + 1e-7 * np.abs(Ed).max()
+    e_gpu = np.abs(res.E.astype(np.float64) - Ed)[m].max()
+    assert e_gpu <= E_REL * np.abs(Ed).max(), f"max |E - fp64| {e_gpu:.3g}"
+    # the FP64 accumulation is closer to the FP64 build than the float build is
+    assert e_gpu <= np.abs(Ef - Ed)[m].max() + 1e-7
     assert np.array_equal(res.Eu, Euf.astype(np.float32))
     assert np.all(res.vis[~m] == -1)
 
