@@ -312,6 +312,7 @@ struct Beam {
 };
 
 BT_HD float sgnOf(const Beam& b, int a) { return ((b.neg >> a) & 1) ? -1.f : 1.f; }
+BT_HD float awAt(const Beam& b, int c, int i) { return c == 0 ? b.aw[0][i] : (c == 1 ? b.aw[1][i] : b.aw[2][i]); }
 
 // |w_a| at the corners (beamGeom / wfExpand, beam_core.h:214-219).
 BT_HD void beamAxes(const Query& q, Beam& b) {
@@ -383,6 +384,20 @@ BT_HD bool all4gt(const float* l, const float* r) { return l[0] > r[0] && l[1] >
 struct Box {
   float lo[3], hi[3];
 };
+// Component access with a run-time axis, as selects (an indexed array would
+// live in local memory).
+BT_HD float boxLo(const Box& b, int c) { return c == 0 ? b.lo[0] : (c == 1 ? b.lo[1] : b.lo[2]); }
+BT_HD float boxHi(const Box& b, int c) { return c == 0 ? b.hi[0] : (c == 1 ? b.hi[1] : b.hi[2]); }
+BT_HD void boxSetLo(Box& b, int c, float v) {
+  b.lo[0] = c == 0 ? v : b.lo[0];
+  b.lo[1] = c == 1 ? v : b.lo[1];
+  b.lo[2] = c == 2 ? v : b.lo[2];
+}
+BT_HD void boxSetHi(Box& b, int c, float v) {
+  b.hi[0] = c == 0 ? v : b.hi[0];
+  b.hi[1] = c == 1 ? v : b.hi[1];
+  b.hi[2] = c == 2 ? v : b.hi[2];
+}
 
 // kd decision at an inner node (BeamCtx::decide, beam_core.h:139-164).
 BT_HD int decide(const Query& q, const Beam& b, int a, float Ns, const Box& box) {
@@ -391,21 +406,21 @@ BT_HD int decide(const Query& q, const Beam& b, int a, float Ns, const Box& box)
     const bool pos = !((b.neg >> c) & 1);
     const float s = pos ? 1.f : -1.f;
     const float Oc = comp(q.P.O, c);
-    float entry = pos ? box.lo[c] : box.hi[c];
-    float exit = pos ? box.hi[c] : box.lo[c];
+    float entry = pos ? boxLo(box, c) : boxHi(box, c);
+    float exit = pos ? boxHi(box, c) : boxLo(box, c);
     float Nmin = s * (entry - Oc);
     float Nmax = s * (exit - Oc);
     float lhs[4], rhs[4], tl[4];
     for (int i = 0; i < 4; ++i) {
-      lhs[i] = b.aw[c][i] * Ns;
-      float r = b.aw[a][i] * Nmin;
+      lhs[i] = awAt(b, c, i) * Ns;
+      float r = awAt(b, a, i) * Nmin;
       float tol = (fabs_(lhs[i]) + fabs_(r)) * kKdRel;
       rhs[i] = r;
       tl[i] = r - tol;
     }
     if (all4lt(lhs, tl)) return kFar;
     for (int i = 0; i < 4; ++i) {
-      float r = b.aw[a][i] * Nmax;
+      float r = awAt(b, a, i) * Nmax;
       float tol = (fabs_(lhs[i]) + fabs_(r)) * kKdRel;
       tl[i] = r + tol;
     }
@@ -415,7 +430,7 @@ BT_HD int decide(const Query& q, const Beam& b, int a, float Ns, const Box& box)
     float lhs[4], tl[4];
     for (int i = 0; i < 4; ++i) {
       lhs[i] = b.farA[i] * Ns;
-      float r = b.aw[a][i] * b.farC;
+      float r = awAt(b, a, i) * b.farC;
       float tol = (fabs_(lhs[i]) + fabs_(r)) * kKdRel;
       tl[i] = r + tol;
     }

@@ -65,19 +65,26 @@ enum RootState { kRootNone = 0, kRootTraced = 1, kRootKilled = 2 };
 enum Phase { kIdle = 0, kLoaded = 1, kTrace = 2, kSplit = 3 };
 
 // Engine state shared by all warps of a pass.
-struct Counters {
-  int count[2];      // records in spill queue 0 / 1
-  int head;          // fetch cursor in the queue being consumed
-  int rootNext;      // next entry of the root list to admit
-  int inflight;      // admitted roots not finished
-  int killed;        // roots abandoned in this pass
-  unsigned long long reserved;  // spill slots reserved by roots in flight
-  int maxSpill;
-  int overflow;      // a spill found no slot (impossible by the reservation rule)
-  int outCount;      // output polygons
-  int done;
-  int launches;
-  int pad;
+struct __align__(128) Counters {
+  unsigned long long reserved;  // ring slots reserved by roots in flight
+  int rootNext;                 // next entry of the root list to admit
+  int inflight;                 // admitted roots not finished
+  int killed;                   // roots abandoned in this pass
+  int error;                    // a bounded ring wait gave up (the ring is reset)
+  int outCount;                 // output polygons
+  int maxQueue;                 // ring occupancy high-water mark (sampled)
+};
+
+// The sub-beam ring: positions are monotonic 64-bit counters; slot
+// pos & mask holds position pos once seq[slot] == pos + 1 (published), and
+// is free for position pos + capacity once seq[slot] == pos + capacity.
+// head and tail sit on separate 128-byte lines: consumers (CAS on head) and
+// producers (atomicAdd on tail) do not contend for one L2 line.
+struct Ring {
+  unsigned long long head;  // next position to take
+  unsigned long long pad0[15];
+  unsigned long long tail;  // next position to fill
+  unsigned long long pad1[15];
 };
 
 // Per-root query: plane, tolerances, mode (WfRoot, cuda/wavefront.cu:80-86).
@@ -124,11 +131,15 @@ struct AppParams {
 
 struct RoundParams {
   SceneDev s;
-  SubBeam* q[2];
-  int cur;
+  SubBeam* slot;
+  uint32_t* seq;
+  Ring* ring;
+  unsigned long long mask;
   int capacity;
   int budget;
+  int reserve;  // ring slots reserved per root: max(budget, 32) (a root's pre-split pieces always fit)
   int numRoots;
+  int rootCap;  // size of the per-root arrays
   const int32_t* rootList;
   RootRec* roots;
   int32_t* live;
@@ -137,6 +148,7 @@ struct RoundParams {
   Counters* ctr;
   unsigned long long* stats;
   int splitBatch;
+  unsigned long long* phaseCycles;  // optional: warp cycles per engine phase (diagnostics)
   AppParams app;
 };
 
@@ -156,8 +168,11 @@ __device__ void storeRoot(RootRec* R, const Query& q, float lightArea, int attem
   *R = r;
 }
 
-__device__ void loadRoot(const RootRec* R, Query& q, float& lightArea) {
-  const float4 a = R->a, b = R->b, c = R->c, d = R->d, e = R->e, f = R->f;
+// Per-root records are written during the launch by the admitting SM; they
+// are read from L2 (an L1 line could hold a neighbouring root's older copy).
+__device__ __forceinline__ void loadRoot(const RootRec* R, Query& q, float& lightArea) {
+  const float4 a = __ldcg(&R->a), b = __ldcg(&R->b), c = __ldcg(&R->c), d = __ldcg(&R->d), e = __ldcg(&R->e),
+               f = __ldcg(&R->f);
   q.P.O = mk(a.x, a.y, a.z);
   q.P.p0 = mk(b.x, b.y, b.z);
   q.P.u = mk(c.x, c.y, c.z);
@@ -173,16 +188,16 @@ __device__ void loadRoot(const RootRec* R, Query& q, float& lightArea) {
   querySetup(q, a.w);
 }
 
-__device__ void rootDone(const RoundParams& p) {
-  atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)p.budget));
+__device__ __forceinline__ void rootDone(const RoundParams& p) {
+  atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)p.reserve));
   atomicSub(&p.ctr->inflight, 1);
 }
 
-__device__ void liveSub(const RoundParams& p, int root, int n) {
+__device__ __forceinline__ void liveSub(const RoundParams& p, int root, int n) {
   if (n > 0 && atomicSub(&p.live[root], n) == n) rootDone(p);
 }
 
-__device__ void killRoot(const RoundParams& p, int root) {
+__device__ __forceinline__ void killRoot(const RoundParams& p, int root) {
   if (atomicExch(&p.state[root], int(kRootKilled)) != int(kRootKilled)) atomicAdd(&p.ctr->killed, 1);
 }
 
@@ -200,57 +215,125 @@ __device__ void appendPoly(const RoundParams& p, int root, const float* x, const
   o.tri[k] = tri;
   o.area[k] = area;
   o.root[k] = root;
-  o.attempt[k] = p.attempt[root];
+  o.attempt[k] = __ldcg(&p.attempt[root]);
 }
+
+// A finished piece handed to the output path in a small temporary: the
+// tracing lane's query and beam never leave registers.
+struct PieceOut {
+  Plane P;
+  float qx[4], qy[4];
+  int n, root, tri, exclude;
+  float lightArea;
+};
 
 // Finished pieces.  Soft: unoccluded area (fixed point) and, with exact, the
 // FP64 Lambert integral; primary: visible polygons; point shadows: occluded
 // pieces projected back into the image (WfOut, cuda/wavefront.cu:193-227).
 template <int App>
-__device__ void outputPiece(const RoundParams& p, const Query& q, float lightArea, int root, const Beam& b, int tri,
-                            Stats& st) {
+__device__ __noinline__ void outputPieceCold(const RoundParams& p, const PieceOut* o) {
   Poly<4> poly;
-  const float area = beamPoly(b, poly);
-  if (tri >= 0) st.hits++;
-  st.beams++;
+  poly.n = o->n;
+  for (int i = 0; i < 4; ++i) {
+    poly.x[i] = o->qx[i];
+    poly.y[i] = o->qy[i];
+  }
+  const float area = poly.area();
+  const int root = o->root;
   if (App == kAppSoft) {
-    if (tri >= 0) return;
-    const double f = double(area) / double(lightArea) * kFixVis;
+    const double f = double(area) / double(o->lightArea) * kFixVis;
     if (f > 0) atomicAdd(&p.app.missFx[root], (unsigned long long)llrint(f));
     if (p.app.exact) {
       V3 P[4];
-      for (int i = 0; i < poly.n; ++i) P[i] = planePoint(q.P, poly.x[i], poly.y[i]);
-      const float4 xs = p.app.shade[2 * root], ns = p.app.shade[2 * root + 1];
+      for (int i = 0; i < poly.n; ++i) P[i] = planePoint(o->P, poly.x[i], poly.y[i]);
+      const float4 xs = __ldcg(&p.app.shade[2 * root]), ns = __ldcg(&p.app.shade[2 * root + 1]);
       const double G = formFactorFP64(mk(xs.x, xs.y, xs.z), mk(ns.x, ns.y, ns.z), P, poly.n);
       const double g = G * kFixG;
       if (g > 0) atomicAdd(&p.app.gFx[root], (unsigned long long)llrint(g));
     }
-    return;
-  }
-  if (tri < 0) return;
-  if (App == kAppPrimary) {
-    appendPoly(p, root, poly.x, poly.y, poly.n, tri, area);
+  } else if (App == kAppPrimary) {
+    appendPoly(p, root, poly.x, poly.y, poly.n, o->tri, area);
   } else {
     float ox[4], oy[4];
-    const int T = q.exclude;
-    if (pointShadowToImage(p.app.camPlane, q.P, poly.x, poly.y, poly.n, ox, oy)) appendPoly(p, root, ox, oy, poly.n, T, 0.f);
+    if (pointShadowToImage(p.app.camPlane, o->P, poly.x, poly.y, poly.n, ox, oy))
+      appendPoly(p, root, ox, oy, poly.n, o->exclude, 0.f);
   }
 }
 
-// Appends one record to the next round's queue (admission pieces).
-__device__ bool pushNext(const RoundParams& p, const SubBeam& r) {
-  const int nxt = p.cur ^ 1;
-  const int g = atomicAdd(&p.ctr->count[nxt], 1);
-  if (g < p.capacity) {
-    p.q[nxt][g] = r;
-    return true;
+template <int App>
+__device__ __forceinline__ void outputPiece(const RoundParams& p, const Query& q, float lightArea, int root,
+                                            const Beam& b, int tri, Stats& st) {
+  if (tri >= 0) st.hits++;
+  st.beams++;
+  if (App == kAppSoft ? tri >= 0 : tri < 0) return;  // soft keeps the visible light, the others the hits
+  PieceOut o;
+  o.P = q.P;
+  for (int i = 0; i < 4; ++i) {
+    o.qx[i] = b.qx[i];
+    o.qy[i] = b.qy[i];
   }
-  atomicExch(&p.ctr->overflow, 1);
+  o.n = b.n;
+  o.root = root;
+  o.tri = tri;
+  o.exclude = q.exclude;
+  o.lightArea = lightArea;
+  outputPieceCold<App>(p, &o);
+}
+
+constexpr int kWaitLimit = 1 << 18;  // polls of one ring slot before the engine reports an error
+
+// Bounded wait for a ring slot's sequence number.  The waits are short by
+// construction (a producer's slot was already taken by the previous lap's
+// consumer; a consumer's slot was already reserved by its producer), so
+// running out means an engine fault: the error flag ends the pass.
+__device__ __forceinline__ bool ringWait(const RoundParams& p, uint32_t idx, uint32_t want) {
+  for (int i = 0; i < kWaitLimit; ++i) {
+    if (__ldcv(&p.seq[idx]) == want) return true;
+    if ((i & 255) == 255 && __ldcv(&p.ctr->error)) return false;
+    __nanosleep(i < 32 ? 32 : 256);
+  }
+  atomicExch(&p.ctr->error, 1);
   return false;
 }
 
-// Admission: the root's first piece stays in the lane, the others go to the
-// next round's queue.
+// Fills ring position `pos` with record r and publishes it.
+__device__ __forceinline__ void ringPut(const RoundParams& p, unsigned long long pos, const SubBeam& r) {
+  const uint32_t idx = uint32_t(pos & p.mask);
+  if (!ringWait(p, idx, uint32_t(pos))) return;
+  p.slot[idx] = r;
+  __threadfence();
+  atomicExch(&p.seq[idx], uint32_t(pos + 1));
+}
+
+// Takes ring position `pos` (claimed by the caller), bypassing L1 (slots are
+// rewritten by other SMs), and frees the slot for the next lap.
+__device__ __forceinline__ bool ringGet(const RoundParams& p, unsigned long long pos, SubBeam& r) {
+  const uint32_t idx = uint32_t(pos & p.mask);
+  if (!ringWait(p, idx, uint32_t(pos + 1))) return false;
+  __threadfence();
+  const float4* src = reinterpret_cast<const float4*>(&p.slot[idx]);
+  float4 v[4];
+  for (int i = 0; i < 4; ++i) v[i] = __ldcg(src + i);
+  memcpy(&r, v, sizeof(SubBeam));
+  __threadfence();
+  atomicExch(&p.seq[idx], uint32_t(pos + (unsigned long long)p.capacity));
+  return true;
+}
+
+// Claims up to `want` published-or-reserved positions for a warp (lane 0);
+// returns how many, from position h.
+__device__ __forceinline__ int ringClaim(const RoundParams& p, int want, unsigned long long& h) {
+  for (int tries = 0; tries < 64; ++tries) {
+    h = __ldcv(&p.ring->head);
+    const unsigned long long t = __ldcv(&p.ring->tail);
+    if (h >= t) return 0;
+    const int n = int(min((unsigned long long)want, t - h));
+    if (atomicCAS(&p.ring->head, h, h + n) == h) return n;
+  }
+  return 0;
+}
+
+// Admission: the root's first piece stays in the lane, the others go to the ring.
 template <int App>
 struct AdmitEnv {
   const RoundParams* p;
@@ -268,17 +351,19 @@ struct AdmitEnv {
       haveFirst = 1;
       return true;
     }
-    return pushNext(*p, r);
+    ringPut(*p, atomicAdd(&p->ring->tail, 1ull), r);
+    return true;
   }
   __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
   __device__ void missed(const Beam& b) { outputPiece<App>(*p, *q, lightArea, root, b, -1, *st); }
   __device__ void dropped(float) {}
 };
 
-// Clip emission into `slots` consecutive slots of the next round's queue
-// reserved by one atomic; pieces dropped as slivers leave holes (n = 0) that
-// the next round skips, as the reference's split does
-// (wfSplitEmit, wavefront_core.h:367-422).
+// Clip emission: pieces collect in chunks of kChunk and each full chunk is
+// written to ring positions reserved only when its records are ready, so
+// consumers never wait on a clip in progress (wfSplitEmit,
+// wavefront_core.h:367-422).
+constexpr int kChunk = 8;
 template <int App>
 struct SplitEnv {
   const RoundParams* p;
@@ -286,10 +371,23 @@ struct SplitEnv {
   float lightArea;
   int root;
   Stats* st;
-  SubBeam* dst;
   int written;
+  int nbuf;
+  SubBeam buf[kChunk];
+  __device__ void flush() {
+    if (nbuf == 0) return;
+    const unsigned long long pos = atomicAdd(&p->ring->tail, (unsigned long long)nbuf);
+    for (int i = 0; i < nbuf; ++i) ringPut(*p, pos + (unsigned long long)i, buf[i]);
+    if ((pos & 63) < (unsigned long long)nbuf) {
+      const unsigned long long hd = __ldcv(&p->ring->head), end = pos + (unsigned long long)nbuf;
+      if (end > hd) atomicMax(&p->ctr->maxQueue, int(min(end - hd, 0x7fffffffull)));
+    }
+    written += nbuf;
+    nbuf = 0;
+  }
   __device__ bool queue(const SubBeam& r) {
-    dst[written++] = r;
+    buf[nbuf++] = r;
+    if (nbuf == kChunk) flush();
     return true;
   }
   __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
@@ -309,10 +407,23 @@ __device__ __forceinline__ bool softPixel(const AppParams& a, int k, int& pix) {
   return x < a.W && y < a.H;
 }
 
+// What admission hands back to the lane (a temporary: the lane's own state
+// stays in registers).
+struct AdmitOut {
+  SubBeam first;
+  Query q;
+  float lightArea;
+  Stats st;
+};
+
 // Sets up root k and queues its pre-split pieces (admitRoot,
 // cuda/wavefront.cu:255-325).  Returns true if the lane took a piece.
 template <int App>
-__device__ bool admit(const RoundParams& p, int k, Stats& st, SubBeam& first, Query& q, float& lightArea) {
+__device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
+  Query& q = out->q;
+  float& lightArea = out->lightArea;
+  Stats& st = out->st;
+  SubBeam& first = out->first;
   p.live[k] = 0;
   p.state[k] = kRootNone;
   const int att = p.attempt[k] + 1;
@@ -390,19 +501,37 @@ __device__ bool admit(const RoundParams& p, int k, Stats& st, SubBeam& first, Qu
   querySetup(q, poly.extent());
   storeRoot(&p.roots[k], q, lightArea, att);
   p.state[k] = kRootTraced;
+  // Pieces reach the ring as they are made and other warps may finish them
+  // at once: hold the live count up until all pieces are counted.
+  constexpr int kHold = 1 << 20;
+  p.live[k] = kHold;
   AdmitEnv<App> env{&p, &q, lightArea, k, &st, SubBeam(), 0, 0};
   const bool ok = admitRoot(p.s, q, poly, k, env, st);
-  p.live[k] = env.queued;
   if (!ok || env.queued > p.budget) killRoot(p, k);
-  if (env.queued == 0) {
-    rootDone(p);
+  const int before = atomicSub(&p.live[k], kHold - env.queued);
+  if (before - (kHold - env.queued) == 0) {
+    rootDone(p);  // no piece left (none made, or all finished already)
     return false;
   }
   if (env.haveFirst) first = env.first;
   return env.haveFirst != 0;
 }
 
-__device__ void flushStats(const RoundParams& p, const Stats& st) {
+__device__ __forceinline__ void addStats(Stats& a, const Stats& b) {
+  a.kdSteps += b.kdSteps;
+  a.leafVisits += b.leafVisits;
+  a.triTests += b.triTests;
+  a.hits += b.hits;
+  a.splits += b.splits;
+  a.beams += b.beams;
+  a.rootBeams += b.rootBeams;
+  a.presplitBeams += b.presplitBeams;
+  a.fiveSplits += b.fiveSplits;
+  a.climbs += b.climbs;
+  a.dropped += b.dropped;
+}
+
+__device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st) {
   unsigned long long v[kStDropped] = {st.kdSteps, st.leafVisits, st.triTests, st.hits, st.splits,
                                       st.beams, st.rootBeams, st.presplitBeams, st.fiveSplits, st.climbs};
   for (int f = 0; f < kStDropped; ++f) {
@@ -415,19 +544,82 @@ __device__ void flushStats(const RoundParams& p, const Stats& st) {
   if (laneId() == 0 && d != 0) atomicAdd(reinterpret_cast<double*>(&p.stats[kStDropped]), d);
 }
 
-// One round: every record of the current queue, then new roots, is traced
-// until it finishes or needs a clip; clips run warp-batched; all pieces go to
-// the next round's queue.  Lanes are refilled from the shared queue as soon
-// as they fall idle, so every warp works on every root.
+// Clips one buffered record (a triangle at its cursor needs it): the pieces
+// go to the ring in consecutive positions.  Returns true if nothing
+// measurable changed and the record (updated in place) continues at the next
+// triangle.  Works on its own query and beam: the caller's stay in registers.
 template <int App>
-__global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
-  const int lane = laneId();
+__device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Stats* cs) {
+  Stats& st = *cs;
+  SubBeam rec = *recp;
+  const int root = rec.root;
+  if (p.state[root] == kRootKilled) {
+    liveSub(p, root, 1);
+    return false;
+  }
+  Query q;
+  float lightArea;
+  Beam b;
+  loadRoot(&p.roots[root], q, lightArea);
+  expand(p.s, q, rec, b);
+  TriInfo ti;
+  Line L[5];
+  int nl = 0;
+  bool commit = false;
+  const int slots = splitPass1<SplitEnv<App>>(p.s, q, rec, b, st, ti, L, nl, commit);
+  if (slots < 0) {
+    killRoot(p, root);
+    liveSub(p, root, 1);
+    return false;
+  }
+  if (!commit) {
+    recp->cursor = rec.cursor + 1;
+    return true;
+  }
+  const int old = atomicAdd(&p.live[root], slots - 1);
+  if (old + slots - 1 > p.budget) {
+    killRoot(p, root);
+    liveSub(p, root, slots);
+    return false;
+  }
+  if (old + slots - 1 == 0) rootDone(p);  // every piece occluded: the root is finished
+  SplitEnv<App> env;
+  env.p = &p;
+  env.q = &q;
+  env.lightArea = lightArea;
+  env.root = root;
+  env.st = &st;
+  env.written = 0;
+  env.nbuf = 0;
+  splitPass2(q, rec, b, ti, L, nl, env, st);
+  env.flush();
+  // slivers dropped by beamGeom were counted in `slots` but never queued
+  if (env.written < slots) liveSub(p, root, slots - env.written);
+  return false;
+}
+
+constexpr int kSplitBuf = 64;   // per warp: records waiting for a clip
+constexpr int kIdleWaits = 400;  // sleeps (up to 33 us each) of an idle warp waiting for work before it leaves the launch
+
+// The persistent engine.  Lanes take records from the ring (one claim per
+// warp for all idle lanes), then admit new roots; each lane traces its
+// record leaf by leaf until it finishes or a triangle needs a clip.  Records
+// that need a clip wait in a per-warp buffer in shared memory; when 32 wait
+// (or the warp has nothing left to trace) the warp parks its tracing lanes'
+// records in shared memory and clips 32 records with all lanes at once, then
+// resumes.  Pieces go to the ring, where any warp takes them: no rounds, no
+// tail of a round, every warp works on every root.
+template <int App>
+__global__ void __launch_bounds__(kThreads) engineKernel(const __grid_constant__ RoundParams p) {
+  __shared__ SubBeam sSplit[kWarps][kSplitBuf];
+  __shared__ SubBeam sPark[kWarps][32];
+  __shared__ int sCnt[kWarps];
+  const int lane = laneId(), wid = threadIdx.x >> 5;
   const unsigned ltMask = (1u << lane) - 1u;
-  const int nCur = min(p.ctr->count[p.cur], p.capacity);
-  const SubBeam* qCur = p.q[p.cur];
-  const int nxt = p.cur ^ 1;
-  bool queueDone = nCur == 0, rootsDone = false;
-  int admitWait = 0, blockedSleeps = 0;
+  if (lane == 0) sCnt[wid] = 0;
+  __syncwarp();
+  bool rootsDone = false;
+  int admitWait = 0, waits = 0;
   int phase = kIdle;
   SubBeam r;
   Beam b;
@@ -437,56 +629,57 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
   int qRoot = -1;
   Stats st;
   st.clear();
+  // optional phase accounting: refill, admit, expand, clip, idle, trace, buffer
+  unsigned long long pc[7] = {0, 0, 0, 0, 0, 0, 0};
+  long long tprev = p.phaseCycles ? clock64() : 0;
+#define BT_PHASE(k)                         \
+  if (p.phaseCycles) {                      \
+    const long long t_ = clock64();         \
+    pc[k] += (unsigned long long)(t_ - tprev); \
+    tprev = t_;                             \
+  }
   for (;;) {
-    // ---- refill idle lanes: the round's queue, then new roots
+    // ---- refill idle lanes: the ring, then new roots
     unsigned idle = __ballot_sync(kFull, phase == kIdle);
-    if (idle && !queueDone) {
-      const int ni = __popc(idle);
-      int base = 0;
-      if (lane == 0) base = atomicAdd(&p.ctr->head, ni);
-      base = __shfl_sync(kFull, base, 0);
-      if (base + ni >= nCur) queueDone = true;
-      const int i = base + __popc(idle & ltMask);
-      if (phase == kIdle && i < nCur) {
-        r = qCur[i];
-        phase = kLoaded;
+    if (idle) {
+      unsigned long long h = 0;
+      int n = 0;
+      if (lane == 0) n = ringClaim(p, __popc(idle), h);
+      n = __shfl_sync(kFull, n, 0);
+      h = __shfl_sync(kFull, h, 0);
+      const int rank = __popc(idle & ltMask);
+      if (phase == kIdle && rank < n) {
+        if (ringGet(p, h + (unsigned long long)rank, r)) phase = kLoaded;
       }
       idle = __ballot_sync(kFull, phase == kIdle);
     }
+    BT_PHASE(0)
     if (idle && !rootsDone && admitWait > 0) {
       --admitWait;
     } else if (idle && !rootsDone) {
-      // Reserve `budget` queue slots for each root taken; take only as many
-      // roots as fit in the free slots.
+      // Reserve ring slots for each root taken; take only as many roots as fit.
       const int ni = __popc(idle);
       int base = -1, fit = 0;
       if (lane == 0) {
-        const unsigned long long bud = (unsigned long long)p.budget, cap = (unsigned long long)p.capacity;
-        const unsigned long long need = (unsigned long long)ni * bud;
+        const unsigned long long res = (unsigned long long)p.reserve, cap = (unsigned long long)p.capacity;
+        const unsigned long long need = (unsigned long long)ni * res;
         const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
         fit = ni;
         if (old + need > cap) {
-          fit = old >= cap ? 0 : int(min((unsigned long long)ni, (cap - old) / bud));
-          atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - fit)) * bud);
+          fit = old >= cap ? 0 : int(min((unsigned long long)ni, (cap - old) / res));
+          atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - fit)) * res);
         }
         if (fit > 0) {
           base = atomicAdd(&p.ctr->rootNext, fit);
           const int got = max(0, min(fit, p.numRoots - base));
-          if (got < fit) atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(fit - got)) * bud);
+          if (got < fit) atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(fit - got)) * res);
           if (got > 0) atomicAdd(&p.ctr->inflight, got);
         }
       }
       base = __shfl_sync(kFull, base, 0);
       fit = __shfl_sync(kFull, fit, 0);
       if (fit == 0) {
-        // No free slots: roots in flight must finish first.  A warp with
-        // work carries on and retries later; an idle warp sleeps a bounded
-        // number of times, then leaves the rest to the next round.
-        admitWait = 8;
-        if (__popc(idle) == 32 && queueDone) {
-          if (++blockedSleeps > 64) rootsDone = true;
-          __nanosleep(2000);
-        }
+        admitWait = 8;  // the ring is fully reserved: retry later
       } else if (base + fit >= p.numRoots) {
         rootsDone = true;
       }
@@ -494,17 +687,25 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
       const int j = base + rank;
       if (fit > 0 && rank < fit && phase == kIdle && j < p.numRoots) {
         const int k = p.rootList ? p.rootList[j] : j;
-        if (admit<App>(p, k, st, r, q, lightArea)) {
+        AdmitOut ao;
+        ao.st.clear();
+        if (admit<App>(p, k, &ao)) {
+          r = ao.first;
+          q = ao.q;
+          lightArea = ao.lightArea;
           qRoot = k;
           phase = kLoaded;
-        } else {
-          qRoot = -1;
         }
+        addStats(st, ao.st);
       }
     }
+    BT_PHASE(1)
     // ---- expand newly loaded records (holes and abandoned roots are dropped)
     if (phase == kLoaded) {
-      if (r.n == 0 || p.state[r.root] == kRootKilled) {
+      if (uint32_t(r.root) >= uint32_t(p.rootCap) || r.node >= p.s.numNodes || r.n > 4) {
+        atomicExch(&p.ctr->error, 2);  // a malformed record: report, never index with it
+        phase = kIdle;
+      } else if (r.n == 0 || p.state[r.root] == kRootKilled) {
         liveSub(p, r.root, 1);
         phase = kIdle;
       } else {
@@ -518,55 +719,75 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
       }
     }
     const unsigned tr = __ballot_sync(kFull, phase == kTrace);
-    const unsigned sp = __ballot_sync(kFull, phase == kSplit);
     const unsigned idleNow = __ballot_sync(kFull, phase == kIdle);
-    if (!tr && !sp) {
-      if (queueDone && rootsDone) break;
+    __syncwarp();
+    const int cnt = sCnt[wid];
+    BT_PHASE(2)
+    if (cnt >= p.splitBatch || (cnt > 0 && (!tr || idleNow))) {
+      // ---- clip: park the tracing lanes, clip up to 32 buffered records
+      const bool parked = phase == kTrace;
+      if (parked) sPark[wid][lane] = r;
+      const int m = min(32, cnt);
+      const bool mine = lane < m;
+      SubBeam* recp = &sSplit[wid][cnt - m + (mine ? lane : 0)];
+      bool cont = false;
+      if (mine) {
+        Stats cs;
+        cs.clear();
+        cont = clipRecord<App>(p, recp, &cs);
+        addStats(st, cs);
+      }
+      SubBeam rec;
+      if (cont) rec = *recp;
+      __syncwarp();
+      if (lane == 0) sCnt[wid] = cnt - m;
+      __syncwarp();
+      if (parked) {
+        if (cont) ringPut(p, atomicAdd(&p.ring->tail, 1ull), rec);  // nothing changed: back to the ring
+        r = sPark[wid][lane];
+      } else if (cont) {
+        r = rec;
+      }
+      if (parked || cont) {
+        if (r.root != qRoot) {
+          loadRoot(&p.roots[r.root], q, lightArea);
+          qRoot = r.root;
+        }
+        expand(p.s, q, r, b);
+        walkBegin(p.s, r, w);
+        phase = kTrace;
+      } else {
+        phase = kIdle;
+      }
+      waits = 0;
+      BT_PHASE(3)
       continue;
     }
-    const bool doSplit = sp && (__popc(sp) >= p.splitBatch || !tr || idleNow);
-    if (doSplit) {
-      if (phase == kSplit) {
-        TriInfo ti;
-        Line L[5];
-        int nl = 0;
-        bool commit = false;
-        const int slots = splitPass1<SplitEnv<App>>(p.s, q, r, b, st, ti, L, nl, commit);
-        const int root = r.root;
-        if (slots < 0) {
-          killRoot(p, root);
-          liveSub(p, root, 1);
-          phase = kIdle;
-        } else if (!commit) {
-          r.cursor += 1;  // nothing measurable changes: continue at the next triangle
-          w.phase = kPhTest;
-          phase = kTrace;
-        } else {
-          const int old = atomicAdd(&p.live[root], slots - 1);
-          if (old + slots - 1 > p.budget) {
-            killRoot(p, root);
-            liveSub(p, root, slots);
-          } else {
-            if (old + slots - 1 == 0) rootDone(p);  // every piece occluded: the root is finished
-            const int base = slots > 0 ? atomicAdd(&p.ctr->count[nxt], slots) : 0;
-            if (base + slots > p.capacity) {
-              atomicExch(&p.ctr->overflow, 1);
-            } else {
-              SplitEnv<App> env{&p, &q, lightArea, root, &st, p.q[nxt] + base, 0};
-              splitPass2(q, r, b, ti, L, nl, env, st);
-              for (int k = env.written; k < slots; ++k) {
-                SubBeam hole = r;
-                hole.n = 0;
-                p.q[nxt][base + k] = hole;
-              }
-            }
-          }
-          phase = kIdle;
-        }
+    if (!tr) {
+      // Nothing to trace or clip in this warp: leave when every root is done,
+      // else wait (bounded) for pieces from other warps.  Lane 0 reads the
+      // shared counters and the warp decides as one (every lane must reach
+      // the same warp-wide intrinsics).
+      int flags = 0;
+      if (lane == 0) {
+        const unsigned long long hd = __ldcv(&p.ring->head), tl = __ldcv(&p.ring->tail);
+        flags = (__ldcv(&p.ctr->error) ? 1 : 0) | (hd >= tl ? 2 : 0) | (__ldcv(&p.ctr->inflight) == 0 ? 4 : 0);
       }
-    } else if (phase == kTrace) {
-      // one leaf: climb / descend to it, then test its triangles
-      int res = advance(p.s, q, b, r, w, st);
+      flags = __shfl_sync(kFull, flags, 0);
+      if (flags & 1) break;
+      if ((rootsDone || admitWait > 0) && (flags & 2)) {
+        if (rootsDone && (flags & 4)) break;
+        if (++waits > kIdleWaits) break;
+        __nanosleep(waits < 8 ? 256u << waits : 32768u);  // back off: idle warps must not crowd the ring's lines
+      }
+      BT_PHASE(4)
+      continue;
+    }
+    waits = 0;
+    // ---- trace one leaf: climb / descend to it, then test its triangles
+    int res = kStepContinue;
+    if (phase == kTrace) {
+      res = advance(p.s, q, b, r, w, st);
       int occ = -1;
       if (res == kStepContinue) {
         for (;;) {
@@ -578,32 +799,34 @@ __global__ void __launch_bounds__(kThreads) roundKernel(const RoundParams p) {
         outputPiece<App>(p, q, lightArea, r.root, b, occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1), st);
         liveSub(p, r.root, 1);
         phase = kIdle;
-      } else if (res == kStepSplit) {
-        phase = kSplit;
       }
     }
+    BT_PHASE(5)
+    // records that need a clip join the warp's clip buffer
+    const unsigned spl = __ballot_sync(kFull, phase == kTrace && res == kStepSplit);
+    if (spl) {
+      const int c0 = sCnt[wid];
+      if (phase == kTrace && res == kStepSplit) {
+        sSplit[wid][c0 + __popc(spl & ltMask)] = r;
+        phase = kIdle;
+      }
+      __syncwarp();
+      if (lane == 0) sCnt[wid] = c0 + __popc(spl);
+      __syncwarp();
+    }
+    BT_PHASE(6)
   }
+#undef BT_PHASE
+  if (p.phaseCycles && lane == 0)
+    for (int k = 0; k < 7; ++k) atomicAdd(&p.phaseCycles[k], pc[k]);
   flushStats(p, st);
 }
 
-// Between launches: the consumed queue is emptied, completion is decided
-// (scheduleKernel's bookkeeping, cuda/wavefront.cu:327-345).
-// Start of a retry pass: per-pass state is cleared; output counts and the
-// spill high-water mark of the call are kept.
-__global__ void passResetKernel(Counters* c) {
-  c->count[0] = c->count[1] = 0;
-  c->head = c->rootNext = c->inflight = c->killed = 0;
-  c->reserved = 0;
-  c->overflow = c->done = 0;
-}
-
-__global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
-  const int nxt = cur ^ 1;
-  if (c->count[nxt] > c->maxSpill) c->maxSpill = c->count[nxt];
-  c->count[cur] = 0;
-  c->head = 0;
-  c->launches++;
-  c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
+// Sets every ring slot free for its first lap (seq[i] = i).
+__global__ void ringInitKernel(uint32_t* seq, int cap, Ring* ring) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cap) seq[i] = uint32_t(i);
+  if (i == 0) ring->head = ring->tail = 0;
 }
 
 // Roots abandoned in a pass, compacted for the retry pass.
@@ -852,8 +1075,10 @@ struct bt_gpu_ctx {
   float offset = 0;  // |scene diagonal| * kEpsRel
   int64_t numTris = 0;
   // engine
-  SubBeam* dQ[2] = {nullptr, nullptr};
-  int capacity = 0;
+  SubBeam* dSlot = nullptr;  // sub-beam ring: capacity records
+  uint32_t* dSeq = nullptr;   // per-slot sequence numbers
+  Ring* dRing = nullptr;
+  int capacity = 0;           // power of two
   Counters* dCtr = nullptr;
   unsigned long long* dStats = nullptr;
   size_t rootCap = 0;
@@ -862,6 +1087,7 @@ struct bt_gpu_ctx {
   unsigned long long *dMiss = nullptr, *dG = nullptr;
   float4* dShade = nullptr;
   int* dKillCount = nullptr;
+  unsigned long long* dPhase = nullptr;
   // outputs
   int64_t outCap = 0;
   float *dOx = nullptr, *dOy = nullptr, *dOarea = nullptr;
@@ -974,7 +1200,7 @@ int ensurePix(bt_gpu_ctx* c, int64_t n) {
 template <int App>
 int gridFor(bt_gpu_ctx* c) {
   int perSM = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, roundKernel<App>, kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, engineKernel<App>, kThreads, 0);
   if (c->cfg.blocks_per_sm > 0) perSM = c->cfg.blocks_per_sm;
   return c->sms * std::max(1, perSM);
 }
@@ -998,26 +1224,39 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
   info->dropped_area = d;
   info->eps_band_corners = st[kStEpsBand];
   info->eps_fp64_flips = st[kStEpsFlip];
-  info->max_spill = std::max(info->max_spill, hc.maxSpill);
+  info->max_spill = std::max(info->max_spill, hc.maxQueue);
 }
 
 // Runs every root of `R` through the engine: passes of launches until all
 // roots are done; roots abandoned over budget are retried with 16x budget.
+int resetRing(bt_gpu_ctx* c) {
+  ringInitKernel<<<(c->capacity + 255) / 256, 256, 0, c->stream>>>(c->dSeq, c->capacity, c->dRing);
+  CK(cudaGetLastError());
+  return BT_OK;
+}
+
+// Runs every root of `R` through the engine: launches of the persistent
+// kernel until all roots are done (one launch unless idle warps left early);
+// roots abandoned over budget are retried in a further pass with 16x budget.
 template <int App>
 int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info) {
   int e = ensureRoots(c, size_t(R));
   if (e) return e;
   CK(cudaMemsetAsync(c->dAttempt, 0, sizeof(int32_t) * size_t(R), c->stream));
   CK(cudaMemsetAsync(c->dStats, 0, sizeof(unsigned long long) * kNumStats, c->stream));
+  CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
   app.missFx = c->dMiss;
   app.gFx = c->dG;
   app.shade = c->dShade;
   RoundParams p;
   p.s = c->s;
-  p.q[0] = c->dQ[0];
-  p.q[1] = c->dQ[1];
+  p.slot = c->dSlot;
+  p.seq = c->dSeq;
+  p.ring = c->dRing;
   p.capacity = c->capacity;
+  p.mask = (unsigned long long)(c->capacity - 1);
   p.roots = c->dRoots;
+  p.rootCap = R;
   p.live = c->dLive;
   p.state = c->dState;
   p.attempt = c->dAttempt;
@@ -1025,59 +1264,72 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.stats = c->dStats;
   p.splitBatch = std::max(1, std::min(32, c->cfg.split_batch));
   p.app = app;
+  p.phaseCycles = nullptr;
+  // BT_PHASES=1: warp cycles per engine phase on stderr (diagnostics).
+  const bool phases = getenv("BT_PHASES") != nullptr;
+  if (phases) {
+    if (!c->dPhase && (e = devAlloc(&c->dPhase, 8))) return e;
+    CK(cudaMemsetAsync(c->dPhase, 0, 8 * sizeof(unsigned long long), c->stream));
+    p.phaseCycles = c->dPhase;
+  }
   const int grid = gridFor<App>(c);
-  // BT_ROUND_LOG=1: one line per round on stderr (diagnostics).
-  FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
+  // BT_ROUND_LOG=1: one line per launch on stderr (diagnostics).
+  FILE* launchLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
   int launches = 0, passes = 0, retried = 0;
   const int32_t* list = nullptr;
   int n = R;
   Counters hc;
+  Ring hr;
   memset(&hc, 0, sizeof hc);
   for (int pass = 0;; ++pass) {
     p.budget = budget;
-    if (int64_t(budget) > c->capacity) {
-      setErr("a root needs more than %d live sub-beams (capacity %d)", budget / 16, c->capacity);
+    p.reserve = std::max(budget, 32);
+    if (int64_t(p.reserve) > c->capacity) {
+      setErr("a root needs more than %d live sub-beams (ring capacity %d)", budget / 16, c->capacity);
       return BT_ERR_CAPACITY;
     }
     p.numRoots = n;
     p.rootList = list;
-    if (pass == 0) {
-      CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
-    } else {
-      passResetKernel<<<1, 1, 0, c->stream>>>(c->dCtr);
-      launches++;
+    if (pass > 0) {
+      // per-pass state; output counts and the ring carry over
+      Counters z;
+      memset(&z, 0, sizeof z);
+      z.outCount = hc.outCount;
+      z.maxQueue = hc.maxQueue;
+      CK(cudaMemcpyAsync(c->dCtr, &z, sizeof z, cudaMemcpyHostToDevice, c->stream));
     }
     ++passes;
-    for (int cur = 0;; cur ^= 1) {
-      p.cur = cur;
+    for (int l = 0;; ++l) {
       CK(cudaEventRecord(c->rev[0], c->stream));
-      roundKernel<App><<<grid, kThreads, 0, c->stream>>>(p);
+      engineKernel<App><<<grid, kThreads, 0, c->stream>>>(p);
       CK(cudaEventRecord(c->rev[1], c->stream));
-      roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, cur, n);
-      launches += 2;
+      launches++;
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(&hr, c->dRing, sizeof hr, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
-      float roundMs = 0;
-      cudaEventElapsedTime(&roundMs, c->rev[0], c->rev[1]);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
       if (info) {
-        info->ms_round += roundMs;
+        info->ms_round += ms;
         info->round_launches++;
       }
-      if (roundLog)
-        fprintf(roundLog, "pass %d round %d produced %d inflight %d rootNext %d ms %.3f\n", pass, launches / 2,
-                hc.count[cur ^ 1], hc.inflight, hc.rootNext, roundMs);
-      if (hc.overflow) {
-        setErr("spill queue overflow (capacity %d)", c->capacity);
-        return BT_ERR_CAPACITY;
+      if (launchLog)
+        fprintf(launchLog, "pass %d launch %d inflight %d rootNext %d/%d ring %llu..%llu ms %.3f\n", pass, l,
+                hc.inflight, hc.rootNext, n, hr.head, hr.tail, ms);
+      if (hc.error) {
+        resetRing(c);
+        setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam ring wait exceeded its bound");
+        return BT_ERR_TIMEOUT;
       }
-      if (hc.done) break;
+      if (hc.rootNext >= n && hc.inflight == 0 && hr.head == hr.tail) break;
       if (launches > kMaxLaunches) {
-        setErr("round limit reached");
+        resetRing(c);
+        setErr("launch limit reached with %d roots in flight", hc.inflight);
         return BT_ERR_TIMEOUT;
       }
     }
-    if (info) info->max_spill = std::max(info->max_spill, hc.maxSpill);
+    if (info) info->max_spill = std::max(info->max_spill, hc.maxQueue);
     if (hc.killed == 0) break;
     if (pass >= c->cfg.max_retries) {
       setErr("%d roots still over budget %d after %d retries", hc.killed, budget, pass);
@@ -1095,6 +1347,16 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     list = dst;
     n = nk;
     budget *= 16;
+  }
+  if (phases) {
+    unsigned long long pc[8];
+    CK(cudaMemcpy(pc, c->dPhase, sizeof pc, cudaMemcpyDeviceToHost));
+    double tot = 0;
+    for (int k = 0; k < 7; ++k) tot += double(pc[k]);
+    const char* nm[7] = {"refill", "admit", "expand", "clip", "idle", "trace", "buffer"};
+    fprintf(stderr, "engine phases (%% of warp cycles, grid %d):", grid);
+    for (int k = 0; k < 7; ++k) fprintf(stderr, " %s %.1f", nm[k], 100.0 * double(pc[k]) / (tot + 1e-30));
+    fprintf(stderr, "\n");
   }
   if (info) {
     info->launches += launches;
@@ -1178,6 +1440,7 @@ int uploadScene(bt_gpu_ctx* c, const bt_scene_desc* sc, const bt_kd_desc* kd) {
     c->s.bounds.hi[a] = kd->bounds[3 + a];
   }
   c->s.numTris = int(nt);
+  c->s.numNodes = uint32_t(nn);
   c->numTris = nt;
   // offset = length(scene.bounds.diag()) * kEpsRel (render.cpp:348)
   V3 dg = mk(sc->bounds[3] - sc->bounds[0], sc->bounds[4] - sc->bounds[1], sc->bounds[5] - sc->bounds[2]);
@@ -1286,20 +1549,25 @@ int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu
   for (auto& ev : c->rev)
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   if ((e = uploadScene(c, scene, kd))) return fail(e);
-  // Spill queues: two of `capacity` 64-byte records.  Default: 2^25 records
-  // (2 GiB per queue), at most 10% of the free memory.
+  // Sub-beam ring: `capacity` 64-byte records (a power of two).  Default
+  // 2^24 (1 GiB), at most 10% of the free memory.
   int64_t cap = c->cfg.capacity;
   if (cap <= 0) {
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    cap = std::min<int64_t>(int64_t(1) << 25, int64_t(fr / 10 / (2 * sizeof(SubBeam))));
+    cap = std::min<int64_t>(int64_t(1) << 24, int64_t(fr / 10 / (sizeof(SubBeam) + 4)));
   }
   cap = std::max<int64_t>(cap, 1024);
   cap = std::min<int64_t>(cap, int64_t(1) << 30);
-  c->capacity = int(cap);
-  if ((e = devAlloc(&c->dQ[0], size_t(cap))) || (e = devAlloc(&c->dQ[1], size_t(cap))) ||
-      (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) || (e = devAlloc(&c->dKillCount, 1)))
+  int64_t pow2 = 1024;
+  while (pow2 * 2 <= cap) pow2 *= 2;
+  c->capacity = int(pow2);
+  if ((e = devAlloc(&c->dSlot, size_t(pow2))) || (e = devAlloc(&c->dSeq, size_t(pow2))) ||
+      (e = devAlloc(&c->dRing, 1)) || (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) ||
+      (e = devAlloc(&c->dKillCount, 1)))
     return fail(e);
+  if ((e = resetRing(c))) return fail(e);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(BT_ERR_CUDA);
   *out = c;
   return BT_OK;
 }
@@ -1308,9 +1576,9 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   if (!c) return BT_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dCtr, c->dStats,
+  void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dSlot, c->dSeq, c->dRing, c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
-                  c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
+                  c->dKillCount, c->dPhase, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu};
   for (void* q : ptrs)
     if (q) cudaFree(q);

@@ -38,6 +38,7 @@ struct SceneDev {
   const float4* triNV;
   Box bounds;
   int numTris;
+  uint32_t numNodes;
 };
 
 // A queued sub-beam: 64 bytes, self-contained (corners on the root's plane,
@@ -138,8 +139,8 @@ BT_HD void expand(const SceneDev& s, const Query& q, const SubBeam& r, Beam& b) 
     b.qx[i] = r.qx[i];
     b.qy[i] = r.qy[i];
   }
-  b.qx[3] = r.qx[l3];
-  b.qy[3] = r.qy[l3];
+  b.qx[3] = l3 == 3 ? r.qx[3] : r.qx[2];
+  b.qy[3] = l3 == 3 ? r.qy[3] : r.qy[2];
   b.n = n;
   b.neg = r.neg;
   beamAxes(q, b);
@@ -208,20 +209,17 @@ BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, 
         const bool pos = !((B.neg >> a) & 1);
         const float Ns = (pos ? 1.f : -1.f) * (sp - comp(q.P.O, a));
         const uint32_t left = r.node + 1, right = nd.y >> 2;
-        Box lbox = w.box, rbox = w.box;
-        lbox.hi[a] = sp;
-        rbox.lo[a] = sp;
         const uint32_t cs = pos ? right : left, co = pos ? left : right;
         int dec = kFar;
         if (Ns > 0) dec = decide(q, B, a, Ns, w.box);
-        if (dec == kFar) {
-          r.node = cs;
-          w.box = pos ? rbox : lbox;
-        } else {
-          if (dec == kBoth) r.trail |= 1ull << d;
-          r.node = co;
-          w.box = pos ? lbox : rbox;
-        }
+        // the child entered is the right one (lo[a] = split) or the left one (hi[a] = split)
+        const bool goRight = dec == kFar ? pos : !pos;
+        if (dec == kBoth) r.trail |= 1ull << d;
+        r.node = dec == kFar ? cs : co;
+        if (goRight)
+          boxSetLo(w.box, a, sp);
+        else
+          boxSetHi(w.box, a, sp);
       }
       r.cursor = 0;
       st.leafVisits++;
@@ -281,32 +279,87 @@ BT_COLD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti
 // Tests the pending triangle (wfTestOne, wavefront_core.h:236-268).
 // kStepFinished: AnyHit beam fully occluded by `occluder` (caller outputs
 // it); kStepSplit: triangle `cursor` needs a clip.
+BT_HD bool voteLine(const Query& q, const Beam& B, const Line& line, bool& allIn) {
+  bool anyIn = false, anyOut = false;
+  for (int k = 0; k < 4; ++k) {
+    float dv = B.qx[k] * line.a + B.qy[k] * line.b + line.c;
+    anyIn |= dv > q.eps;
+    anyOut |= dv < -q.eps;
+  }
+  if (anyOut) allIn = false;
+  return anyIn;
+}
+
+// The tests after the three edges (depth line, far plane, inside, beam side)
+// of BeamCtx::classifyTri (beam_core.h:386-408); ti holds the full setup.
+BT_HD int classifyAfterEdges(const Query& q, const Beam& B, const TriInfo& ti, bool allIn) {
+  if (q.mode == kModeNearest && B.hit >= 0) {
+    if (!voteLine(q, B, closerLine(q, ti, B.hitA, B.hitC, B.hitN, B.hit), allIn)) return kTriKeep;
+  }
+  if (q.farIsPlane) {
+    const float farA[3] = {0.f, 0.f, q.farCq};
+    if (!voteLine(q, B, closerLine(q, ti, farA, q.farCq, q.P.n, -1), allIn)) return kTriKeep;
+  }
+  if (allIn) return kTriAllIn;
+  if (separated(q, B, ti)) return kTriKeep;
+  return kTriClip;
+}
+
+BT_HD V3 edgePlane(const V3* r, const uint32_t* T, int i, int j) {
+  return T[i] < T[j] ? cross(r[i], r[j]) : neg(cross(r[j], r[i]));
+}
+
 BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats& st, int& occluder) {
   const uint2 leaf = s.node[r.node];
   const uint32_t i = uint32_t(r.cursor);
   r.cursor = int32_t(i + 1);
+  // Triangle setup as BeamCtx::triSetup (beam_core.h:260-286) computes it,
+  // but the edge lines one at a time: the test stops at the first edge that
+  // separates (trivial case (a), the usual outcome).  Every value is
+  // computed exactly as in the full setup, so outcomes are identical.
+  const TriRec t = loadRef(s, leaf.x + i);
   TriInfo ti;
-  setupRef(s, q, leaf.x + i, ti);
-  if (!ti.ok) return kStepContinue;
+  ti.tri = t.tri;
+  ti.r[0] = sub(t.v0, q.P.O);
+  ti.r[1] = sub(t.v1, q.P.O);
+  ti.r[2] = sub(t.v2, q.P.O);
+  const V3 m0 = edgePlane(ti.r, t.vi, 0, 1);
+  const float D = dot(ti.r[2], m0);
+  const float scale = length(m0) * length(ti.r[2]);
+  if (!((D < 0 ? -D : D) > kDegRel * scale)) return kStepContinue;  // edge-on: not a test
+  if (q.cull && D > 0) return kStepContinue;                        // back-facing
   st.triTests++;
-  const int t = ti.tri;
-  if (B.hit == t) return kStepContinue;
-  Line L[5];
-  int nl;
-  const int res = classifyTri(q, B, ti, L, nl);
+  if (B.hit == t.tri) return kStepContinue;
+  const float sg = D > 0 ? 1.f : -1.f;
+  bool allIn = true;
+  ti.edge[0] = makeLine(sg * dot(m0, q.P.u), sg * dot(m0, q.P.v), sg * dot(m0, q.P.d), q.ext);
+  if (!voteLine(q, B, ti.edge[0], allIn)) return kStepContinue;
+  const V3 m1 = edgePlane(ti.r, t.vi, 1, 2);
+  ti.edge[1] = makeLine(sg * dot(m1, q.P.u), sg * dot(m1, q.P.v), sg * dot(m1, q.P.d), q.ext);
+  if (!voteLine(q, B, ti.edge[1], allIn)) return kStepContinue;
+  const V3 m2 = edgePlane(ti.r, t.vi, 2, 0);
+  ti.edge[2] = makeLine(sg * dot(m2, q.P.u), sg * dot(m2, q.P.v), sg * dot(m2, q.P.d), q.ext);
+  if (!voteLine(q, B, ti.edge[2], allIn)) return kStepContinue;
+  ti.n = t.n;
+  ti.A[0] = dot(t.n, q.P.u);
+  ti.A[1] = dot(t.n, q.P.v);
+  ti.A[2] = dot(t.n, q.P.d);
+  ti.C = dot(t.n, ti.r[0]);
+  ti.ok = 1;
+  const int res = classifyAfterEdges(q, B, ti, allIn);
   if (res == kTriKeep) return kStepContinue;
   if (res == kTriAllIn) {
     if (q.mode == kModeAnyHit) {
-      occluder = t;
+      occluder = t.tri;
       return kStepFinished;
     }
-    setStatus(q, B, t, ti.A, ti.C);
+    setStatus(q, B, t.tri, ti.A, ti.C);
     B.hitA[0] = ti.A[0];
     B.hitA[1] = ti.A[1];
     B.hitA[2] = ti.A[2];
     B.hitC = ti.C;
     B.hitN = ti.n;
-    r.hit = t;
+    r.hit = t.tri;
     return kStepContinue;
   }
   r.cursor = int32_t(i);

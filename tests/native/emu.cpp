@@ -201,6 +201,7 @@ EMU_API void* emu_create(const bt_scene_desc* sc, const bt_kd_desc* kd) {
     e->s.bounds.hi[a] = kd->bounds[3 + a];
   }
   e->s.numTris = int(nt);
+  e->s.numNodes = uint32_t(nn);
   return e;
 }
 
