@@ -66,25 +66,22 @@ enum Phase { kIdle = 0, kLoaded = 1, kTrace = 2, kSplit = 3 };
 
 // Engine state shared by all warps of a pass.
 struct __align__(128) Counters {
-  unsigned long long reserved;  // ring slots reserved by roots in flight
+  unsigned long long reserved;  // queue slots reserved by roots in flight
   int rootNext;                 // next entry of the root list to admit
   int inflight;                 // admitted roots not finished
   int killed;                   // roots abandoned in this pass
-  int error;                    // a bounded ring wait gave up (the ring is reset)
+  int error;                    // a queue append found no slot (impossible by the reservation rule)
   int outCount;                 // output polygons
-  int maxQueue;                 // ring occupancy high-water mark (sampled)
-};
-
-// The sub-beam ring: positions are monotonic 64-bit counters; slot
-// pos & mask holds position pos once seq[slot] == pos + 1 (published), and
-// is free for position pos + capacity once seq[slot] == pos + capacity.
-// head and tail sit on separate 128-byte lines: consumers (CAS on head) and
-// producers (atomicAdd on tail) do not contend for one L2 line.
-struct Ring {
-  unsigned long long head;  // next position to take
-  unsigned long long pad0[15];
-  unsigned long long tail;  // next position to fill
-  unsigned long long pad1[15];
+  int maxQueue;                 // largest trace queue
+  int done;                     // set by roundEnd: every root of the pass is done
+  int rounds;
+  int pad0[6];
+  int count[2];                 // records in trace queue 0 / 1
+  int head;                     // fetch cursor of the trace queue being drained
+  int pad1[13];
+  int clipCount;                // records waiting for a clip
+  int clipHead;                 // fetch cursor of the clip queue
+  int pad2[14];
 };
 
 // Per-root query: plane, tolerances, mode (WfRoot, cuda/wavefront.cu:80-86).
@@ -131,13 +128,12 @@ struct AppParams {
 
 struct RoundParams {
   SceneDev s;
-  SubBeam* slot;
-  uint32_t* seq;
-  Ring* ring;
-  unsigned long long mask;
+  SubBeam* tq[2];  // trace queues: round r drains tq[r & 1], its clips fill tq[(r + 1) & 1]
+  SubBeam* cq;     // clip queue of the round
+  int cur;
   int capacity;
   int budget;
-  int reserve;  // ring slots reserved per root: max(budget, 32) (a root's pre-split pieces always fit)
+  int reserve;  // queue slots reserved per root: max(budget, 32) (a root's pre-split pieces always fit)
   int numRoots;
   int rootCap;  // size of the per-root arrays
   const int32_t* rootList;
@@ -147,8 +143,7 @@ struct RoundParams {
   int32_t* attempt;
   Counters* ctr;
   unsigned long long* stats;
-  int splitBatch;
-  unsigned long long* phaseCycles;  // optional: warp cycles per engine phase (diagnostics)
+  unsigned long long* phaseCycles;  // optional: warp cycles per trace-loop phase (diagnostics)
   AppParams app;
 };
 
@@ -280,60 +275,19 @@ __device__ __forceinline__ void outputPiece(const RoundParams& p, const Query& q
   outputPieceCold<App>(p, &o);
 }
 
-constexpr int kWaitLimit = 1 << 18;  // polls of one ring slot before the engine reports an error
-
-// Bounded wait for a ring slot's sequence number.  The waits are short by
-// construction (a producer's slot was already taken by the previous lap's
-// consumer; a consumer's slot was already reserved by its producer), so
-// running out means an engine fault: the error flag ends the pass.
-__device__ __forceinline__ bool ringWait(const RoundParams& p, uint32_t idx, uint32_t want) {
-  for (int i = 0; i < kWaitLimit; ++i) {
-    if (__ldcv(&p.seq[idx]) == want) return true;
-    if ((i & 255) == 255 && __ldcv(&p.ctr->error)) return false;
-    __nanosleep(i < 32 ? 32 : 256);
+// Appends n records to trace queue `q` (one atomic); returns the first slot
+// or -1 (and flags an error) if they do not fit, which the reservation rule
+// rules out.
+__device__ __forceinline__ int queueAppend(const RoundParams& p, int q, int n) {
+  const int at = atomicAdd(&p.ctr->count[q], n);
+  if (at + n > p.capacity) {
+    atomicExch(&p.ctr->error, 1);
+    return -1;
   }
-  atomicExch(&p.ctr->error, 1);
-  return false;
+  return at;
 }
 
-// Fills ring position `pos` with record r and publishes it.
-__device__ __forceinline__ void ringPut(const RoundParams& p, unsigned long long pos, const SubBeam& r) {
-  const uint32_t idx = uint32_t(pos & p.mask);
-  if (!ringWait(p, idx, uint32_t(pos))) return;
-  p.slot[idx] = r;
-  __threadfence();
-  atomicExch(&p.seq[idx], uint32_t(pos + 1));
-}
-
-// Takes ring position `pos` (claimed by the caller), bypassing L1 (slots are
-// rewritten by other SMs), and frees the slot for the next lap.
-__device__ __forceinline__ bool ringGet(const RoundParams& p, unsigned long long pos, SubBeam& r) {
-  const uint32_t idx = uint32_t(pos & p.mask);
-  if (!ringWait(p, idx, uint32_t(pos + 1))) return false;
-  __threadfence();
-  const float4* src = reinterpret_cast<const float4*>(&p.slot[idx]);
-  float4 v[4];
-  for (int i = 0; i < 4; ++i) v[i] = __ldcg(src + i);
-  memcpy(&r, v, sizeof(SubBeam));
-  __threadfence();
-  atomicExch(&p.seq[idx], uint32_t(pos + (unsigned long long)p.capacity));
-  return true;
-}
-
-// Claims up to `want` published-or-reserved positions for a warp (lane 0);
-// returns how many, from position h.
-__device__ __forceinline__ int ringClaim(const RoundParams& p, int want, unsigned long long& h) {
-  for (int tries = 0; tries < 64; ++tries) {
-    h = __ldcv(&p.ring->head);
-    const unsigned long long t = __ldcv(&p.ring->tail);
-    if (h >= t) return 0;
-    const int n = int(min((unsigned long long)want, t - h));
-    if (atomicCAS(&p.ring->head, h, h + n) == h) return n;
-  }
-  return 0;
-}
-
-// Admission: the root's first piece stays in the lane, the others go to the ring.
+// Admission: every pre-split piece goes to the round's trace queue.
 template <int App>
 struct AdmitEnv {
   const RoundParams* p;
@@ -341,28 +295,21 @@ struct AdmitEnv {
   float lightArea;
   int root;
   Stats* st;
-  SubBeam first;
-  int haveFirst;
   int queued;
   __device__ bool queue(const SubBeam& r) {
     ++queued;
-    if (!haveFirst) {
-      first = r;
-      haveFirst = 1;
-      return true;
-    }
-    ringPut(*p, atomicAdd(&p->ring->tail, 1ull), r);
-    return true;
+    const int at = queueAppend(*p, p->cur, 1);
+    if (at >= 0) p->tq[p->cur][at] = r;
+    return at >= 0;
   }
   __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
   __device__ void missed(const Beam& b) { outputPiece<App>(*p, *q, lightArea, root, b, -1, *st); }
   __device__ void dropped(float) {}
 };
 
-// Clip emission: pieces collect in chunks of kChunk and each full chunk is
-// written to ring positions reserved only when its records are ready, so
-// consumers never wait on a clip in progress (wfSplitEmit,
-// wavefront_core.h:367-422).
+// Clip emission into the next round's trace queue: pieces collect in chunks
+// of kChunk, each chunk appended with one atomic, so siblings stay adjacent
+// (wfSplitEmit, wavefront_core.h:367-422).
 constexpr int kChunk = 8;
 template <int App>
 struct SplitEnv {
@@ -376,12 +323,10 @@ struct SplitEnv {
   SubBeam buf[kChunk];
   __device__ void flush() {
     if (nbuf == 0) return;
-    const unsigned long long pos = atomicAdd(&p->ring->tail, (unsigned long long)nbuf);
-    for (int i = 0; i < nbuf; ++i) ringPut(*p, pos + (unsigned long long)i, buf[i]);
-    if ((pos & 63) < (unsigned long long)nbuf) {
-      const unsigned long long hd = __ldcv(&p->ring->head), end = pos + (unsigned long long)nbuf;
-      if (end > hd) atomicMax(&p->ctr->maxQueue, int(min(end - hd, 0x7fffffffull)));
-    }
+    const int nxt = p->cur ^ 1;
+    const int at = queueAppend(*p, nxt, nbuf);
+    if (at >= 0)
+      for (int i = 0; i < nbuf; ++i) p->tq[nxt][at + i] = buf[i];
     written += nbuf;
     nbuf = 0;
   }
@@ -410,20 +355,18 @@ __device__ __forceinline__ bool softPixel(const AppParams& a, int k, int& pix) {
 // What admission hands back to the lane (a temporary: the lane's own state
 // stays in registers).
 struct AdmitOut {
-  SubBeam first;
   Query q;
   float lightArea;
   Stats st;
 };
 
 // Sets up root k and queues its pre-split pieces (admitRoot,
-// cuda/wavefront.cu:255-325).  Returns true if the lane took a piece.
+// cuda/wavefront.cu:255-325).
 template <int App>
 __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   Query& q = out->q;
   float& lightArea = out->lightArea;
   Stats& st = out->st;
-  SubBeam& first = out->first;
   p.live[k] = 0;
   p.state[k] = kRootNone;
   const int att = p.attempt[k] + 1;
@@ -501,20 +444,12 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   querySetup(q, poly.extent());
   storeRoot(&p.roots[k], q, lightArea, att);
   p.state[k] = kRootTraced;
-  // Pieces reach the ring as they are made and other warps may finish them
-  // at once: hold the live count up until all pieces are counted.
-  constexpr int kHold = 1 << 20;
-  p.live[k] = kHold;
-  AdmitEnv<App> env{&p, &q, lightArea, k, &st, SubBeam(), 0, 0};
+  AdmitEnv<App> env{&p, &q, lightArea, k, &st, 0};
   const bool ok = admitRoot(p.s, q, poly, k, env, st);
+  p.live[k] = env.queued;  // the pieces are traced by a later kernel
   if (!ok || env.queued > p.budget) killRoot(p, k);
-  const int before = atomicSub(&p.live[k], kHold - env.queued);
-  if (before - (kHold - env.queued) == 0) {
-    rootDone(p);  // no piece left (none made, or all finished already)
-    return false;
-  }
-  if (env.haveFirst) first = env.first;
-  return env.haveFirst != 0;
+  if (env.queued == 0) rootDone(p);
+  return env.queued > 0;
 }
 
 __device__ __forceinline__ void addStats(Stats& a, const Stats& b) {
@@ -598,28 +533,62 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   return false;
 }
 
-constexpr int kSplitBuf = 64;   // per warp: records waiting for a clip
-constexpr int kIdleWaits = 400;  // sleeps (up to 33 us each) of an idle warp waiting for work before it leaves the launch
+// ---- round kernels ------------------------------------------------------
 
-// The persistent engine.  Lanes take records from the ring (one claim per
-// warp for all idle lanes), then admit new roots; each lane traces its
-// record leaf by leaf until it finishes or a triangle needs a clip.  Records
-// that need a clip wait in a per-warp buffer in shared memory; when 32 wait
-// (or the warp has nothing left to trace) the warp parks its tracing lanes'
-// records in shared memory and clips 32 records with all lanes at once, then
-// resumes.  Pieces go to the ring, where any warp takes them: no rounds, no
-// tail of a round, every warp works on every root.
+// Admission: each lane sets up one root (claimed per warp under the queue
+// reservation) and queues its pieces in the round's trace queue.  Roots that
+// do not fit wait for a later round.
 template <int App>
-__global__ void __launch_bounds__(kThreads) engineKernel(const __grid_constant__ RoundParams p) {
-  __shared__ SubBeam sSplit[kWarps][kSplitBuf];
-  __shared__ SubBeam sPark[kWarps][32];
-  __shared__ int sCnt[kWarps];
-  const int lane = laneId(), wid = threadIdx.x >> 5;
+__global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ RoundParams p) {
+  const int lane = laneId();
+  Stats st;
+  st.clear();
+  for (;;) {
+    if (__ldcv(&p.ctr->done)) break;
+    int base = -1, fit = 0;
+    if (lane == 0) {
+      const unsigned long long res = (unsigned long long)p.reserve, cap = (unsigned long long)p.capacity;
+      const unsigned long long need = 32ull * res;
+      const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
+      fit = 32;
+      if (old + need > cap) {
+        fit = old >= cap ? 0 : int(min(32ull, (cap - old) / res));
+        atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(32 - fit)) * res);
+      }
+      if (fit > 0) {
+        base = atomicAdd(&p.ctr->rootNext, fit);
+        const int got = max(0, min(fit, p.numRoots - base));
+        if (got < fit) atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(fit - got)) * res);
+        if (got > 0) atomicAdd(&p.ctr->inflight, got);
+        fit = got;
+      }
+    }
+    base = __shfl_sync(kFull, base, 0);
+    fit = __shfl_sync(kFull, fit, 0);
+    if (fit <= 0) break;  // queues full or every root claimed
+    if (lane < fit) {
+      const int j = base + lane;
+      const int k = p.rootList ? p.rootList[j] : j;
+      AdmitOut ao;
+      ao.st.clear();
+      admit<App>(p, k, &ao);
+      addStats(st, ao.st);
+    }
+  }
+  flushStats(p, st);
+}
+
+// Trace: persistent warps drain the round's queue.  Each lane traces its
+// record leaf by leaf until it finishes or a triangle needs a clip; idle
+// lanes are refilled at once (one atomic per warp, ballot/popc ranks).
+// Records needing a clip are compacted into the clip queue.
+template <int App>
+__global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ RoundParams p) {
+  const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
-  if (lane == 0) sCnt[wid] = 0;
-  __syncwarp();
-  bool rootsDone = false;
-  int admitWait = 0, waits = 0;
+  const int nCur = min(p.ctr->count[p.cur], p.capacity);
+  const SubBeam* queue = p.tq[p.cur];
+  bool exhausted = nCur == 0;
   int phase = kIdle;
   SubBeam r;
   Beam b;
@@ -629,162 +598,46 @@ __global__ void __launch_bounds__(kThreads) engineKernel(const __grid_constant__
   int qRoot = -1;
   Stats st;
   st.clear();
-  // optional phase accounting: refill, admit, expand, clip, idle, trace, buffer
-  unsigned long long pc[7] = {0, 0, 0, 0, 0, 0, 0};
+  unsigned long long pc[4] = {0, 0, 0, 0};  // refill, trace, append, idle (optional accounting)
   long long tprev = p.phaseCycles ? clock64() : 0;
-#define BT_PHASE(k)                         \
-  if (p.phaseCycles) {                      \
-    const long long t_ = clock64();         \
-    pc[k] += (unsigned long long)(t_ - tprev); \
-    tprev = t_;                             \
+#define BT_PHASE(k)                              \
+  if (p.phaseCycles) {                           \
+    const long long t_ = clock64();              \
+    pc[k] += (unsigned long long)(t_ - tprev);   \
+    tprev = t_;                                  \
   }
   for (;;) {
-    // ---- refill idle lanes: the ring, then new roots
-    unsigned idle = __ballot_sync(kFull, phase == kIdle);
-    if (idle) {
-      unsigned long long h = 0;
-      int n = 0;
-      if (lane == 0) n = ringClaim(p, __popc(idle), h);
-      n = __shfl_sync(kFull, n, 0);
-      h = __shfl_sync(kFull, h, 0);
-      const int rank = __popc(idle & ltMask);
-      if (phase == kIdle && rank < n) {
-        if (ringGet(p, h + (unsigned long long)rank, r)) phase = kLoaded;
+    const unsigned idle = __ballot_sync(kFull, phase == kIdle);
+    if (idle && !exhausted) {
+      const int ni = __popc(idle);
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&p.ctr->head, ni);
+      base = __shfl_sync(kFull, base, 0);
+      if (base + ni >= nCur) exhausted = true;
+      const int i = base + __popc(idle & ltMask);
+      if (phase == kIdle && i < nCur) {
+        r = queue[i];
+        if (uint32_t(r.root) >= uint32_t(p.rootCap) || r.node >= p.s.numNodes || r.n > 4) {
+          atomicExch(&p.ctr->error, 2);  // a malformed record: report, never index with it
+        } else if (r.n == 0 || p.state[r.root] == kRootKilled) {
+          liveSub(p, r.root, 1);  // a dropped sliver or an abandoned root
+        } else {
+          if (r.root != qRoot) {
+            loadRoot(&p.roots[r.root], q, lightArea);
+            qRoot = r.root;
+          }
+          expand(p.s, q, r, b);
+          walkBegin(p.s, r, w);
+          phase = kTrace;
+        }
       }
-      idle = __ballot_sync(kFull, phase == kIdle);
     }
     BT_PHASE(0)
-    if (idle && !rootsDone && admitWait > 0) {
-      --admitWait;
-    } else if (idle && !rootsDone) {
-      // Reserve ring slots for each root taken; take only as many roots as fit.
-      const int ni = __popc(idle);
-      int base = -1, fit = 0;
-      if (lane == 0) {
-        const unsigned long long res = (unsigned long long)p.reserve, cap = (unsigned long long)p.capacity;
-        const unsigned long long need = (unsigned long long)ni * res;
-        const unsigned long long old = atomicAdd(&p.ctr->reserved, need);
-        fit = ni;
-        if (old + need > cap) {
-          fit = old >= cap ? 0 : int(min((unsigned long long)ni, (cap - old) / res));
-          atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(ni - fit)) * res);
-        }
-        if (fit > 0) {
-          base = atomicAdd(&p.ctr->rootNext, fit);
-          const int got = max(0, min(fit, p.numRoots - base));
-          if (got < fit) atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)(fit - got)) * res);
-          if (got > 0) atomicAdd(&p.ctr->inflight, got);
-        }
-      }
-      base = __shfl_sync(kFull, base, 0);
-      fit = __shfl_sync(kFull, fit, 0);
-      if (fit == 0) {
-        admitWait = 8;  // the ring is fully reserved: retry later
-      } else if (base + fit >= p.numRoots) {
-        rootsDone = true;
-      }
-      const int rank = __popc(idle & ltMask);
-      const int j = base + rank;
-      if (fit > 0 && rank < fit && phase == kIdle && j < p.numRoots) {
-        const int k = p.rootList ? p.rootList[j] : j;
-        AdmitOut ao;
-        ao.st.clear();
-        if (admit<App>(p, k, &ao)) {
-          r = ao.first;
-          q = ao.q;
-          lightArea = ao.lightArea;
-          qRoot = k;
-          phase = kLoaded;
-        }
-        addStats(st, ao.st);
-      }
-    }
-    BT_PHASE(1)
-    // ---- expand newly loaded records (holes and abandoned roots are dropped)
-    if (phase == kLoaded) {
-      if (uint32_t(r.root) >= uint32_t(p.rootCap) || r.node >= p.s.numNodes || r.n > 4) {
-        atomicExch(&p.ctr->error, 2);  // a malformed record: report, never index with it
-        phase = kIdle;
-      } else if (r.n == 0 || p.state[r.root] == kRootKilled) {
-        liveSub(p, r.root, 1);
-        phase = kIdle;
-      } else {
-        if (r.root != qRoot) {
-          loadRoot(&p.roots[r.root], q, lightArea);
-          qRoot = r.root;
-        }
-        expand(p.s, q, r, b);
-        walkBegin(p.s, r, w);
-        phase = kTrace;
-      }
-    }
-    const unsigned tr = __ballot_sync(kFull, phase == kTrace);
-    const unsigned idleNow = __ballot_sync(kFull, phase == kIdle);
-    __syncwarp();
-    const int cnt = sCnt[wid];
-    BT_PHASE(2)
-    if (cnt >= p.splitBatch || (cnt > 0 && (!tr || idleNow))) {
-      // ---- clip: park the tracing lanes, clip up to 32 buffered records
-      const bool parked = phase == kTrace;
-      if (parked) sPark[wid][lane] = r;
-      const int m = min(32, cnt);
-      const bool mine = lane < m;
-      SubBeam* recp = &sSplit[wid][cnt - m + (mine ? lane : 0)];
-      bool cont = false;
-      if (mine) {
-        Stats cs;
-        cs.clear();
-        cont = clipRecord<App>(p, recp, &cs);
-        addStats(st, cs);
-      }
-      SubBeam rec;
-      if (cont) rec = *recp;
-      __syncwarp();
-      if (lane == 0) sCnt[wid] = cnt - m;
-      __syncwarp();
-      if (parked) {
-        if (cont) ringPut(p, atomicAdd(&p.ring->tail, 1ull), rec);  // nothing changed: back to the ring
-        r = sPark[wid][lane];
-      } else if (cont) {
-        r = rec;
-      }
-      if (parked || cont) {
-        if (r.root != qRoot) {
-          loadRoot(&p.roots[r.root], q, lightArea);
-          qRoot = r.root;
-        }
-        expand(p.s, q, r, b);
-        walkBegin(p.s, r, w);
-        phase = kTrace;
-      } else {
-        phase = kIdle;
-      }
-      waits = 0;
-      BT_PHASE(3)
+    if (!__any_sync(kFull, phase == kTrace)) {
+      if (exhausted) break;
       continue;
     }
-    if (!tr) {
-      // Nothing to trace or clip in this warp: leave when every root is done,
-      // else wait (bounded) for pieces from other warps.  Lane 0 reads the
-      // shared counters and the warp decides as one (every lane must reach
-      // the same warp-wide intrinsics).
-      int flags = 0;
-      if (lane == 0) {
-        const unsigned long long hd = __ldcv(&p.ring->head), tl = __ldcv(&p.ring->tail);
-        flags = (__ldcv(&p.ctr->error) ? 1 : 0) | (hd >= tl ? 2 : 0) | (__ldcv(&p.ctr->inflight) == 0 ? 4 : 0);
-      }
-      flags = __shfl_sync(kFull, flags, 0);
-      if (flags & 1) break;
-      if ((rootsDone || admitWait > 0) && (flags & 2)) {
-        if (rootsDone && (flags & 4)) break;
-        if (++waits > kIdleWaits) break;
-        __nanosleep(waits < 8 ? 256u << waits : 32768u);  // back off: idle warps must not crowd the ring's lines
-      }
-      BT_PHASE(4)
-      continue;
-    }
-    waits = 0;
-    // ---- trace one leaf: climb / descend to it, then test its triangles
+    // one leaf: climb / descend to it, then test its triangles
     int res = kStepContinue;
     if (phase == kTrace) {
       res = advance(p.s, q, b, r, w, st);
@@ -801,32 +654,65 @@ __global__ void __launch_bounds__(kThreads) engineKernel(const __grid_constant__
         phase = kIdle;
       }
     }
-    BT_PHASE(5)
-    // records that need a clip join the warp's clip buffer
-    const unsigned spl = __ballot_sync(kFull, phase == kTrace && res == kStepSplit);
-    if (spl) {
-      const int c0 = sCnt[wid];
+    BT_PHASE(1)
+    const unsigned clip = __ballot_sync(kFull, phase == kTrace && res == kStepSplit);
+    if (clip) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&p.ctr->clipCount, __popc(clip));
+      base = __shfl_sync(kFull, base, 0);
       if (phase == kTrace && res == kStepSplit) {
-        sSplit[wid][c0 + __popc(spl & ltMask)] = r;
+        p.cq[base + __popc(clip & ltMask)] = r;  // (r's corners are the beam's)
         phase = kIdle;
       }
-      __syncwarp();
-      if (lane == 0) sCnt[wid] = c0 + __popc(spl);
-      __syncwarp();
     }
-    BT_PHASE(6)
+    BT_PHASE(2)
   }
 #undef BT_PHASE
   if (p.phaseCycles && lane == 0)
-    for (int k = 0; k < 7; ++k) atomicAdd(&p.phaseCycles[k], pc[k]);
+    for (int k = 0; k < 3; ++k) atomicAdd(&p.phaseCycles[k], pc[k]);
   flushStats(p, st);
 }
 
-// Sets every ring slot free for its first lap (seq[i] = i).
-__global__ void ringInitKernel(uint32_t* seq, int cap, Ring* ring) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < cap) seq[i] = uint32_t(i);
-  if (i == 0) ring->head = ring->tail = 0;
+// Clip: one lane per record of the clip queue; pieces go to the next
+// round's trace queue.  A record whose clip changes nothing measurable
+// continues at its next triangle in the next round.
+template <int App>
+__global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ RoundParams p) {
+  const int lane = laneId();
+  const int n = min(p.ctr->clipCount, p.capacity);
+  Stats st;
+  st.clear();
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&p.ctr->clipHead, 32);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      SubBeam rec = p.cq[i];
+      Stats cs;
+      cs.clear();
+      if (clipRecord<App>(p, &rec, &cs)) {
+        const int at = queueAppend(p, p.cur ^ 1, 1);
+        if (at >= 0) p.tq[p.cur ^ 1][at] = rec;
+      }
+      addStats(st, cs);
+    }
+  }
+  flushStats(p, st);
+}
+
+// Between rounds: the drained queues are emptied, completion is decided
+// (scheduleKernel's bookkeeping, cuda/wavefront.cu:327-345).
+__global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
+  const int nxt = cur ^ 1;
+  if (c->count[nxt] > c->maxQueue) c->maxQueue = c->count[nxt];
+  c->count[cur] = 0;
+  c->head = 0;
+  c->clipCount = 0;
+  c->clipHead = 0;
+  c->rounds++;
+  c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
 }
 
 // Roots abandoned in a pass, compacted for the retry pass.
@@ -1075,10 +961,8 @@ struct bt_gpu_ctx {
   float offset = 0;  // |scene diagonal| * kEpsRel
   int64_t numTris = 0;
   // engine
-  SubBeam* dSlot = nullptr;  // sub-beam ring: capacity records
-  uint32_t* dSeq = nullptr;   // per-slot sequence numbers
-  Ring* dRing = nullptr;
-  int capacity = 0;           // power of two
+  SubBeam* dQ[3] = {nullptr, nullptr, nullptr};  // trace queues 0, 1 and the clip queue
+  int capacity = 0;
   Counters* dCtr = nullptr;
   unsigned long long* dStats = nullptr;
   size_t rootCap = 0;
@@ -1197,11 +1081,11 @@ int ensurePix(bt_gpu_ctx* c, int64_t n) {
   return BT_OK;
 }
 
-template <int App>
-int gridFor(bt_gpu_ctx* c) {
+template <class K>
+int gridFor(bt_gpu_ctx* c, K kernel) {
   int perSM = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, engineKernel<App>, kThreads, 0);
-  if (c->cfg.blocks_per_sm > 0) perSM = c->cfg.blocks_per_sm;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, 0);
+  if (c->cfg.blocks_per_sm > 0) perSM = std::min(perSM, c->cfg.blocks_per_sm);
   return c->sms * std::max(1, perSM);
 }
 
@@ -1229,15 +1113,15 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
 
 // Runs every root of `R` through the engine: passes of launches until all
 // roots are done; roots abandoned over budget are retried with 16x budget.
-int resetRing(bt_gpu_ctx* c) {
-  ringInitKernel<<<(c->capacity + 255) / 256, 256, 0, c->stream>>>(c->dSeq, c->capacity, c->dRing);
-  CK(cudaGetLastError());
-  return BT_OK;
-}
+// Runs every root of `R` through the engine.  A round is three kernels --
+// admit (new roots, as far as the queue reservation allows), trace (drain
+// the round's queue), clip (pieces into the next round's queue) -- plus the
+// bookkeeping kernel; rounds are launched in batches of kRoundsPerCheck
+// between reads of the completion flag (rounds after completion return at
+// once).  Roots abandoned over budget are retried in a further pass with a
+// 16x budget.
+constexpr int kRoundsPerCheck = 8;
 
-// Runs every root of `R` through the engine: launches of the persistent
-// kernel until all roots are done (one launch unless idle warps left early);
-// roots abandoned over budget are retried in a further pass with 16x budget.
 template <int App>
 int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info) {
   int e = ensureRoots(c, size_t(R));
@@ -1250,11 +1134,10 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   app.shade = c->dShade;
   RoundParams p;
   p.s = c->s;
-  p.slot = c->dSlot;
-  p.seq = c->dSeq;
-  p.ring = c->dRing;
+  p.tq[0] = c->dQ[0];
+  p.tq[1] = c->dQ[1];
+  p.cq = c->dQ[2];
   p.capacity = c->capacity;
-  p.mask = (unsigned long long)(c->capacity - 1);
   p.roots = c->dRoots;
   p.rootCap = R;
   p.live = c->dLive;
@@ -1262,36 +1145,34 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.attempt = c->dAttempt;
   p.ctr = c->dCtr;
   p.stats = c->dStats;
-  p.splitBatch = std::max(1, std::min(32, c->cfg.split_batch));
   p.app = app;
   p.phaseCycles = nullptr;
-  // BT_PHASES=1: warp cycles per engine phase on stderr (diagnostics).
+  // BT_PHASES=1: warp cycles per trace-loop phase on stderr (diagnostics).
   const bool phases = getenv("BT_PHASES") != nullptr;
   if (phases) {
     if (!c->dPhase && (e = devAlloc(&c->dPhase, 8))) return e;
     CK(cudaMemsetAsync(c->dPhase, 0, 8 * sizeof(unsigned long long), c->stream));
     p.phaseCycles = c->dPhase;
   }
-  const int grid = gridFor<App>(c);
-  // BT_ROUND_LOG=1: one line per launch on stderr (diagnostics).
-  FILE* launchLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
+  const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App>), gC = gridFor(c, clipKernel<App>);
+  // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
+  FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
   int launches = 0, passes = 0, retried = 0;
   const int32_t* list = nullptr;
   int n = R;
   Counters hc;
-  Ring hr;
   memset(&hc, 0, sizeof hc);
   for (int pass = 0;; ++pass) {
     p.budget = budget;
     p.reserve = std::max(budget, 32);
     if (int64_t(p.reserve) > c->capacity) {
-      setErr("a root needs more than %d live sub-beams (ring capacity %d)", budget / 16, c->capacity);
+      setErr("a root needs more than %d live sub-beams (queue capacity %d)", budget / 16, c->capacity);
       return BT_ERR_CAPACITY;
     }
     p.numRoots = n;
     p.rootList = list;
     if (pass > 0) {
-      // per-pass state; output counts and the ring carry over
+      // per-pass state; the output count carries over
       Counters z;
       memset(&z, 0, sizeof z);
       z.outCount = hc.outCount;
@@ -1299,32 +1180,35 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       CK(cudaMemcpyAsync(c->dCtr, &z, sizeof z, cudaMemcpyHostToDevice, c->stream));
     }
     ++passes;
-    for (int l = 0;; ++l) {
+    for (int round = 0;;) {
       CK(cudaEventRecord(c->rev[0], c->stream));
-      engineKernel<App><<<grid, kThreads, 0, c->stream>>>(p);
+      for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
+        p.cur = round & 1;
+        admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
+        traceKernel<App><<<gT, kThreads, 0, c->stream>>>(p);
+        clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
+        roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
+        launches += 4;
+      }
       CK(cudaEventRecord(c->rev[1], c->stream));
-      launches++;
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaMemcpyAsync(&hr, c->dRing, sizeof hr, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
       float ms = 0;
       cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
       if (info) {
         info->ms_round += ms;
-        info->round_launches++;
+        info->round_launches += 3 * kRoundsPerCheck;
       }
-      if (launchLog)
-        fprintf(launchLog, "pass %d launch %d inflight %d rootNext %d/%d ring %llu..%llu ms %.3f\n", pass, l,
-                hc.inflight, hc.rootNext, n, hr.head, hr.tail, ms);
+      if (roundLog)
+        fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d ms %.3f\n", pass, hc.rounds,
+                hc.inflight, hc.rootNext, n, hc.count[round & 1], ms);
       if (hc.error) {
-        resetRing(c);
-        setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam ring wait exceeded its bound");
-        return BT_ERR_TIMEOUT;
+        setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam queue overflow (capacity %d)", c->capacity);
+        return BT_ERR_CAPACITY;
       }
-      if (hc.rootNext >= n && hc.inflight == 0 && hr.head == hr.tail) break;
+      if (hc.done) break;
       if (launches > kMaxLaunches) {
-        resetRing(c);
         setErr("launch limit reached with %d roots in flight", hc.inflight);
         return BT_ERR_TIMEOUT;
       }
@@ -1351,12 +1235,9 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   if (phases) {
     unsigned long long pc[8];
     CK(cudaMemcpy(pc, c->dPhase, sizeof pc, cudaMemcpyDeviceToHost));
-    double tot = 0;
-    for (int k = 0; k < 7; ++k) tot += double(pc[k]);
-    const char* nm[7] = {"refill", "admit", "expand", "clip", "idle", "trace", "buffer"};
-    fprintf(stderr, "engine phases (%% of warp cycles, grid %d):", grid);
-    for (int k = 0; k < 7; ++k) fprintf(stderr, " %s %.1f", nm[k], 100.0 * double(pc[k]) / (tot + 1e-30));
-    fprintf(stderr, "\n");
+    double tot = double(pc[0] + pc[1] + pc[2]) + 1e-30;
+    fprintf(stderr, "trace loop (%% of warp cycles): refill %.1f trace %.1f append %.1f\n", 100.0 * pc[0] / tot,
+            100.0 * pc[1] / tot, 100.0 * pc[2] / tot);
   }
   if (info) {
     info->launches += launches;
@@ -1549,25 +1430,21 @@ int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu
   for (auto& ev : c->rev)
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   if ((e = uploadScene(c, scene, kd))) return fail(e);
-  // Sub-beam ring: `capacity` 64-byte records (a power of two).  Default
-  // 2^24 (1 GiB), at most 10% of the free memory.
+  // Sub-beam queues: three of `capacity` 64-byte records.  Default 2^23
+  // records (512 MiB each), at most 10% of the free memory.
   int64_t cap = c->cfg.capacity;
   if (cap <= 0) {
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    cap = std::min<int64_t>(int64_t(1) << 24, int64_t(fr / 10 / (sizeof(SubBeam) + 4)));
+    cap = std::min<int64_t>(int64_t(1) << 23, int64_t(fr / 10 / (3 * sizeof(SubBeam))));
   }
   cap = std::max<int64_t>(cap, 1024);
   cap = std::min<int64_t>(cap, int64_t(1) << 30);
-  int64_t pow2 = 1024;
-  while (pow2 * 2 <= cap) pow2 *= 2;
-  c->capacity = int(pow2);
-  if ((e = devAlloc(&c->dSlot, size_t(pow2))) || (e = devAlloc(&c->dSeq, size_t(pow2))) ||
-      (e = devAlloc(&c->dRing, 1)) || (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) ||
+  c->capacity = int(cap);
+  if ((e = devAlloc(&c->dQ[0], size_t(cap))) || (e = devAlloc(&c->dQ[1], size_t(cap))) ||
+      (e = devAlloc(&c->dQ[2], size_t(cap))) || (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) ||
       (e = devAlloc(&c->dKillCount, 1)))
     return fail(e);
-  if ((e = resetRing(c))) return fail(e);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(BT_ERR_CUDA);
   *out = c;
   return BT_OK;
 }
@@ -1576,7 +1453,7 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   if (!c) return BT_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dSlot, c->dSeq, c->dRing, c->dCtr, c->dStats,
+  void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
                   c->dKillCount, c->dPhase, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu};
