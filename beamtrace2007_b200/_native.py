@@ -121,6 +121,8 @@ SIGNATURES = {
                                 C.POINTER(RunInfo)]),
     "bt_gpu_soft_points_device": (_I, [_P, C.POINTER(AreaLight), C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P,
                                        _P, C.POINTER(RunInfo)]),
+    "bt_gpu_soft_points_noalloc": (_I, [C.POINTER(SceneDesc), C.POINTER(KdDesc), C.POINTER(AreaLight),
+                                        C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P, _P, C.POINTER(RunInfo)]),
     "bt_gpu_soft_device": (_I, [_P, C.POINTER(Camera), C.POINTER(AreaLight), C.POINTER(SoftOpts), _P, _P, _P, _P,
                                 C.POINTER(RunInfo)]),
     "bt_gpu_primary_rays": (_I, [_P, C.POINTER(Camera), _P, _P, _P]),

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1800,6 +1801,351 @@ int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int
   if (tri) CK(cudaMemcpyAsync(tri, dtri, sizeof(int32_t) * npix, cudaMemcpyDeviceToHost, c->stream));
   if (flag) CK(cudaMemcpyAsync(flag, dflag, size_t(npix), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free soft shadows (bt_gpu_soft_points_noalloc).
+//
+// Every byte of device scratch this entry point needs -- the scene in the
+// engine's layout, the per-point root records and the three sub-beam queues
+// -- comes out of one fixed array compiled into this library, so a call
+// makes no device allocation.  The array lives at file scope; its name in
+// host code is only a host-side stand-in, so the host looks up its device
+// address once per device with cudaGetSymbolAddress and passes that
+// address on.  All calls on a device share the array: a call clears what
+// has to start at zero, and two calls whose work overlaps on the GPU would
+// corrupt each other (see the lock below).
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) unsigned char g_noallocScratch[BT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int64_t kNoAllocMinQueue = 8192;  // sub-beam records per queue, at least
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_noallocScratch on this device
+  int sms = 0;
+  cudaEvent_t rev[2] = {nullptr, nullptr};
+  std::mutex run;  // one call at a time per device in this process
+};
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noallocSetup;
+
+// Byte offsets of the sections of the scratch array (each 256-aligned).
+struct NoAllocLayout {
+  size_t err, ctr, stats, kill, phase;
+  size_t node, box, parent, ref, triNV;
+  size_t roots, live, state, attempt, list0, list1, miss, g, shade;
+  size_t queues;
+  int64_t cap;  // records per queue
+};
+
+// Lays the sections out; false when the fixed part leaves less than
+// kNoAllocMinQueue records per queue.  *need = bytes of the fixed part plus
+// the smallest queues.
+bool noallocLayout(int64_t nn, int64_t nr, int64_t nt, int64_t n, NoAllocLayout* L, size_t* need) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t R = size_t(std::max<int64_t>(n, 1));
+  L->err = take(2 * sizeof(int));
+  L->ctr = take(sizeof(Counters));
+  L->stats = take(kNumStats * sizeof(unsigned long long));
+  L->kill = take(sizeof(int));
+  L->phase = take(8 * sizeof(unsigned long long));
+  L->node = take(size_t(nn) * sizeof(uint2));
+  L->box = take(size_t(2 * nn) * sizeof(float4));
+  L->parent = take(size_t(nn) * sizeof(uint32_t));
+  L->ref = take(size_t(4 * nr) * sizeof(float4));
+  L->triNV = take(size_t(2 * nt) * sizeof(float4));
+  L->roots = take(R * sizeof(RootRec));
+  L->live = take(R * sizeof(int32_t));
+  L->state = take(R * sizeof(int32_t));
+  L->attempt = take(R * sizeof(int32_t));
+  L->list0 = take(R * sizeof(int32_t));
+  L->list1 = take(R * sizeof(int32_t));
+  L->miss = take(R * sizeof(unsigned long long));
+  L->g = take(R * sizeof(unsigned long long));
+  L->shade = take(2 * R * sizeof(float4));
+  L->queues = off;
+  *need = off + 3 * size_t(kNoAllocMinQueue) * sizeof(SubBeam);
+  if (*need > size_t(BT_NOALLOC_SCRATCH_BYTES)) return false;
+  L->cap = int64_t((size_t(BT_NOALLOC_SCRATCH_BYTES) - off) / (3 * sizeof(SubBeam)));
+  return true;
+}
+
+struct PackArgs {
+  const float* pos;
+  int64_t nv;
+  const uint32_t* tris;
+  const float* nrm;
+  int64_t nt;
+  const float* split;
+  const uint32_t* data;
+  const uint32_t* offset;
+  const uint32_t* parent;
+  const float* box;
+  int64_t nn;
+  const uint32_t* triIdx;
+  int64_t nr;
+  uint2* oNode;
+  float4* oBox;
+  uint32_t* oParent;
+  float4* oRef;
+  float4* oTriNV;
+  int* err;  // [0]: first failure (1 node, 2 reference, 3 triangle), [1]: its index
+};
+
+__device__ void packFail(int* err, int code, int64_t i) {
+  if (atomicCAS(err, 0, code) == 0) atomicExch(err + 1, int(i));
+}
+
+// The device-side twin of uploadScene's packing: kd nodes as {split bits or
+// leaf offset, data}, node boxes as two float4, parents, 64-byte triangle
+// references and per-triangle normal + first vertex.  Every index read from
+// the caller's arrays is checked before it is used; a bad one is recorded
+// in `err` and its record is skipped.  Interior nodes must have their
+// children after them and every node but the root its parent before it,
+// which bt_kd_build's trees satisfy and which keeps descents and climbs
+// finite.
+__global__ void packSceneKernel(PackArgs a) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  const int64_t m = max(a.nn, max(a.nr, a.nt));
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride) {
+    if (i < a.nn) {
+      const uint32_t d = a.data[i];
+      uint32_t x;
+      bool ok;
+      if ((d & 3u) == 3u) {
+        x = a.offset[i];
+        ok = int64_t(x) + int64_t(d >> 2) <= a.nr;
+      } else {
+        x = __float_as_uint(a.split[i]);
+        ok = int64_t(d >> 2) > i + 1 && int64_t(d >> 2) < a.nn;
+      }
+      const uint32_t par = a.parent[i];
+      if (i > 0) ok = ok && int64_t(par) < i;
+      if (!ok) {
+        packFail(a.err, 1, i);
+      } else {
+        a.oNode[i] = make_uint2(x, d);
+        const float* b = a.box + 6 * i;
+        a.oBox[2 * i] = make_float4(b[0], b[1], b[2], b[3]);
+        a.oBox[2 * i + 1] = make_float4(b[4], b[5], 0.f, 0.f);
+        a.oParent[i] = par;
+      }
+    }
+    if (i < a.nr) {
+      const uint32_t t = a.triIdx[i];
+      bool ok = int64_t(t) < a.nt;
+      uint32_t v0 = 0, v1 = 0, v2 = 0;
+      if (ok) {
+        v0 = a.tris[3 * size_t(t)];
+        v1 = a.tris[3 * size_t(t) + 1];
+        v2 = a.tris[3 * size_t(t) + 2];
+        ok = int64_t(v0) < a.nv && int64_t(v1) < a.nv && int64_t(v2) < a.nv;
+      }
+      if (!ok) {
+        packFail(a.err, 2, i);
+      } else {
+        const float* p0 = a.pos + 3 * size_t(v0);
+        const float* p1 = a.pos + 3 * size_t(v1);
+        const float* p2 = a.pos + 3 * size_t(v2);
+        const float* nr = a.nrm + 3 * size_t(t);
+        a.oRef[4 * i] = make_float4(p0[0], p0[1], p0[2], p1[0]);
+        a.oRef[4 * i + 1] = make_float4(p1[1], p1[2], p2[0], p2[1]);
+        a.oRef[4 * i + 2] = make_float4(p2[2], nr[0], nr[1], nr[2]);
+        a.oRef[4 * i + 3] = make_float4(__uint_as_float(v0), __uint_as_float(v1), __uint_as_float(v2), __uint_as_float(t));
+      }
+    }
+    if (i < a.nt) {
+      const uint32_t v0 = a.tris[3 * size_t(i)];
+      if (int64_t(v0) >= a.nv) {
+        packFail(a.err, 3, i);
+      } else {
+        const float* nr = a.nrm + 3 * size_t(i);
+        const float* p0 = a.pos + 3 * size_t(v0);
+        a.oTriNV[2 * i] = make_float4(nr[0], nr[1], nr[2], 0.f);
+        a.oTriNV[2 * i + 1] = make_float4(p0[0], p0[1], p0[2], 0.f);
+      }
+    }
+  }
+}
+
+// True when p is a 4-byte-aligned address of device (or managed) memory of
+// device `dev`; a host address handed to a kernel would fault.
+bool deviceReachable(const void* p, int dev) {
+  if ((reinterpret_cast<uintptr_t>(p) & 3u) != 0) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (at.type == cudaMemoryTypeManaged) return true;
+  return at.type == cudaMemoryTypeDevice && at.device == dev;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_gpu_soft_points_noalloc(const bt_scene_desc* sc, const bt_kd_desc* kd, const bt_area_light* L,
+                               const bt_soft_opts* o, int64_t n, const int32_t* dTri, const float* dX, const float* dN,
+                               float* dVis, float* dE, float* dEu, bt_run_info* info) {
+  const int64_t kMax32 = 0x7fffffff;
+  if (!sc || !kd || !L || n < 0 || n > kMax32 || sc->num_tris <= 0 || sc->num_tris > kMax32 || sc->num_verts <= 0 ||
+      sc->num_verts > kMax32 || kd->num_nodes <= 0 || kd->num_nodes > kMax32 || kd->num_refs < 0 ||
+      kd->num_refs > kMax32 || !sc->pos || !sc->tris || !sc->tri_normals || !kd->split || !kd->data || !kd->offset ||
+      !kd->parent || !kd->node_box || (kd->num_refs > 0 && !kd->tri_indices) || (n > 0 && (!dTri || !dX || !dN))) {
+    setErr("bt_gpu_soft_points_noalloc: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  NoAllocLayout lay;
+  size_t need = 0;
+  if (!noallocLayout(kd->num_nodes, kd->num_refs, sc->num_tris, n, &lay, &need)) {
+    setErr("bt_gpu_soft_points_noalloc: %lld kd nodes, %lld references, %lld triangles and %lld points need %zu bytes "
+           "of scratch; the fixed limit is %lld bytes (BT_NOALLOC_SCRATCH_BYTES)",
+           (long long)kd->num_nodes, (long long)kd->num_refs, (long long)sc->num_tris, (long long)n, need,
+           (long long)BT_NOALLOC_SCRATCH_BYTES);
+    return BT_ERR_TOO_LARGE;
+  }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    setErr("bt_gpu_soft_points_noalloc: device %d is beyond the %d this library serves", dev, kNoAllocMaxDevices);
+    return BT_ERR_INVALID;
+  }
+  NoAllocDevice& D = g_noalloc[dev];
+  {
+    // One-time set-up per device, with that device current: the device
+    // address of the scratch array, the SM count and two timing events.
+    std::lock_guard<std::mutex> lk(g_noallocSetup);
+    if (!D.ready) {
+      void* p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_noallocScratch));
+      CK(cudaDeviceGetAttribute(&D.sms, cudaDevAttrMultiProcessorCount, dev));
+      for (auto& ev : D.rev)
+        if (!ev) CK(cudaEventCreate(&ev));
+      D.scratch = static_cast<unsigned char*>(p);
+      D.ready = true;
+    }
+  }
+  const void* ins[] = {sc->pos, sc->tris, sc->tri_normals, kd->split, kd->data, kd->offset, kd->parent, kd->node_box};
+  for (const void* p : ins)
+    if (!deviceReachable(p, dev)) {
+      setErr("bt_gpu_soft_points_noalloc: a scene array is not 4-byte-aligned device memory of device %d", dev);
+      return BT_ERR_INVALID;
+    }
+  if ((kd->num_refs > 0 && !deviceReachable(kd->tri_indices, dev)) ||
+      (n > 0 && (!deviceReachable(dTri, dev) || !deviceReachable(dX, dev) || !deviceReachable(dN, dev) ||
+                 (dVis && !deviceReachable(dVis, dev)) || (dE && !deviceReachable(dE, dev)) ||
+                 (dEu && !deviceReachable(dEu, dev))))) {
+    setErr("bt_gpu_soft_points_noalloc: a point or output array is not 4-byte-aligned device memory of device %d", dev);
+    return BT_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> run(D.run);
+  unsigned char* S = D.scratch;
+  auto at = [&](size_t off) { return static_cast<void*>(S + off); };
+
+  // the scene, packed into the scratch array
+  int* dErr = static_cast<int*>(at(lay.err));
+  CK(cudaMemsetAsync(dErr, 0, 2 * sizeof(int), 0));
+  PackArgs pa;
+  pa.pos = sc->pos;
+  pa.nv = sc->num_verts;
+  pa.tris = sc->tris;
+  pa.nrm = sc->tri_normals;
+  pa.nt = sc->num_tris;
+  pa.split = kd->split;
+  pa.data = kd->data;
+  pa.offset = kd->offset;
+  pa.parent = kd->parent;
+  pa.box = kd->node_box;
+  pa.nn = kd->num_nodes;
+  pa.triIdx = kd->tri_indices;
+  pa.nr = kd->num_refs;
+  pa.oNode = static_cast<uint2*>(at(lay.node));
+  pa.oBox = static_cast<float4*>(at(lay.box));
+  pa.oParent = static_cast<uint32_t*>(at(lay.parent));
+  pa.oRef = static_cast<float4*>(at(lay.ref));
+  pa.oTriNV = static_cast<float4*>(at(lay.triNV));
+  pa.err = dErr;
+  const int64_t m = std::max(kd->num_nodes, std::max(kd->num_refs, sc->num_tris));
+  const int pg = int(std::min<int64_t>((m + 255) / 256, int64_t(D.sms) * 8));
+  packSceneKernel<<<pg, 256, 0, 0>>>(pa);
+  CK(cudaGetLastError());
+  int herr[2] = {0, 0};
+  CK(cudaMemcpy(herr, dErr, sizeof herr, cudaMemcpyDeviceToHost));
+  if (herr[0]) {
+    static const char* what[] = {"", "kd node", "kd reference", "triangle"};
+    setErr("bt_gpu_soft_points_noalloc: %s %d is malformed (an index out of range or out of order)",
+           what[herr[0] & 3], herr[1]);
+    return BT_ERR_INVALID;
+  }
+
+  // an engine context that only views the scratch array (it owns nothing
+  // and never reaches bt_gpu_destroy); the legacy default stream
+  bt_gpu_ctx c;
+  bt_gpu_config_default(&c.cfg);
+  c.device = dev;
+  c.sms = D.sms;
+  c.stream = nullptr;
+  c.rev[0] = D.rev[0];
+  c.rev[1] = D.rev[1];
+  c.s.node = pa.oNode;
+  c.s.box = pa.oBox;
+  c.s.parent = pa.oParent;
+  c.s.ref = pa.oRef;
+  c.s.triNV = pa.oTriNV;
+  for (int a = 0; a < 3; ++a) {
+    c.s.bounds.lo[a] = kd->bounds[a];
+    c.s.bounds.hi[a] = kd->bounds[3 + a];
+  }
+  c.s.numTris = int(sc->num_tris);
+  c.s.numNodes = uint32_t(kd->num_nodes);
+  c.numTris = sc->num_tris;
+  V3 dg = mk(sc->bounds[3] - sc->bounds[0], sc->bounds[4] - sc->bounds[1], sc->bounds[5] - sc->bounds[2]);
+  c.offset = length(dg) * kEpsRel;
+  c.capacity = int(std::min<int64_t>(lay.cap, kMax32));
+  SubBeam* q = static_cast<SubBeam*>(at(lay.queues));
+  c.dQ[0] = q;
+  c.dQ[1] = q + lay.cap;
+  c.dQ[2] = q + 2 * lay.cap;
+  c.dCtr = static_cast<Counters*>(at(lay.ctr));
+  c.dStats = static_cast<unsigned long long*>(at(lay.stats));
+  c.dKillCount = static_cast<int*>(at(lay.kill));
+  c.dPhase = static_cast<unsigned long long*>(at(lay.phase));
+  c.rootCap = size_t(std::max<int64_t>(n, 1));
+  c.dRoots = static_cast<RootRec*>(at(lay.roots));
+  c.dLive = static_cast<int32_t*>(at(lay.live));
+  c.dState = static_cast<int32_t*>(at(lay.state));
+  c.dAttempt = static_cast<int32_t*>(at(lay.attempt));
+  c.dList[0] = static_cast<int32_t*>(at(lay.list0));
+  c.dList[1] = static_cast<int32_t*>(at(lay.list1));
+  c.dMiss = static_cast<unsigned long long*>(at(lay.miss));
+  c.dG = static_cast<unsigned long long*>(at(lay.g));
+  c.dShade = static_cast<float4*>(at(lay.shade));
+
+  if (info) memset(info, 0, sizeof *info);
+  const auto t0 = std::chrono::steady_clock::now();
+  // The engine clears the counters, statistics and attempt tags at the start
+  // of every pass and writes each root's state when it admits the root, so
+  // nothing a previous call left in the array is read.
+  int e = softCore(&c, L, o, n, nullptr, dTri, dX, dN, dVis, dE, dEu, info);
+  if (e) return e;
+  CK(cudaStreamSynchronize(0));
+  if (info)
+    info->ms_total = info->ms_trace =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return BT_OK;
 }
 

@@ -187,6 +187,52 @@ BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light
                                      const int32_t* d_tri, const float* d_X, const float* d_N, float* d_vis,
                                      float* d_E, float* d_Eu, bt_run_info* info);
 
+/* Size of the device scratch array inside this library that
+ * bt_gpu_soft_points_noalloc works in: 64 MiB, held on every GPU that has
+ * loaded the library until the process exits. */
+#define BT_NOALLOC_SCRATCH_BYTES (64ll << 20)
+
+/* bt_gpu_soft_points_device for callers that cannot allocate device memory.
+ * No counterpart in the reference.
+ *
+ * Who needs it: a host application whose own allocator owns the GPU's
+ * memory (a renderer's or a framework's memory pool) and hands this library
+ * buffers from that pool.  cudaMalloc beside such a pool fails once the pool
+ * holds the memory, and cudaFree stalls every stream on the device while the
+ * application is mid-frame.  This call allocates nothing and needs no
+ * bt_gpu_ctx: the caller passes the scene and the shading points in its own
+ * device buffers; everything else comes from one fixed scratch array inside
+ * the library.
+ *
+ * Inputs: d_scene and d_kd are the finalised scene and its kd-tree as
+ * bt_scene_finalize and bt_kd_build produce them, with every pointer member
+ * a device address on the current device (counts and bounds are host
+ * values); d_tri[n], d_X[3n], d_N[3n] the shading points as for
+ * bt_gpu_soft_points_device.  Outputs d_vis, d_E, d_Eu (n each, any may be
+ * NULL) are device buffers.  Results equal bt_gpu_soft_points_device's on
+ * the same inputs.
+ *
+ * Limit: the scene in the engine's layout (44 bytes per kd node, 64 per
+ * reference, 32 per triangle), 164 bytes per point and three sub-beam queues
+ * of at least 8192 64-byte records must fit in BT_NOALLOC_SCRATCH_BYTES
+ * (each section rounded up to 256 bytes); larger calls return
+ * BT_ERR_TOO_LARGE before any GPU work.  A kd-tree whose indices are out of
+ * range or out of order returns BT_ERR_INVALID.
+ *
+ * Runs on the current device's legacy default stream and returns when the
+ * results are complete.  The first call on a device sets up (looks up the
+ * scratch array's device address, creates two timing events): make it
+ * before any stream capture.  All calls on a device share the scratch array,
+ * which keeps the last call's contents; each call clears what must start at
+ * zero.  Calls whose GPU work overlaps race on the array: this library
+ * serialises its own calls per device within a process, so do not run this
+ * entry point on the same device from another library copy or module at the
+ * same time. */
+BT_API int bt_gpu_soft_points_noalloc(const bt_scene_desc* d_scene, const bt_kd_desc* d_kd,
+                                      const bt_area_light* light, const bt_soft_opts* opts, int64_t n,
+                                      const int32_t* d_tri, const float* d_X, const float* d_N, float* d_vis,
+                                      float* d_E, float* d_Eu, bt_run_info* info);
+
 /* bt_gpu_soft on device buffers (W*H each; d_vis/d_E/d_Eu may be NULL):
  * everything stays in device memory.  Runs on the context's stream and
  * returns when the results are complete. */
