@@ -80,9 +80,10 @@ struct __align__(128) Counters {
   int count[2];                 // records in trace queue 0 / 1
   int head;                     // fetch cursor of the trace queue being drained
   int pad1[13];
-  int clipCount;                // records waiting for a clip
-  int clipHead;                 // fetch cursor of the clip queue
-  int pad2[14];
+  int clipCount;                // records waiting for a clip (from the bottom of the clip queue)
+  int clipHead;                 // fetch cursor of the clip queue (clips, then deferred outputs)
+  int outQ;                     // finished pieces waiting for output (from the top of the clip queue)
+  int pad2[13];
 };
 
 // Per-root query: plane, tolerances, mode (WfRoot, cuda/wavefront.cu:80-86).
@@ -138,7 +139,7 @@ struct RoundParams {
   int numRoots;
   int rootCap;  // size of the per-root arrays
   const int32_t* rootList;
-  RootRec* roots;
+  RootRec* roots;  // per-root query records
   int32_t* live;
   int32_t* state;
   int32_t* attempt;
@@ -597,6 +598,8 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
   Walk w;
   float lightArea = 0;
   int qRoot = -1;
+  bool outPending = false;
+  int outTri = -1;
   Stats st;
   st.clear();
   unsigned long long pc[4] = {0, 0, 0, 0};  // refill, trace, append, idle (optional accounting)
@@ -650,12 +653,41 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
         }
       }
       if (res == kStepFinished) {
-        outputPiece<App>(p, q, lightArea, r.root, b, occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1), st);
+        outTri = occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1);
+        if (outTri >= 0) st.hits++;
+        st.beams++;
+        outPending = App == kAppSoft ? outTri < 0 : outTri >= 0;  // soft keeps the visible light, the others the hits
         liveSub(p, r.root, 1);
         phase = kIdle;
       }
     }
     BT_PHASE(1)
+    // Finished pieces are output by the clip kernel, all lanes at once
+    // (the output step is long and only a few lanes finish per step).
+    const unsigned outm = __ballot_sync(kFull, outPending);
+    if (outm) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&p.ctr->outQ, __popc(outm));
+      base = __shfl_sync(kFull, base, 0);
+      if (outPending) {
+        SubBeam o;
+        for (int k = 0; k < 4; ++k) {
+          o.qx[k] = b.qx[k];
+          o.qy[k] = b.qy[k];
+        }
+        o.trail = 0;
+        o.node = 0;
+        o.root = r.root;
+        o.hit = outTri;
+        o.cursor = 0;
+        o.depth = 0;
+        o.n = int8_t(b.n);
+        o.neg = 0;
+        const int k = base + __popc(outm & ltMask);
+        if (k < p.capacity) p.cq[p.capacity - 1 - k] = o;
+        outPending = false;
+      }
+    }
     const unsigned clip = __ballot_sync(kFull, phase == kTrace && res == kStepSplit);
     if (clip) {
       int base = 0;
@@ -680,7 +712,14 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
 template <int App>
 __global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
-  const int n = min(p.ctr->clipCount, p.capacity);
+  // clip records fill the clip queue from the bottom, deferred outputs from
+  // the top; together they are at most the round's trace records
+  const int nClip = p.ctr->clipCount, nOut = p.ctr->outQ;
+  if (int64_t(nClip) + nOut > p.capacity) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) atomicExch(&p.ctr->error, 1);
+    return;
+  }
+  const int n = nClip + nOut;
   Stats st;
   st.clear();
   for (;;) {
@@ -689,7 +728,7 @@ __global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ R
     base = __shfl_sync(kFull, base, 0);
     if (base >= n) break;
     const int i = base + lane;
-    if (i < n) {
+    if (i < nClip) {
       SubBeam rec = p.cq[i];
       Stats cs;
       cs.clear();
@@ -698,6 +737,27 @@ __global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ R
         if (at >= 0) p.tq[p.cur ^ 1][at] = rec;
       }
       addStats(st, cs);
+    } else if (i < n) {
+      const SubBeam o = p.cq[p.capacity - 1 - (i - nClip)];
+      if (uint32_t(o.root) >= uint32_t(p.rootCap) || o.n < 3 || o.n > 4) {
+        atomicExch(&p.ctr->error, 2);
+      } else {
+        PieceOut po;
+        float lightArea;
+        Query q;
+        loadRoot(&p.roots[o.root], q, lightArea);
+        po.P = q.P;
+        for (int k = 0; k < 4; ++k) {
+          po.qx[k] = o.qx[k];
+          po.qy[k] = o.qy[k];
+        }
+        po.n = o.n;
+        po.root = o.root;
+        po.tri = o.hit;
+        po.exclude = q.exclude;
+        po.lightArea = lightArea;
+        outputPieceCold<App>(p, &po);
+      }
     }
   }
   flushStats(p, st);
@@ -712,6 +772,7 @@ __global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
   c->head = 0;
   c->clipCount = 0;
   c->clipHead = 0;
+  c->outQ = 0;
   c->rounds++;
   c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
 }
