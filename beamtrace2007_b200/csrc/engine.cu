@@ -1,17 +1,20 @@
-// The B200 beam engine: persistent warps over sub-beam records, and the
-// C-ABI entry points (include/bt_gpu.h).
+// The B200 beam engine: rounds of persistent-grid kernels over sub-beam
+// records, and the C-ABI entry points (include/bt_gpu.h).
 //
-// Sub-beams are 64-byte self-contained records in two global queues.  Each
-// launch ("round") is a persistent grid that drains the current queue: a lane
-// takes a record, traces it leaf by leaf until it finishes or a triangle
-// needs a clip, and takes the next record as soon as it is free (one atomic
-// per warp for all idle lanes, ballot/popc compaction).  When the queue is
-// empty, idle lanes admit new roots.  Lanes that need a clip park until
-// `split_batch` lanes of the warp wait (or no lane can trace), then clip
-// together, so tracing and clipping each run with most lanes converged; the
-// pieces of a clip go to the next round's queue in consecutive slots taken
-// with one atomic (siblings stay adjacent).  Every warp works on every root,
-// so no lane starves while work exists anywhere on the GPU.
+// Sub-beams are 64-byte self-contained records.  A round is three kernels:
+//   admit  roots whose queue reservation fits become pre-split records in the
+//          round's trace queue;
+//   trace  a persistent grid drains the trace queue: a lane takes a record,
+//          traces it leaf by leaf until it finishes or a triangle needs a
+//          clip, and takes the next record as soon as it is free (one atomic
+//          per warp for all idle lanes, ballot/popc compaction).  Records
+//          that need a clip go to the bottom of the clip queue, finished
+//          pieces to its top;
+//   clip   one lane per clip record (pieces go to the next round's trace
+//          queue, siblings in consecutive slots) and per finished piece
+//          (the output step: soft-shadow accumulators, polygon lists);
+// plus a one-thread bookkeeping kernel.  Every warp works on every root, so
+// no lane starves while work exists anywhere on the GPU.
 //
 // Memory is bounded without waiting: a root is admitted only if `budget`
 // queue slots are free for it, and a root that would exceed its budget is
@@ -145,11 +148,35 @@ struct RoundParams {
   int32_t* attempt;
   Counters* ctr;
   unsigned long long* stats;
-  unsigned long long* phaseCycles;  // optional: warp cycles per trace-loop phase (diagnostics)
   AppParams app;
 };
 
 __device__ __forceinline__ int laneId() { return threadIdx.x & 31; }
+
+// The current root-to-node path of a tracing lane, in shared memory: entry
+// k (the node at depth k) at col[k * kThreads], so the lanes of a warp hit
+// distinct banks.  Entries [known, depth) are valid; a record fresh from
+// the queue knows none and fills them from parent links on its first climb
+// below `known` (the reference's own walk, done once per record).
+constexpr int kPathDepth = 64;  // the restart trail has 64 bits
+struct PathCache {
+  uint32_t* col;
+  int known;
+  __device__ __forceinline__ void begin(int depth) { known = depth; }
+  __device__ __forceinline__ void descend(int depth, uint32_t node) {
+    if (depth < kPathDepth) col[depth * kThreads] = node;
+  }
+  __device__ __forceinline__ uint32_t ancestor(const SceneDev& s, uint32_t node, int depth, int d) {
+    if (d >= known) return col[d * kThreads];
+    uint32_t x = known < depth ? col[known * kThreads] : node;
+    for (int k = known < depth ? known : depth; k > d; --k) {
+      x = __ldg(&s.parent[x]);
+      if (k - 1 < kPathDepth) col[(k - 1) * kThreads] = x;
+    }
+    known = d;
+    return x;
+  }
+};
 
 __device__ __forceinline__ float asF(int i) { return __int_as_float(i); }
 __device__ __forceinline__ int asI(float f) { return __float_as_int(f); }
@@ -598,18 +625,14 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
   Walk w;
   float lightArea = 0;
   int qRoot = -1;
+  __shared__ uint32_t pathStack[kPathDepth * kThreads];
+  PathCache path;
+  path.col = pathStack + threadIdx.x;
+  path.known = 0;
   bool outPending = false;
   int outTri = -1;
   Stats st;
   st.clear();
-  unsigned long long pc[4] = {0, 0, 0, 0};  // refill, trace, append, idle (optional accounting)
-  long long tprev = p.phaseCycles ? clock64() : 0;
-#define BT_PHASE(k)                              \
-  if (p.phaseCycles) {                           \
-    const long long t_ = clock64();              \
-    pc[k] += (unsigned long long)(t_ - tprev);   \
-    tprev = t_;                                  \
-  }
   for (;;) {
     const unsigned idle = __ballot_sync(kFull, phase == kIdle);
     if (idle && !exhausted) {
@@ -632,26 +655,28 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
           }
           expand(p.s, q, r, b);
           walkBegin(p.s, r, w);
+          path.begin(r.depth);
           phase = kTrace;
         }
       }
     }
-    BT_PHASE(0)
     if (!__any_sync(kFull, phase == kTrace)) {
       if (exhausted) break;
       continue;
     }
     // one leaf: climb / descend to it, then test its triangles
     int res = kStepContinue;
+    int occ = -1;
     if (phase == kTrace) {
-      res = advance(p.s, q, b, r, w, st);
-      int occ = -1;
+      res = advance(p.s, q, b, r, w, st, path);
       if (res == kStepContinue) {
         for (;;) {
           res = testOne(p.s, q, r, b, st, occ);
           if (res != kStepContinue || !moreInLeaf(p.s, q, r)) break;
         }
       }
+    }
+    if (phase == kTrace) {
       if (res == kStepFinished) {
         outTri = occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1);
         if (outTri >= 0) st.hits++;
@@ -661,7 +686,6 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
         phase = kIdle;
       }
     }
-    BT_PHASE(1)
     // Finished pieces are output by the clip kernel, all lanes at once
     // (the output step is long and only a few lanes finish per step).
     const unsigned outm = __ballot_sync(kFull, outPending);
@@ -698,11 +722,7 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
         phase = kIdle;
       }
     }
-    BT_PHASE(2)
   }
-#undef BT_PHASE
-  if (p.phaseCycles && lane == 0)
-    for (int k = 0; k < 3; ++k) atomicAdd(&p.phaseCycles[k], pc[k]);
   flushStats(p, st);
 }
 
@@ -1033,7 +1053,6 @@ struct bt_gpu_ctx {
   unsigned long long *dMiss = nullptr, *dG = nullptr;
   float4* dShade = nullptr;
   int* dKillCount = nullptr;
-  unsigned long long* dPhase = nullptr;
   // outputs
   int64_t outCap = 0;
   float *dOx = nullptr, *dOy = nullptr, *dOarea = nullptr;
@@ -1045,6 +1064,7 @@ struct bt_gpu_ctx {
   int blocksSoft = 0, blocksPrimary = 0, blocksPoint = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t rev[2] = {nullptr, nullptr};
+  cudaEvent_t kev[32] = {};  // kernel_timing: 4 per round of a batch (before admit, trace, clip, after clip)
 };
 
 extern "C" {
@@ -1057,7 +1077,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->primary_budget = 4096;
   c->capacity = 0;
   c->blocks_per_sm = 0;
-  c->split_batch = 12;
+  c->kernel_timing = 0;
   c->max_retries = 4;
 }
 
@@ -1173,8 +1193,6 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
   info->max_spill = std::max(info->max_spill, hc.maxQueue);
 }
 
-// Runs every root of `R` through the engine: passes of launches until all
-// roots are done; roots abandoned over budget are retried with 16x budget.
 // Runs every root of `R` through the engine.  A round is three kernels --
 // admit (new roots, as far as the queue reservation allows), trace (drain
 // the round's queue), clip (pieces into the next round's queue) -- plus the
@@ -1208,18 +1226,12 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.ctr = c->dCtr;
   p.stats = c->dStats;
   p.app = app;
-  p.phaseCycles = nullptr;
-  // BT_PHASES=1: warp cycles per trace-loop phase on stderr (diagnostics).
-  const bool phases = getenv("BT_PHASES") != nullptr;
-  if (phases) {
-    if (!c->dPhase && (e = devAlloc(&c->dPhase, 8))) return e;
-    CK(cudaMemsetAsync(c->dPhase, 0, 8 * sizeof(unsigned long long), c->stream));
-    p.phaseCycles = c->dPhase;
-  }
   const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App>), gC = gridFor(c, clipKernel<App>);
+  static_assert(4 * kRoundsPerCheck <= 32, "kernel_timing events");
+  const bool ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
   // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
   FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
-  int launches = 0, passes = 0, retried = 0;
+  int launches = 0, passes = 0, retried = 0, roundsRun = 0;
   const int32_t* list = nullptr;
   int n = R;
   Counters hc;
@@ -1246,9 +1258,13 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       CK(cudaEventRecord(c->rev[0], c->stream));
       for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
         p.cur = round & 1;
+        if (ktime) CK(cudaEventRecord(c->kev[4 * k], c->stream));
         admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 1], c->stream));
         traceKernel<App><<<gT, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 2], c->stream));
         clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 3], c->stream));
         roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
         launches += 4;
       }
@@ -1261,6 +1277,15 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       if (info) {
         info->ms_round += ms;
         info->round_launches += 3 * kRoundsPerCheck;
+        if (ktime) {
+          double* dst[3] = {&info->ms_kernel_admit, &info->ms_kernel_trace, &info->ms_kernel_clip};
+          for (int k = 0; k < kRoundsPerCheck; ++k)
+            for (int j = 0; j < 3; ++j) {
+              float t = 0;
+              CK(cudaEventElapsedTime(&t, c->kev[4 * k + j], c->kev[4 * k + j + 1]));
+              *dst[j] += t;
+            }
+        }
       }
       if (roundLog)
         fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d ms %.3f\n", pass, hc.rounds,
@@ -1276,6 +1301,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       }
     }
     if (info) info->max_spill = std::max(info->max_spill, hc.maxQueue);
+    roundsRun += hc.rounds;
     if (hc.killed == 0) break;
     if (pass >= c->cfg.max_retries) {
       setErr("%d roots still over budget %d after %d retries", hc.killed, budget, pass);
@@ -1294,14 +1320,8 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     n = nk;
     budget *= 16;
   }
-  if (phases) {
-    unsigned long long pc[8];
-    CK(cudaMemcpy(pc, c->dPhase, sizeof pc, cudaMemcpyDeviceToHost));
-    double tot = double(pc[0] + pc[1] + pc[2]) + 1e-30;
-    fprintf(stderr, "trace loop (%% of warp cycles): refill %.1f trace %.1f append %.1f\n", 100.0 * pc[0] / tot,
-            100.0 * pc[1] / tot, 100.0 * pc[2] / tot);
-  }
   if (info) {
+    info->rounds += roundsRun;
     info->launches += launches;
     info->passes += passes;
     info->retried_roots += retried;
@@ -1491,6 +1511,9 @@ int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   for (auto& ev : c->rev)
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
+  if (c->cfg.kernel_timing)
+    for (auto& ev : c->kev)
+      if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   if ((e = uploadScene(c, scene, kd))) return fail(e);
   // Sub-beam queues: three of `capacity` 64-byte records.  Default 2^23
   // records (512 MiB each), at most 10% of the free memory.
@@ -1517,13 +1540,15 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
-                  c->dKillCount, c->dPhase, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
+                  c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->rev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->kev)
     if (ev) cudaEventDestroy(ev);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1900,7 +1925,7 @@ std::mutex g_noallocSetup;
 
 // Byte offsets of the sections of the scratch array (each 256-aligned).
 struct NoAllocLayout {
-  size_t err, ctr, stats, kill, phase;
+  size_t err, ctr, stats, kill;
   size_t node, box, parent, ref, triNV;
   size_t roots, live, state, attempt, list0, list1, miss, g, shade;
   size_t queues;
@@ -1922,7 +1947,6 @@ bool noallocLayout(int64_t nn, int64_t nr, int64_t nt, int64_t n, NoAllocLayout*
   L->ctr = take(sizeof(Counters));
   L->stats = take(kNumStats * sizeof(unsigned long long));
   L->kill = take(sizeof(int));
-  L->phase = take(8 * sizeof(unsigned long long));
   L->node = take(size_t(nn) * sizeof(uint2));
   L->box = take(size_t(2 * nn) * sizeof(float4));
   L->parent = take(size_t(nn) * sizeof(uint32_t));
@@ -2184,7 +2208,6 @@ int bt_gpu_soft_points_noalloc(const bt_scene_desc* sc, const bt_kd_desc* kd, co
   c.dCtr = static_cast<Counters*>(at(lay.ctr));
   c.dStats = static_cast<unsigned long long*>(at(lay.stats));
   c.dKillCount = static_cast<int*>(at(lay.kill));
-  c.dPhase = static_cast<unsigned long long*>(at(lay.phase));
   c.rootCap = size_t(std::max<int64_t>(n, 1));
   c.dRoots = static_cast<RootRec*>(at(lay.roots));
   c.dLive = static_cast<int32_t*>(at(lay.live));

@@ -192,72 +192,77 @@ BT_HD int highestBit64(unsigned long long x) {
 #endif
 }
 
-// Descends to the next leaf / climbs to the next pending far child until a
-// triangle is pending (kStepContinue, phase kPhTest) or no cell is left
-// (kStepFinished: the caller outputs the beam) (wfAdvance,
-// wavefront_core.h:157-231).
-BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st) {
-  for (;;) {
-    if (w.phase == kPhDescend) {
-      for (;;) {
-        const uint2 nd = s.node[r.node];
-        if (isLeaf(nd)) break;
-        st.kdSteps++;
-        const int d = r.depth++;
-        const int a = int(nd.y & 3u);
-        const float sp = splitOf(nd);
-        const bool pos = !((B.neg >> a) & 1);
-        const float Ns = (pos ? 1.f : -1.f) * (sp - comp(q.P.O, a));
-        const uint32_t left = r.node + 1, right = nd.y >> 2;
-        const uint32_t cs = pos ? right : left, co = pos ? left : right;
-        int dec = kFar;
-        if (Ns > 0) dec = decide(q, B, a, Ns, w.box);
-        // the child entered is the right one (lo[a] = split) or the left one (hi[a] = split)
-        const bool goRight = dec == kFar ? pos : !pos;
-        if (dec == kBoth) r.trail |= 1ull << d;
-        r.node = dec == kFar ? cs : co;
-        if (goRight)
-          boxSetLo(w.box, a, sp);
-        else
-          boxSetHi(w.box, a, sp);
-      }
-      r.cursor = 0;
-      st.leafVisits++;
-      w.phase = kPhTest;
-    }
-    if (w.phase == kPhTest) {
-      const uint2 leaf = s.node[r.node];
-      const uint32_t cnt = leaf.y >> 2;
-      uint32_t i = uint32_t(r.cursor);
-      while (i < cnt && refTri(s, leaf.x + i) == q.exclude) ++i;
-      r.cursor = int32_t(i);
-      if (i < cnt) return kStepContinue;
-      w.phase = kPhClimb;
-    }
-    for (;;) {
-      if (r.trail == 0) return kStepFinished;
-      const int d = highestBit64(r.trail);
-      uint32_t node = r.node;
-      for (int depth = r.depth; depth > d; --depth) {
-        node = s.parent[node];
-        st.climbs++;
-      }
-      r.trail &= (1ull << d) - 1;
-      const uint2 nd = s.node[node];
-      const uint32_t cs = ((B.neg >> (nd.y & 3u)) & 1) ? node + 1 : (nd.y >> 2);
-      r.node = node;
-      r.depth = int16_t(d);
-      const Box cb = loadBox(s, cs);
-      if (overlaps(q, B, cb)) {
-        r.node = cs;
-        r.depth = int16_t(d + 1);
-        r.cursor = -1;
-        w.phase = kPhDescend;
-        w.box = cb;
-        break;
-      }
-    }
+// Ancestors of the current kd node for the restart-trail climb.  The
+// reference walks parent links one level at a time; ParentClimb does the
+// same.  The kernels use a per-lane copy of the current root-to-node path
+// in shared memory instead (PathCache, engine.cu): the same nodes, found
+// without the chain of dependent loads.  Either way the climb counter
+// counts levels, as the reference's does.
+struct ParentClimb {
+  BT_HD void begin(int) {}
+  BT_HD void descend(int, uint32_t) {}
+  BT_HD uint32_t ancestor(const SceneDev& s, uint32_t node, int depth, int d) {
+    for (; depth > d; --depth) node = s.parent[node];
+    return node;
   }
+};
+
+// One node visit of the descent (the inner loop of wfAdvance,
+// wavefront_core.h:163-189): a kd step into the child the beam enters
+// (false), or the leaf is reached (true: cursor 0, leaf counted).
+template <class Anc>
+BT_HD bool descendStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc) {
+  const uint2 nd = s.node[r.node];
+  if (isLeaf(nd)) {
+    r.cursor = 0;
+    st.leafVisits++;
+    return true;
+  }
+  st.kdSteps++;
+  const int d = r.depth++;
+  anc.descend(d, r.node);
+  const int a = int(nd.y & 3u);
+  const float sp = splitOf(nd);
+  const bool pos = !((B.neg >> a) & 1);
+  const float Ns = (pos ? 1.f : -1.f) * (sp - comp(q.P.O, a));
+  const uint32_t left = r.node + 1, right = nd.y >> 2;
+  const uint32_t cs = pos ? right : left, co = pos ? left : right;
+  int dec = kFar;
+  if (Ns > 0) dec = decide(q, B, a, Ns, w.box);
+  // the child entered is the right one (lo[a] = split) or the left one (hi[a] = split)
+  const bool goRight = dec == kFar ? pos : !pos;
+  if (dec == kBoth) r.trail |= 1ull << d;
+  r.node = dec == kFar ? cs : co;
+  if (goRight)
+    boxSetLo(w.box, a, sp);
+  else
+    boxSetHi(w.box, a, sp);
+  return false;
+}
+
+// One pop of the restart trail (wfAdvance's climb, wavefront_core.h:
+// 204-229): the deepest pending far child is entered if the beam overlaps
+// its box (kClimbDescend, w.box set), skipped (kClimbNext), or nothing is
+// pending (kClimbFinished).
+enum { kClimbFinished = 0, kClimbDescend = 1, kClimbNext = 2 };
+template <class Anc>
+BT_HD int climbStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc) {
+  if (r.trail == 0) return kClimbFinished;
+  const int d = highestBit64(r.trail);
+  const uint32_t node = anc.ancestor(s, r.node, r.depth, d);
+  st.climbs += uint32_t(r.depth - d);
+  r.trail &= (1ull << d) - 1;
+  const uint2 nd = s.node[node];
+  const uint32_t cs = ((B.neg >> (nd.y & 3u)) & 1) ? node + 1 : (nd.y >> 2);
+  r.node = node;
+  r.depth = int16_t(d);
+  const Box cb = loadBox(s, cs);
+  if (!overlaps(q, B, cb)) return kClimbNext;
+  r.node = cs;
+  r.depth = int16_t(d + 1);
+  r.cursor = -1;
+  w.box = cb;
+  return kClimbDescend;
 }
 
 // True if the leaf has another triangle to test (skipping the excluded one)
@@ -270,6 +275,39 @@ BT_HD bool moreInLeaf(const SceneDev& s, const Query& q, SubBeam& r) {
   r.cursor = int32_t(i);
   return i < cnt;
 }
+
+// Descends to the next leaf / climbs to the next pending far child until a
+// triangle is pending (kStepContinue, phase kPhTest) or no cell is left
+// (kStepFinished: the caller outputs the beam) (wfAdvance,
+// wavefront_core.h:157-231).
+template <class Anc>
+BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc) {
+  for (;;) {
+    if (w.phase == kPhDescend) {
+      while (!descendStep(s, q, B, r, w, st, anc)) {
+      }
+      w.phase = kPhTest;
+    }
+    if (w.phase == kPhTest) {
+      if (moreInLeaf(s, q, r)) return kStepContinue;
+      w.phase = kPhClimb;
+    }
+    for (;;) {
+      const int c = climbStep(s, q, B, r, w, st, anc);
+      if (c == kClimbFinished) return kStepFinished;
+      if (c == kClimbDescend) {
+        w.phase = kPhDescend;
+        break;
+      }
+    }
+  }
+}
+
+BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st) {
+  ParentClimb anc;
+  return advance(s, q, B, r, w, st, anc);
+}
+
 
 BT_COLD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
   TriRec t = loadRef(s, k);

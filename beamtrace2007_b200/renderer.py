@@ -162,7 +162,7 @@ class GpuRenderer:
     on one GPU for the renderer's lifetime."""
 
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
-                 capacity: int = 0, blocks_per_sm: int = 0, split_batch: int = 0):
+                 capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -171,8 +171,7 @@ class GpuRenderer:
         cfg.primary_budget = primary_budget
         cfg.capacity = capacity
         cfg.blocks_per_sm = blocks_per_sm
-        if split_batch:
-            cfg.split_batch = split_batch
+        cfg.kernel_timing = int(kernel_timing)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()

@@ -11,11 +11,17 @@ pixel through the persistent-warp engine.  Synthetic, seeded data.
 `value`: pixels/s with the scene resident in HBM, outputs in device memory,
 each frame timed with CUDA events on the engine's stream; L2 is flushed
 (a 256 MiB write) between timed frames because the scene fits in L2.
+`roofline`: the trace kernel (the dominant one), algorithmic bytes per
+launch over its launch time from CUDA events recorded between the round
+kernels on the engine's stream inside the timed frames (kernel_timing);
+`traffic` is the DRAM bytes per launch of the committed ncu capture.
 `e2e`: the same frames through bt_gpu_soft with host output buffers (the
 GpuRenderer::softShadows contract), wall-clocked per call, device-to-host
 copies of tri/vis/E/Eu inside.
 `cpu_baseline` / `--impl reference`: the reference's own CPU tracer
-(compiled from its sources, oracle/_ref) on the host's cores.
+(compiled from its sources, oracle/_ref) on the host's cores; the
+reference arm also times the reference's own GPU engine built for sm_100a
+(`reference_gpu`) when oracle/_ref/libbtref_gpu.so is present.
 
 Multi-GPU: the frames of different GPUs are independent (replicas only):
 each rank renders the workload on its own GPU, `value` = all ranks' pixels /
@@ -136,17 +142,17 @@ def dist_barrier(ws: int):
         dist.barrier()
 
 
-def cpu_reference(scene, steps: int, warmup: int, min_seconds: float = 3.0):
-    """The reference CPU tracer (oracle/_ref) on the same frame, all host threads."""
+def cpu_reference(scene, steps: int, warmup: int, min_seconds: float = 10.0, max_frames: int = 1000):
+    """The reference CPU tracer (oracle/_ref) on the same frame, all host threads:
+    at least `steps` frames and about `min_seconds` of work."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from ref import RefTracer, ref_available
-    from beamtrace2007_b200.renderer import make_camera
     if not ref_available("f"):
         return None
     threads = os.cpu_count() or 1
     rf = RefTracer(scene.pos, scene.tris, "f")
     v = scene.views[0]
-    cam = make_camera(v.eye, v.target, v.fov, scene.up, W, H).as_array()
+    cam = rf.camera_make(v.eye, v.target, v.fov, scene.up, W, H)  # the reference's Camera::make
     L = scene.light_array()
     for _ in range(warmup):
         rf.soft_image(cam, W, H, L, exact=True, threads=threads)
@@ -155,7 +161,7 @@ def cpu_reference(scene, steps: int, warmup: int, min_seconds: float = 3.0):
     while len(times) < steps or time.perf_counter() - t_start < min_seconds:
         r = rf.soft_image(cam, W, H, L, exact=True, threads=threads)
         times.append(r["primary_s"] + r["trace_s"])
-        if len(times) >= 1000:
+        if len(times) >= max_frames:
             break
     per = float(np.median(times))
     return {"value": W * H / per, "unit": "px/s", "cores": threads, "kind": "reference",
@@ -164,13 +170,42 @@ def cpu_reference(scene, steps: int, warmup: int, min_seconds: float = 3.0):
             "ms_per_frame": per * 1e3}
 
 
+def reference_gpu(scene, steps: int, warmup: int):
+    """The reference's own GPU engine (cuda/ built for sm_100a from its
+    sources, oracle/_ref/libbtref_gpu.so) on the same frame, if built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref import RefGpu, RefTracer, ref_gpu_available
+    if not ref_gpu_available():
+        return None
+    try:
+        g = RefGpu(scene.pos, scene.tris)
+    except OSError as e:
+        return {"unavailable": str(e)[:200]}
+    v = scene.views[0]
+    cam = RefTracer(scene.pos, scene.tris, "f").camera_make(v.eye, v.target, v.fov, scene.up, W, H)
+    L = scene.light_array()
+    for _ in range(warmup):
+        g.soft(cam, W, H, L, exact=True)
+    ms, fb = [], 0
+    for _ in range(steps):
+        r = g.soft(cam, W, H, L, exact=True)
+        ms.append((r["primary_s"] + r["trace_s"]) * 1e3)
+        fb += r["overflow_px"]
+    g.close()
+    per = float(np.median(ms))
+    return {"value": W * H / per * 1e3, "unit": "px/s", "ms_per_frame": per, "frames": steps,
+            "cpu_fallback_pixels": fb,
+            "build": "reference cuda/gpu_render.cu + cuda/wavefront.cu for sm_100a, --use_fast_math on wavefront.cu "
+                     "as its cuda/CMakeLists.txt sets (wall-clocked GpuRenderer::softShadows)"}
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
     from beamtrace2007_b200 import scenes
     s = scenes.plant()
-    c = cpu_reference(s, args.steps, args.warmup)
+    c = cpu_reference(s, args.steps, args.warmup, min_seconds=0.0, max_frames=args.steps)
     if c is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbtref_f.so not built"}))
         return 0
@@ -181,8 +216,25 @@ def run_reference_arm(args):
             "cpu_baseline": {"value": c["value"], "unit": "px/s", "cores": c["cores"], "kind": "reference",
                              "sample": c["sample"]},
             "e2e": {"value": c["value"], "unit": "px/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        import torch
+        if torch.cuda.is_available():
+            g = reference_gpu(s, max(args.steps, 5), args.warmup)
+            if g is not None:
+                line["reference_gpu"] = g
+    except Exception as e:  # the CPU arm stands on its own
+        line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line))
     return 0
+
+
+def trace_traffic():
+    """DRAM bytes per trace-kernel launch from the committed ncu capture."""
+    tp = os.path.join(ROOT, "profiles", "trace_kernel_plant512_traffic.json")
+    if os.path.exists(tp):
+        d = json.load(open(tp))
+        return d.get("bytes_per_launch"), d.get("command")
+    return None, None
 
 
 def main():
@@ -192,6 +244,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--capacity", type=int, default=0,
+                    help="sub-beam records per queue (0: the engine's default); small values for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -212,7 +266,7 @@ def main():
     cam = make_camera(v.eye, v.target, v.fov, s.up, W, H)
     L = N.AreaLight.from_array(s.light_array())
     opts = N.SoftOpts(1, 0.0)
-    g = GpuRenderer(ps, device=local)
+    g = GpuRenderer(ps, device=local, capacity=args.capacity, kernel_timing=True)
     lib = N.lib()
     npx = W * H
     dtri = torch.empty(npx, dtype=torch.int32, device="cuda")
@@ -231,14 +285,13 @@ def main():
     torch.cuda.synchronize()
     dist_barrier(ws)
     torch.cuda.synchronize()
-    ms, round_ms, infos = [], [], []
+    ms, infos = [], []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.fill_(1)
             torch.cuda.synchronize()
             d = frame()
             ms.append(d["ms_total"])
-            round_ms.append(d["ms_round"])
             infos.append(d)
         torch.cuda.synchronize()
         dist_barrier(ws)
@@ -258,16 +311,18 @@ def main():
     e2e_s = dist_max(sum(e2e_t), ws)
     value = ws * npx * args.steps / total_s
     last = infos[-1]
-    # algorithmic bytes of one frame (counters are the oracle's, bitwise)
-    b_alg = (64 * last["tri_tests"] + 12 * last["kd_steps"] + 12 * last["leaf_visits"] + 128 * last["beams"]
-             + 40 * npx)
-    rms = float(np.mean(round_ms))
-    achieved = b_alg / (rms * 1e-3) / 1e9
+    # Algorithmic bytes (counters are the reference's, bitwise): the frame
+    # B_alg = 64 triTests + 12 kdSteps + 12 leafVisits + 128 beams + 40 px;
+    # the trace kernel's share reads the triangle references, kd nodes and
+    # each final sub-beam record once: 64 triTests + 12 kdSteps + 12 leafVisits + 64 beams.
+    b_frame = (64 * last["tri_tests"] + 12 * last["kd_steps"] + 12 * last["leaf_visits"] + 128 * last["beams"]
+               + 40 * npx)
+    b_trace = 64 * last["tri_tests"] + 12 * last["kd_steps"] + 12 * last["leaf_visits"] + 64 * last["beams"]
+    trace_ms = float(np.mean([d["ms_kernel_trace"] for d in infos]))
+    launches_per_frame = float(np.mean([d["rounds"] for d in infos]))
+    achieved = b_trace / (trace_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "round_kernel_plant512_traffic.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("bytes_per_frame")
+    traffic, traffic_cmd = trace_traffic()
     if rank != 0:
         g.close()
         return 0
@@ -277,14 +332,21 @@ def main():
             "config": dict(workload_config(), parallelism=f"replicas{ws}"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "roundKernel<soft>", "algorithmic_bytes_per_frame": b_alg,
-                         "kernel_ms_per_frame": rms},
+                         "kernel": "traceKernel<soft>",
+                         "algorithmic_bytes_per_launch": b_trace / launches_per_frame,
+                         "launches_per_frame": launches_per_frame,
+                         "kernel_ms_per_launch": trace_ms / launches_per_frame,
+                         "traffic_source": traffic_cmd,
+                         "frame": {"algorithmic_bytes": b_frame, "achieved_gbs": b_frame / (total_s / args.steps) / 1e9,
+                                   "frac": b_frame / (total_s / args.steps) / 1e9 / peak}},
             "e2e": {"value": ws * npx * args.steps / e2e_s, "unit": "px/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": npx * 16},
             "gpu_launches": int(sum(d["launches"] for d in infos)),
             "clocks": clk.summary(),
-            "counters": {k: last[k] for k in ("tri_tests", "kd_steps", "leaf_visits", "beams", "splits",
-                                               "round_launches", "passes", "retried_roots", "max_spill")},
+            "kernels_ms_per_frame": {k: float(np.mean([d["ms_kernel_" + k] for d in infos]))
+                                     for k in ("admit", "trace", "clip")},
+            "counters": {k: last[k] for k in ("tri_tests", "kd_steps", "leaf_visits", "beams", "splits", "climbs",
+                                               "rounds", "passes", "retried_roots", "max_spill")},
             "ms_primary": float(np.mean([d["ms_primary"] for d in infos])),
             "ms_trace": float(np.mean([d["ms_trace"] for d in infos]))}
     if not args.no_cpu_baseline and ws == 1:

@@ -254,3 +254,47 @@ class RefTracer:
         n = np.ascontiguousarray(n, np.float64)
         poly = np.ascontiguousarray(poly, np.float64)
         return float(self.lib.btr_form_factor(_ptr(x), _ptr(n), _ptr(poly), int(len(poly))))
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libbtref_gpu.so"))
+
+
+class RefGpu:
+    """The reference's own GPU renderer (cuda/gpu_render.cu + cuda/wavefront.cu
+    compiled for sm_100a from its sources by `make -C oracle ref_gpu`), driven
+    through oracle/ref_gpu_capi.cpp.  Baseline timing only."""
+
+    def __init__(self, pos: np.ndarray, tris: np.ndarray, cost_intersect: float = 0.4):
+        lib = C.CDLL(os.path.join(REF_DIR, "libbtref_gpu.so"))
+        lib.btrg_available.restype = C.c_int
+        lib.btrg_create.restype = C.c_void_p
+        lib.btrg_create.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double]
+        lib.btrg_soft.restype = None
+        lib.btrg_soft.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.btrg_destroy.restype = None
+        lib.btrg_destroy.argtypes = [C.c_void_p]
+        self.lib = lib
+        pos = np.ascontiguousarray(pos, np.float32)
+        tris = np.ascontiguousarray(tris, np.uint32)
+        self.h = lib.btrg_create(pos.ctypes.data, len(pos), tris.ctypes.data, len(tris), float(cost_intersect))
+
+    def soft(self, cam, W, H, light, exact=True) -> dict:
+        """GpuRenderer::softShadows; timing = primary s, trace s, kernel s,
+        CPU-fallback s, overflow pixels (gpu_render.h:59-64)."""
+        n = W * H
+        tri = np.zeros(n, np.int32)
+        vis, E = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        tm = np.zeros(5)
+        cam = np.ascontiguousarray(cam, np.float64)
+        light = np.ascontiguousarray(light, np.float64)
+        self.lib.btrg_soft(self.h, cam.ctypes.data, int(W), int(H), light.ctypes.data, int(exact), tri.ctypes.data,
+                           vis.ctypes.data, E.ctypes.data, tm.ctypes.data)
+        return dict(tri=tri, vis=vis, E=E, primary_s=tm[0], trace_s=tm[1], kernel_s=tm[2], fallback_s=tm[3],
+                    overflow_px=int(tm[4]))
+
+    def close(self):
+        if self.h:
+            self.lib.btrg_destroy(self.h)
+            self.h = None
