@@ -153,31 +153,6 @@ struct RoundParams {
 
 __device__ __forceinline__ int laneId() { return threadIdx.x & 31; }
 
-// The current root-to-node path of a tracing lane, in shared memory: entry
-// k (the node at depth k) at col[k * kThreads], so the lanes of a warp hit
-// distinct banks.  Entries [known, depth) are valid; a record fresh from
-// the queue knows none and fills them from parent links on its first climb
-// below `known` (the reference's own walk, done once per record).
-constexpr int kPathDepth = 64;  // the restart trail has 64 bits
-struct PathCache {
-  uint32_t* col;
-  int known;
-  __device__ __forceinline__ void begin(int depth) { known = depth; }
-  __device__ __forceinline__ void descend(int depth, uint32_t node) {
-    if (depth < kPathDepth) col[depth * kThreads] = node;
-  }
-  __device__ __forceinline__ uint32_t ancestor(const SceneDev& s, uint32_t node, int depth, int d) {
-    if (d >= known) return col[d * kThreads];
-    uint32_t x = known < depth ? col[known * kThreads] : node;
-    for (int k = known < depth ? known : depth; k > d; --k) {
-      x = __ldg(&s.parent[x]);
-      if (k - 1 < kPathDepth) col[(k - 1) * kThreads] = x;
-    }
-    known = d;
-    return x;
-  }
-};
-
 __device__ __forceinline__ float asF(int i) { return __int_as_float(i); }
 __device__ __forceinline__ int asI(float f) { return __float_as_int(f); }
 
@@ -625,10 +600,6 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
   Walk w;
   float lightArea = 0;
   int qRoot = -1;
-  __shared__ uint32_t pathStack[kPathDepth * kThreads];
-  PathCache path;
-  path.col = pathStack + threadIdx.x;
-  path.known = 0;
   bool outPending = false;
   int outTri = -1;
   Stats st;
@@ -655,7 +626,6 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
           }
           expand(p.s, q, r, b);
           walkBegin(p.s, r, w);
-          path.begin(r.depth);
           phase = kTrace;
         }
       }
@@ -666,17 +636,15 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
     }
     // one leaf: climb / descend to it, then test its triangles
     int res = kStepContinue;
-    int occ = -1;
     if (phase == kTrace) {
-      res = advance(p.s, q, b, r, w, st, path);
+      res = advance(p.s, q, b, r, w, st);
+      int occ = -1;
       if (res == kStepContinue) {
         for (;;) {
           res = testOne(p.s, q, r, b, st, occ);
           if (res != kStepContinue || !moreInLeaf(p.s, q, r)) break;
         }
       }
-    }
-    if (phase == kTrace) {
       if (res == kStepFinished) {
         outTri = occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1);
         if (outTri >= 0) st.hits++;
@@ -1064,7 +1032,7 @@ struct bt_gpu_ctx {
   int blocksSoft = 0, blocksPrimary = 0, blocksPoint = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t rev[2] = {nullptr, nullptr};
-  cudaEvent_t kev[32] = {};  // kernel_timing: 4 per round of a batch (before admit, trace, clip, after clip)
+  cudaEvent_t kev[32] = {};  // kernel_timing: 2 per round of a batch, around the trace kernel
 };
 
 extern "C" {
@@ -1227,7 +1195,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.stats = c->dStats;
   p.app = app;
   const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App>), gC = gridFor(c, clipKernel<App>);
-  static_assert(4 * kRoundsPerCheck <= 32, "kernel_timing events");
+  static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
   const bool ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
   // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
   FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
@@ -1258,13 +1226,11 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       CK(cudaEventRecord(c->rev[0], c->stream));
       for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
         p.cur = round & 1;
-        if (ktime) CK(cudaEventRecord(c->kev[4 * k], c->stream));
         admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 1], c->stream));
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
         traceKernel<App><<<gT, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 2], c->stream));
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
         clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[4 * k + 3], c->stream));
         roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
         launches += 4;
       }
@@ -1277,15 +1243,12 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       if (info) {
         info->ms_round += ms;
         info->round_launches += 3 * kRoundsPerCheck;
-        if (ktime) {
-          double* dst[3] = {&info->ms_kernel_admit, &info->ms_kernel_trace, &info->ms_kernel_clip};
-          for (int k = 0; k < kRoundsPerCheck; ++k)
-            for (int j = 0; j < 3; ++j) {
-              float t = 0;
-              CK(cudaEventElapsedTime(&t, c->kev[4 * k + j], c->kev[4 * k + j + 1]));
-              *dst[j] += t;
-            }
-        }
+        if (ktime)
+          for (int k = 0; k < kRoundsPerCheck; ++k) {
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, c->kev[2 * k], c->kev[2 * k + 1]));
+            info->ms_kernel_trace += t;
+          }
       }
       if (roundLog)
         fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d ms %.3f\n", pass, hc.rounds,

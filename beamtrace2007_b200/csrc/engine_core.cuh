@@ -192,12 +192,10 @@ BT_HD int highestBit64(unsigned long long x) {
 #endif
 }
 
-// Ancestors of the current kd node for the restart-trail climb.  The
-// reference walks parent links one level at a time; ParentClimb does the
-// same.  The kernels use a per-lane copy of the current root-to-node path
-// in shared memory instead (PathCache, engine.cu): the same nodes, found
-// without the chain of dependent loads.  Either way the climb counter
-// counts levels, as the reference's does.
+// Ancestors of the current kd node for the restart-trail climb: parent
+// links one level at a time, as the reference walks them.  (The step
+// functions take the walk as a parameter so that a cache of the current
+// path can stand in for it; the climb counter counts levels either way.)
 struct ParentClimb {
   BT_HD void begin(int) {}
   BT_HD void descend(int, uint32_t) {}

@@ -343,8 +343,8 @@ def main():
                     "d2h_bytes_per_step": npx * 16},
             "gpu_launches": int(sum(d["launches"] for d in infos)),
             "clocks": clk.summary(),
-            "kernels_ms_per_frame": {k: float(np.mean([d["ms_kernel_" + k] for d in infos]))
-                                     for k in ("admit", "trace", "clip")},
+            "kernels_ms_per_frame": {"trace": trace_ms,
+                                     "admit_clip_bookkeeping": float(np.mean([d["ms_round"] for d in infos])) - trace_ms},
             "counters": {k: last[k] for k in ("tri_tests", "kd_steps", "leaf_visits", "beams", "splits", "climbs",
                                                "rounds", "passes", "retried_roots", "max_spill")},
             "ms_primary": float(np.mean([d["ms_primary"] for d in infos])),

@@ -108,7 +108,7 @@ typedef struct {
   int32_t primary_budget;   /* live sub-beams per primary tile (wfPrimaryBudget) */
   int64_t capacity;         /* sub-beam records per spill queue (wfCapacity); 0 = from free memory */
   int32_t blocks_per_sm;    /* persistent CTAs per SM; 0 = occupancy */
-  int32_t kernel_timing;    /* nonzero: CUDA events between the round kernels fill ms_kernel_* */
+  int32_t kernel_timing;    /* nonzero: CUDA events around the trace kernels fill ms_kernel_trace */
   int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
 } bt_gpu_config;
 
@@ -130,7 +130,7 @@ typedef struct {
   int32_t passes, retried_roots, max_spill;
   int64_t roots;
   int32_t rounds;             /* rounds run (each: admit, trace, clip, bookkeeping launches) */
-  /* summed device time of the admit / trace / clip launches (kernel_timing only, else 0) */
+  /* summed device time of the trace launches (kernel_timing only, else 0); admit and clip reserved (0) */
   double ms_kernel_admit, ms_kernel_trace, ms_kernel_clip;
 } bt_run_info;
 
