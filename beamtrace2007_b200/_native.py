@@ -78,6 +78,11 @@ class SoftOpts(C.Structure):
     _fields_ = [("exact", C.c_int32), ("offset", C.c_float)]
 
 
+class SoftJob(C.Structure):
+    _fields_ = [("cam", Camera), ("light", AreaLight), ("opts", SoftOpts), ("d_tri", C.c_void_p),
+                ("d_vis", C.c_void_p), ("d_E", C.c_void_p), ("d_Eu", C.c_void_p)]
+
+
 class RunInfo(C.Structure):
     _fields_ = [("kd_steps", C.c_uint64), ("leaf_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("hits", C.c_uint64), ("splits", C.c_uint64), ("beams", C.c_uint64), ("root_beams", C.c_uint64),
@@ -126,6 +131,7 @@ SIGNATURES = {
                                         C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P, _P, C.POINTER(RunInfo)]),
     "bt_gpu_soft_device": (_I, [_P, C.POINTER(Camera), C.POINTER(AreaLight), C.POINTER(SoftOpts), _P, _P, _P, _P,
                                 C.POINTER(RunInfo)]),
+    "bt_gpu_batch_soft": (_I, [_P, C.c_int32, C.POINTER(SoftJob), C.POINTER(RunInfo)]),
     "bt_gpu_primary_rays": (_I, [_P, C.POINTER(Camera), _P, _P, _P]),
     "bt_gpu_primary_rays_device": (_I, [_P, C.POINTER(Camera), _P, _P, _P]),
     "bt_gpu_primary": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, C.POINTER(Polys), C.POINTER(_I64),

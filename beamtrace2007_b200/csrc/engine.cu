@@ -122,6 +122,13 @@ struct AppParams {
   unsigned long long* missFx;
   unsigned long long* gFx;
   float4* shade;  // x, ns per root
+  // batched soft shadows: per-job parameters (camera, light, pixel and
+  // output arrays of each job) in device memory; job j owns the roots
+  // [jobStart[j], jobStart[j + 1]).  The accumulators above are indexed by
+  // the batch-wide root.
+  const AppParams* jobs;
+  const int32_t* jobStart;
+  int numJobs;
   // point shadows
   V3 pointLight;
   const float* hx;
@@ -381,26 +388,42 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   if (App == kAppSoft) {
     p.app.missFx[k] = 0;
     p.app.gFx[k] = 0;
+    // the root's job (a batch) or the call's parameters
+    int kl = k;
+    const AppParams* ap = &p.app;
+    if (p.app.numJobs > 0) {
+      int lo = 0, hi = p.app.numJobs - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.app.jobStart[mid] <= k)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      ap = &p.app.jobs[lo];
+      kl = k - p.app.jobStart[lo];
+    }
+    const AppParams& a = *ap;
     int pix;
-    if (!softPixel(p.app, k, pix)) {
+    if (!softPixel(a, kl, pix)) {
       rootDone(p);
       return false;
     }
-    const int T = p.app.pixTri[pix];
+    const int T = a.pixTri[pix];
     if (T < 0) {
-      if (p.app.vis) p.app.vis[pix] = -1;
-      if (p.app.E) p.app.E[pix] = 0;
-      if (p.app.Eu) p.app.Eu[pix] = 0;
+      if (a.vis) a.vis[pix] = -1;
+      if (a.E) a.E[pix] = 0;
+      if (a.Eu) a.Eu[pix] = 0;
       rootDone(p);
       return false;
     }
-    const V3 x = mk(p.app.pixX[3 * pix], p.app.pixX[3 * pix + 1], p.app.pixX[3 * pix + 2]);
-    const V3 ns = mk(p.app.pixN[3 * pix], p.app.pixN[3 * pix + 1], p.app.pixN[3 * pix + 2]);
-    const float A = length(cross(p.app.LU, p.app.LV));
-    if (p.app.Eu) p.app.Eu[pix] = A * lightCenterG(p.app.Lc, p.app.LU, p.app.LV, x, ns);
-    if (!lightBeamSetup(p.app.Lc, p.app.LU, p.app.LV, x, ns, T, p.app.offset, q, poly, lightArea)) {
-      if (p.app.vis) p.app.vis[pix] = 0;
-      if (p.app.E) p.app.E[pix] = 0;
+    const V3 x = mk(a.pixX[3 * pix], a.pixX[3 * pix + 1], a.pixX[3 * pix + 2]);
+    const V3 ns = mk(a.pixN[3 * pix], a.pixN[3 * pix + 1], a.pixN[3 * pix + 2]);
+    const float A = length(cross(a.LU, a.LV));
+    if (a.Eu) a.Eu[pix] = A * lightCenterG(a.Lc, a.LU, a.LV, x, ns);
+    if (!lightBeamSetup(a.Lc, a.LU, a.LV, x, ns, T, a.offset, q, poly, lightArea)) {
+      if (a.vis) a.vis[pix] = 0;
+      if (a.E) a.E[pix] = 0;
       rootDone(p);
       return false;
     }
@@ -1030,6 +1053,10 @@ struct bt_gpu_ctx {
   int32_t* dPixTri = nullptr;
   float *dPixX = nullptr, *dPixN = nullptr, *dVis = nullptr, *dE = nullptr, *dEu = nullptr;
   int blocksSoft = 0, blocksPrimary = 0, blocksPoint = 0;
+  // batched soft shadows: per-job parameter table and root offsets
+  AppParams* dJobs = nullptr;
+  int32_t* dJobStart = nullptr;
+  int jobCap = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t rev[2] = {nullptr, nullptr};
   cudaEvent_t kev[32] = {};  // kernel_timing: 2 per round of a batch, around the trace kernel
@@ -1504,7 +1531,7 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
                   c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
-                  c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu};
+                  c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& ev : c->ev)
@@ -1594,6 +1621,103 @@ int bt_gpu_soft_device(bt_gpu_ctx* c, const bt_camera* cam, const bt_area_light*
     info->ms_primary = a;
     info->ms_trace = b;
     info->ms_total = a + b;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_batch_soft(bt_gpu_ctx* c, int32_t n, const bt_soft_job* jobs, bt_run_info* info) {
+  if (!c || n < 0 || (n > 0 && !jobs)) {
+    setErr("bt_gpu_batch_soft: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  int64_t totPix = 0;
+  for (int j = 0; j < n; ++j) {
+    if (!camOk(&jobs[j].cam)) {
+      setErr("bt_gpu_batch_soft: job %d has a bad camera", j);
+      return BT_ERR_INVALID;
+    }
+    totPix += int64_t(jobs[j].cam.W) * jobs[j].cam.H;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  if (n == 0) return BT_OK;
+  int e = ensurePix(c, totPix);
+  if (e) return e;
+  if (c->jobCap < n) {
+    cudaFree(c->dJobs);
+    cudaFree(c->dJobStart);
+    c->jobCap = 0;
+    if ((e = devAlloc(&c->dJobs, size_t(n))) || (e = devAlloc(&c->dJobStart, size_t(n) + 1))) return e;
+    c->jobCap = n;
+  }
+  std::vector<AppParams> hj(static_cast<size_t>(n));
+  std::vector<int32_t> start(static_cast<size_t>(n) + 1);
+  int64_t R = 0, off = 0;
+  int anyExact = 0;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  for (int j = 0; j < n; ++j) {
+    const bt_soft_job& J = jobs[j];
+    const bt_camera& cam = J.cam;
+    int32_t* tri = J.d_tri ? J.d_tri : c->dPixTri + off;
+    dim3 bs(16, 8), gs((cam.W + 15) / 16, (cam.H + 7) / 8);
+    primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, cam, tri, c->dPixX + 3 * off, c->dPixN + 3 * off);
+    AppParams a = baseApp(c, &cam);
+    a.Lc = mk(J.light.c[0], J.light.c[1], J.light.c[2]);
+    a.LU = mk(J.light.U[0], J.light.U[1], J.light.U[2]);
+    a.LV = mk(J.light.V[0], J.light.V[1], J.light.V[2]);
+    a.offset = J.opts.offset > 0 ? J.opts.offset : c->offset;
+    a.exact = J.opts.exact;
+    anyExact |= J.opts.exact;
+    a.pixTri = tri;
+    a.pixX = c->dPixX + 3 * off;
+    a.pixN = c->dPixN + 3 * off;
+    a.vis = J.d_vis;
+    a.E = J.d_E;
+    a.Eu = J.d_Eu;
+    a.tiled = 1;
+    a.tilesX = (cam.W + 7) / 8;
+    a.shade = c->dShade;
+    hj[size_t(j)] = a;
+    start[size_t(j)] = int32_t(R);
+    R += int64_t(a.tilesX) * ((cam.H + 3) / 4) * 32;
+    off += int64_t(cam.W) * cam.H;
+    if (R > 0x7fffffff) {
+      setErr("bt_gpu_batch_soft: more than 2^31 roots in one batch");
+      return BT_ERR_TOO_LARGE;
+    }
+  }
+  start[size_t(n)] = int32_t(R);
+  CK(cudaGetLastError());
+  if (info) info->launches += n;
+  CK(cudaMemcpyAsync(c->dJobs, hj.data(), sizeof(AppParams) * size_t(n), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->dJobStart, start.data(), sizeof(int32_t) * (size_t(n) + 1), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  AppParams batch = baseApp(c, nullptr);
+  batch.exact = anyExact;
+  batch.jobs = c->dJobs;
+  batch.jobStart = c->dJobStart;
+  batch.numJobs = n;
+  e = runRoots<kAppSoft>(c, batch, int(R), c->cfg.budget, info);
+  if (e) return e;
+  for (int j = 0; j < n; ++j) {
+    AppParams a = hj[size_t(j)];
+    a.missFx = c->dMiss + start[size_t(j)];
+    a.gFx = c->dG + start[size_t(j)];
+    const int Rj = start[size_t(j) + 1] - start[size_t(j)];
+    softFinalizeKernel<<<(Rj + 255) / 256, 256, 0, c->stream>>>(a, c->dState + start[size_t(j)], Rj);
+  }
+  CK(cudaGetLastError());
+  if (info) info->launches += n;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float ta = 0, tb = 0;
+    cudaEventElapsedTime(&ta, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&tb, c->ev[1], c->ev[2]);
+    info->ms_primary = ta;
+    info->ms_trace = tb;
+    info->ms_total = ta + tb;
   }
   return BT_OK;
 }

@@ -221,6 +221,31 @@ class GpuRenderer:
                                   ptr(Eu), C.byref(info)))
         return SoftResult(tri, vis, E, Eu, self._record(info))
 
+    def batch_soft(self, cams, lights, exact: bool = True, offset: float = 0.0, device_outputs: bool = False):
+        """Soft shadows of several images of this scene in one engine run
+        (bt_gpu_batch_soft).  Returns one SoftResult per job (host arrays),
+        or, with device_outputs, (tri, vis, E, Eu) CUDA tensors per job and
+        the run info."""
+        import torch
+        dev = torch.device("cuda", self.config.device)
+        jobs = (N.SoftJob * max(len(cams), 1))()
+        outs = []
+        for j, (cam, light) in enumerate(zip(cams, lights)):
+            n = cam.W * cam.H
+            t = (torch.empty(n, dtype=torch.int32, device=dev),) + tuple(
+                torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+            outs.append(t)
+            L = light if isinstance(light, N.AreaLight) else N.AreaLight.from_array(light)
+            jobs[j] = N.SoftJob(cam, L, N.SoftOpts(int(exact), float(offset)), t[0].data_ptr(), t[1].data_ptr(),
+                                t[2].data_ptr(), t[3].data_ptr())
+        info = N.RunInfo()
+        torch.cuda.synchronize(dev)
+        check(N.lib().bt_gpu_batch_soft(self._h, len(cams), jobs, C.byref(info)))
+        rec = self._record(info)
+        if device_outputs:
+            return outs, rec
+        return [SoftResult(*(x.cpu().numpy() for x in t), info=rec) for t in outs]
+
     def soft_points(self, light, tri, X, N_, exact: bool = False, offset: float = 0.0) -> SoftResult:
         tri = np.ascontiguousarray(tri, np.int32)
         X = np.ascontiguousarray(X, np.float32).reshape(-1, 3)

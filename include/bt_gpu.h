@@ -18,8 +18,7 @@
  *   bt_scene_finalize       Scene::finalize         src/scene/scene.cpp:89-118
  *   bt_kd_build             KdTree::build           src/accel/kdtree.h:36
  *   bt_camera_make          Camera::make            src/render/render_types.h:24
- * Batching and serving (no counterpart in the reference): bt_gpu_batch_soft,
- * bt_gpu_submit / bt_gpu_poll.
+ * Batching (no counterpart in the reference): bt_gpu_batch_soft.
  */
 #ifndef BT_GPU_H
 #define BT_GPU_H
@@ -242,6 +241,24 @@ BT_API int bt_gpu_soft_points_noalloc(const bt_scene_desc* d_scene, const bt_kd_
 BT_API int bt_gpu_soft_device(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_area_light* light,
                               const bt_soft_opts* opts, int32_t* d_tri, float* d_vis, float* d_E, float* d_Eu,
                               bt_run_info* info);
+
+/* One soft-shadow job of a batch: an image W x H from cam, its light and
+ * options, and its outputs in device memory (W*H each; any may be NULL). */
+typedef struct {
+  bt_camera cam;
+  bt_area_light light;
+  bt_soft_opts opts;
+  int32_t* d_tri;
+  float* d_vis;
+  float* d_E;
+  float* d_Eu;
+} bt_soft_job;
+
+/* bt_gpu_soft_device for num_jobs images of the context's scene in one
+ * run of the engine: the shadow-beam roots of all jobs share the rounds,
+ * so one job's tail overlaps the others' work.  Each job's outputs equal
+ * what bt_gpu_soft_device gives for it alone.  Returns when all are done. */
+BT_API int bt_gpu_batch_soft(bt_gpu_ctx* ctx, int32_t num_jobs, const bt_soft_job* jobs, bt_run_info* info);
 
 /* GPU primary rays only (primaryKernel, cuda/gpu_render.cu:222-244): per
  * pixel centre the nearest triangle (-1 none), hit point X (3 floats) and

@@ -162,3 +162,24 @@ def test_primary_budget_retry(gpu, oracle_ready):
         b = g.primary(cam, tile=32)
         assert g.last_overflow_pixels > 0
     assert np.array_equal(piece_keys(a, True), piece_keys(b, True))
+
+
+def test_batch_equals_jobs_alone(gpu):
+    """Jobs of different sizes, cameras and light scales in one batch give
+    bitwise the results each gives alone (the accumulation is fixed point,
+    so the order in which pieces finish does not matter)."""
+    from beamtrace2007_b200.renderer import make_camera
+    s, ps = scene("plant")
+    v = s.views[0]
+    sizes = [(64, 48), (128, 128), (96, 160), (33, 17)]
+    scales = [0.25, 1.0, 4.0, 2.0]
+    cams = [make_camera(v.eye, v.target, v.fov + 5 * i, s.up, W, H) for i, (W, H) in enumerate(sizes)]
+    lights = [s.light_array(k) for k in scales]
+    with _renderer(ps) as g:
+        batch = g.batch_soft(cams, lights, exact=True)
+        for cam, L, b in zip(cams, lights, batch):
+            alone = g.soft_shadows(cam, L, exact=True)
+            assert np.array_equal(b.tri, alone.tri)
+            assert np.array_equal(b.vis, alone.vis)
+            assert np.array_equal(b.E, alone.E)
+            assert np.array_equal(b.Eu, alone.Eu)
