@@ -657,7 +657,10 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
       if (exhausted) break;
       continue;
     }
-    // one leaf: climb / descend to it, then test its triangles
+    // Per step a lane moves its record to the next leaf cell that holds a
+    // triangle to test (descents, trail pops), then tests that leaf's
+    // triangles in order until one needs a clip, the beam is finished, or
+    // the leaf is exhausted.
     int res = kStepContinue;
     if (phase == kTrace) {
       res = advance(p.s, q, b, r, w, st);
