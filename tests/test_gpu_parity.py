@@ -183,3 +183,24 @@ def test_batch_equals_jobs_alone(gpu):
             assert np.array_equal(b.vis, alone.vis)
             assert np.array_equal(b.E, alone.E)
             assert np.array_equal(b.Eu, alone.Eu)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_soft_points_vs_golden_and_restatement(gpu, k):
+    """Supplied shading points (the committed fixture: the reference's own
+    primary-ray points and its FP64 results, light scales 1 and 4): the GPU
+    within 1e-4 of the reference's double build and of the independent FP64
+    restatement (oracle/restate_soft.py)."""
+    import os
+    from conftest import ROOT
+    from restate_soft import soft_points
+    g = np.load(os.path.join(ROOT, "tests", "golden", "plant_soft_points.npz"))
+    s, ps = scene("plant")
+    L = g[f"light{k}"]
+    with _renderer(ps) as r:
+        res = r.soft_points(L, g["tri"], g["X"], g["N"], exact=True, offset=float(g["offset"]))
+    assert np.abs(res.vis.astype(np.float64) - g[f"vis{k}"]).max() <= VIS_TOL
+    vr, Er = soft_points(ps.pos, ps.tris, L, float(g["offset"]), g["tri"], g["X"].astype(np.float64),
+                         g["N"].astype(np.float64))
+    assert np.abs(res.vis.astype(np.float64) - vr).max() <= VIS_TOL
+    assert np.abs(res.E.astype(np.float64) - Er).max() <= E_REL * np.abs(Er).max()
