@@ -528,7 +528,8 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   Line L[5];
   int nl = 0;
   bool commit = false;
-  const int slots = splitPass1<SplitEnv<App>>(p.s, q, rec, b, st, ti, L, nl, commit);
+  PieceLog log;
+  const int slots = splitPass1<SplitEnv<App>>(p.s, q, rec, b, st, ti, L, nl, commit, &log);
   if (slots < 0) {
     killRoot(p, root);
     liveSub(p, root, 1);
@@ -553,7 +554,7 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   env.st = &st;
   env.written = 0;
   env.nbuf = 0;
-  splitPass2(q, rec, b, ti, L, nl, env, st);
+  splitPass2(q, rec, b, ti, L, nl, env, st, &log);
   env.flush();
   // slivers dropped by beamGeom were counted in `slots` but never queued
   if (env.written < slots) liveSub(p, root, slots - env.written);

@@ -468,13 +468,41 @@ struct EmitSink {
   }
 };
 
-// One clipper instance per environment: measure (pass 1) or emit (pass 2).
+// The pieces of pass 1 in push order, so that pass 2 can emit them without
+// clipping again (pieces have at most 5 corners; a clip with more than
+// kPieceLog pieces is replayed instead).
+constexpr int kPieceLog = 8;
+struct PieceLog {
+  int count;
+  int8_t level[kPieceLog], n[kPieceLog];
+  float x[kPieceLog][5], y[kPieceLog][5];
+  BT_HD void add(int l, const Poly<kPolyMax>& p) {
+    if (count < kPieceLog) {
+      level[count] = int8_t(l);
+      n[count] = int8_t(p.n);
+      for (int i = 0; i < 5; ++i) {
+        x[count][i] = i < p.n ? p.x[i] : 0.f;
+        y[count][i] = i < p.n ? p.y[i] : 0.f;
+      }
+    }
+    ++count;
+  }
+};
+
+// One clipper instance per environment: measure (pass 1, optionally
+// logging the pieces) or emit (pass 2).
 template <class Env>
 struct ClipSink {
   int emitting;
   AreaSink area;
   EmitSink<Env> emit;
-  BT_HD bool push(int l, const Poly<kPolyMax>& p) { return emitting ? emit.push(l, p) : area.push(l, p); }
+  PieceLog* log;
+  BT_HD bool push(int l, const Poly<kPolyMax>& p) {
+    if (emitting) return emit.push(l, p);
+    if (!area.push(l, p)) return false;
+    if (log) log->add(l, p);
+    return true;
+  }
 };
 
 // Clip of a record whose pending triangle needs it (after testOne returned
@@ -485,7 +513,7 @@ struct ClipSink {
 // (0 if nothing changes: the record continues unchanged at cursor + 1).
 template <class Env>
 BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
-                       Line* L, int& nl, bool& commit) {
+                       Line* L, int& nl, bool& commit, PieceLog* log = nullptr) {
   const uint2 leaf = s.node[r.node];
   setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
   classifyTri(q, B, ti, L, nl);
@@ -494,6 +522,8 @@ BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, cons
   ClipSink<Env> sink;
   sink.emitting = 0;
   sink.area = AreaSink{0.f, 0, 0};
+  sink.log = log;
+  if (log) log->count = 0;
   uint32_t five = 0;
   if (!clipTri<kPolyMax>(q, B, Lc, nl, sink, five)) return -1;
   st.fiveSplits += five;
@@ -504,13 +534,28 @@ BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, cons
 
 template <class Env>
 BT_COLD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
-                        Stats& st) {
+                        Stats& st, const PieceLog* log = nullptr) {
   st.splits++;
   SubBeam base = r;
   base.cursor = r.cursor + 1;
+  EmitSink<Env> emit{&q, &base, &B, ti.tri, &env, &st};
+  if (log && log->count <= kPieceLog) {
+    // the same pieces in the same order as a replayed clip would push them
+    for (int k = 0; k < log->count; ++k) {
+      Poly<kPolyMax> p;
+      p.n = log->n[k];
+      for (int i = 0; i < kPolyMax; ++i) {
+        p.x[i] = i < 5 ? log->x[k][i] : 0.f;
+        p.y[i] = i < 5 ? log->y[k][i] : 0.f;
+      }
+      emit.push(log->level[k], p);
+    }
+    return;
+  }
   ClipSink<Env> sink;
   sink.emitting = 1;
-  sink.emit = EmitSink<Env>{&q, &base, &B, ti.tri, &env, &st};
+  sink.emit = emit;
+  sink.log = nullptr;
   uint32_t five = 0;  // counted in pass 1
   clipTri<kPolyMax>(q, B, L, nl, sink, five);
 }

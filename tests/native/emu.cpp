@@ -115,7 +115,8 @@ void traceRoot(const SceneDev& s, const Query& q, const Poly<8>& poly, std::vect
         Line L[5];
         int nl = 0;
         bool commit = false;
-        int slots = splitPass1<RootEnv>(s, q, r, b, st, ti, L, nl, commit);
+        PieceLog log;
+        int slots = splitPass1<RootEnv>(s, q, r, b, st, ti, L, nl, commit, &log);
         if (slots < 0) {
           out.clear();
           return;
@@ -125,7 +126,7 @@ void traceRoot(const SceneDev& s, const Query& q, const Poly<8>& poly, std::vect
           w.phase = kPhTest;
           continue;
         }
-        splitPass2(q, r, b, ti, L, nl, env, st);
+        splitPass2(q, r, b, ti, L, nl, env, st, &log);
         break;
       }
     }
