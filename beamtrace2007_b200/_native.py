@@ -71,7 +71,7 @@ class GpuInfo(C.Structure):
 class GpuConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("budget", C.c_int32), ("primary_budget", C.c_int32),
                 ("capacity", C.c_int64), ("blocks_per_sm", C.c_int32), ("kernel_timing", C.c_int32),
-                ("max_retries", C.c_int32)]
+                ("max_retries", C.c_int32), ("tail_records", C.c_int64)]
 
 
 class SoftOpts(C.Structure):
@@ -91,7 +91,7 @@ class RunInfo(C.Structure):
                 ("ms_primary", C.c_double), ("ms_trace", C.c_double), ("ms_total", C.c_double),
                 ("ms_round", C.c_double), ("launches", C.c_int32), ("round_launches", C.c_int32),
                 ("passes", C.c_int32), ("retried_roots", C.c_int32), ("max_spill", C.c_int32),
-                ("roots", C.c_int64), ("rounds", C.c_int32), ("ms_kernel_admit", C.c_double),
+                ("roots", C.c_int64), ("rounds", C.c_int32), ("tail_rounds", C.c_int32), ("ms_kernel_admit", C.c_double),
                 ("ms_kernel_trace", C.c_double), ("ms_kernel_clip", C.c_double)]
 
     def as_dict(self) -> dict:

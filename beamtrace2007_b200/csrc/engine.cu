@@ -331,6 +331,8 @@ struct SplitEnv {
   Stats* st;
   int written;
   int nbuf;
+  SubBeam* keep;  // tail rounds: the first piece stays with the clipping lane
+  bool kept;
   SubBeam buf[kChunk];
   __device__ void flush() {
     if (nbuf == 0) return;
@@ -342,6 +344,12 @@ struct SplitEnv {
     nbuf = 0;
   }
   __device__ bool queue(const SubBeam& r) {
+    if (keep && !kept) {
+      *keep = r;
+      kept = true;
+      ++written;
+      return true;
+    }
     buf[nbuf++] = r;
     if (nbuf == kChunk) flush();
     return true;
@@ -511,7 +519,8 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
 // measurable changed and the record (updated in place) continues at the next
 // triangle.  Works on its own query and beam: the caller's stay in registers.
 template <int App>
-__device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Stats* cs) {
+__device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Stats* cs, SubBeam* keep = nullptr,
+                                        bool* kept = nullptr) {
   Stats& st = *cs;
   SubBeam rec = *recp;
   const int root = rec.root;
@@ -554,8 +563,11 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   env.st = &st;
   env.written = 0;
   env.nbuf = 0;
+  env.keep = keep;
+  env.kept = false;
   splitPass2(q, rec, b, ti, L, nl, env, st, &log);
   env.flush();
+  if (kept) *kept = env.kept;
   // slivers dropped by beamGeom were counted in `slots` but never queued
   if (env.written < slots) liveSub(p, root, slots - env.written);
   return false;
@@ -610,7 +622,7 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // record leaf by leaf until it finishes or a triangle needs a clip; idle
 // lanes are refilled at once (one atomic per warp, ballot/popc ranks).
 // Records needing a clip are compacted into the clip queue.
-template <int App>
+template <int App, bool Fused>
 __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
@@ -674,11 +686,34 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
       }
       if (res == kStepFinished) {
         outTri = occ >= 0 ? occ : (q.mode == kModeNearest ? b.hit : -1);
-        if (outTri >= 0) st.hits++;
-        st.beams++;
-        outPending = App == kAppSoft ? outTri < 0 : outTri >= 0;  // soft keeps the visible light, the others the hits
+        if (Fused) {
+          outputPiece<App>(p, q, lightArea, r.root, b, outTri, st);
+        } else {
+          if (outTri >= 0) st.hits++;
+          st.beams++;
+          outPending = App == kAppSoft ? outTri < 0 : outTri >= 0;  // soft keeps the visible light, the others the hits
+        }
         liveSub(p, r.root, 1);
         phase = kIdle;
+      }
+      if (Fused && res == kStepSplit) {
+        // Tail rounds: clip here and go on with one of the pieces, so that a
+        // chain of splits advances several levels per round.
+        SubBeam kept;
+        bool hasKept = false;
+        Stats cs;
+        cs.clear();
+        if (clipRecord<App>(p, &r, &cs, &kept, &hasKept)) {
+          w.phase = kPhTest;  // nothing changed measurably: the next triangle
+        } else if (hasKept) {
+          r = kept;
+          expand(p.s, q, r, b);
+          walkBegin(p.s, r, w);
+        } else {
+          phase = kIdle;
+        }
+        addStats(st, cs);
+        res = kStepContinue;
       }
     }
     // Finished pieces are output by the clip kernel, all lanes at once
@@ -1078,6 +1113,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->blocks_per_sm = 0;
   c->kernel_timing = 0;
   c->max_retries = 4;
+  c->tail_records = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1225,12 +1261,15 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.ctr = c->dCtr;
   p.stats = c->dStats;
   p.app = app;
-  const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App>), gC = gridFor(c, clipKernel<App>);
+  const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App, false>),
+            gC = gridFor(c, clipKernel<App>), gF = gridFor(c, traceKernel<App, true>);
+  // tail rounds: every root admitted and fewer queued records than this
+  const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads;
   static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
   const bool ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
   // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
   FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
-  int launches = 0, passes = 0, retried = 0, roundsRun = 0;
+  int launches = 0, passes = 0, retried = 0, roundsRun = 0, tailRounds = 0;
   const int32_t* list = nullptr;
   int n = R;
   Counters hc;
@@ -1255,15 +1294,26 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     ++passes;
     for (int round = 0;;) {
       CK(cudaEventRecord(c->rev[0], c->stream));
+      // the mode of this batch of rounds, from the counters of the last one
+      const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
+                        c->cfg.tail_records >= 0;
       for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
         p.cur = round & 1;
-        admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
-        traceKernel<App><<<gT, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
-        clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
+        if (tail) {
+          if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+          traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
+          if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+          launches += 2;
+          tailRounds++;
+        } else {
+          admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
+          if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+          traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
+          if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+          clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
+          launches += 4;
+        }
         roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
-        launches += 4;
       }
       CK(cudaEventRecord(c->rev[1], c->stream));
       CK(cudaGetLastError());
@@ -1316,6 +1366,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   }
   if (info) {
     info->rounds += roundsRun;
+    info->tail_rounds += tailRounds;
     info->launches += launches;
     info->passes += passes;
     info->retried_roots += retried;

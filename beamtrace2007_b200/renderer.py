@@ -162,7 +162,8 @@ class GpuRenderer:
     on one GPU for the renderer's lifetime."""
 
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
-                 capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False):
+                 capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
+                 tail_records: int = 0):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -172,6 +173,7 @@ class GpuRenderer:
         cfg.capacity = capacity
         cfg.blocks_per_sm = blocks_per_sm
         cfg.kernel_timing = int(kernel_timing)
+        cfg.tail_records = int(tail_records)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()

@@ -109,6 +109,8 @@ typedef struct {
   int32_t blocks_per_sm;    /* persistent CTAs per SM; 0 = occupancy */
   int32_t kernel_timing;    /* nonzero: CUDA events around the trace kernels fill ms_kernel_trace */
   int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
+  int64_t tail_records;     /* tail rounds (one fused trace-and-clip kernel) below this many queued
+                               records once every root is admitted; 0 = the trace grid's lanes, < 0 = never */
 } bt_gpu_config;
 
 typedef struct {
@@ -129,6 +131,7 @@ typedef struct {
   int32_t passes, retried_roots, max_spill;
   int64_t roots;
   int32_t rounds;             /* rounds run (each: admit, trace, clip, bookkeeping launches) */
+  int32_t tail_rounds;        /* of those, tail rounds (fused trace and clip, bookkeeping) */
   /* summed device time of the trace launches (kernel_timing only, else 0); admit and clip reserved (0) */
   double ms_kernel_admit, ms_kernel_trace, ms_kernel_clip;
 } bt_run_info;
