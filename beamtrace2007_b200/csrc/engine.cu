@@ -176,6 +176,10 @@ __device__ void storeRoot(RootRec* R, const Query& q, float lightArea, int attem
 
 // Per-root records are written during the launch by the admitting SM; they
 // are read from L2 (an L1 line could hold a neighbouring root's older copy).
+// Soft- and point-shadow queries are always AnyHit with the far plane and
+// no culling (lightBeamSetup, pointShadowSetup); stating that at compile
+// time drops the Nearest-mode hit-plane state and code from those kernels.
+template <int App>
 __device__ __forceinline__ void loadRoot(const RootRec* R, Query& q, float& lightArea) {
   const float4 a = __ldcg(&R->a), b = __ldcg(&R->b), c = __ldcg(&R->c), d = __ldcg(&R->d), e = __ldcg(&R->e),
                f = __ldcg(&R->f);
@@ -187,9 +191,9 @@ __device__ __forceinline__ void loadRoot(const RootRec* R, Query& q, float& ligh
   q.P.d = mk(f.x, f.y, f.z);
   q.exclude = asI(b.w);
   const int fl = asI(d.w);
-  q.mode = fl & 1;
-  q.farIsPlane = (fl >> 1) & 1;
-  q.cull = (fl >> 2) & 1;
+  q.mode = App == kAppPrimary ? (fl & 1) : int(kModeAnyHit);
+  q.farIsPlane = App == kAppPrimary ? (fl >> 1) & 1 : 1;
+  q.cull = App == kAppPrimary ? (fl >> 2) & 1 : 0;
   lightArea = c.w;
   querySetup(q, a.w);
 }
@@ -531,7 +535,7 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   Query q;
   float lightArea;
   Beam b;
-  loadRoot(&p.roots[root], q, lightArea);
+  loadRoot<App>(&p.roots[root], q, lightArea);
   expand(p.s, q, rec, b);
   TriInfo ti;
   Line L[5];
@@ -622,8 +626,10 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // record leaf by leaf until it finishes or a triangle needs a clip; idle
 // lanes are refilled at once (one atomic per warp, ballot/popc ranks).
 // Records needing a clip are compacted into the clip queue.
+// (At least 3 CTAs per SM: lets the compiler keep the lane's state in up to
+// 170 registers; at 4 CTAs it spills, which costs more than the warps gain.)
 template <int App, bool Fused>
-__global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ RoundParams p) {
+__global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
   const int nCur = min(p.ctr->count[p.cur], p.capacity);
@@ -657,7 +663,7 @@ __global__ void __launch_bounds__(kThreads) traceKernel(const __grid_constant__ 
           liveSub(p, r.root, 1);  // a dropped sliver or an abandoned root
         } else {
           if (r.root != qRoot) {
-            loadRoot(&p.roots[r.root], q, lightArea);
+            loadRoot<App>(&p.roots[r.root], q, lightArea);
             qRoot = r.root;
           }
           expand(p.s, q, r, b);
@@ -795,7 +801,7 @@ __global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ R
         PieceOut po;
         float lightArea;
         Query q;
-        loadRoot(&p.roots[o.root], q, lightArea);
+        loadRoot<App>(&p.roots[o.root], q, lightArea);
         po.P = q.P;
         for (int k = 0; k < 4; ++k) {
           po.qx[k] = o.qx[k];
