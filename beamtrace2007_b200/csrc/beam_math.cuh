@@ -45,7 +45,10 @@ enum { kNear = 0, kFar = 1, kBoth = 2 };                 // kd decisions
 enum { kTriKeep = 0, kTriAllIn = 1, kTriClip = 2 };      // beam-triangle outcome
 enum { kModeNearest = 0, kModeAnyHit = 1 };
 
-BT_HD float fabs_(float x) { return x < 0 ? -x : x; }
+// |x| as the FP unit's operand modifier.  It differs from x < 0 ? -x : x only
+// in the sign of a zero, and every use here is compared or feeds a tolerance
+// that is compared, where -0 and +0 are equal.
+BT_HD float fabs_(float x) { return fabsf(x); }
 
 struct V3 {
   float x, y, z;

@@ -207,10 +207,13 @@ struct ParentClimb {
 
 // One node visit of the descent (the inner loop of wfAdvance,
 // wavefront_core.h:163-189): a kd step into the child the beam enters
-// (false), or the leaf is reached (true: cursor 0, leaf counted).
+// (false), or the leaf is reached (true: cursor 0, leaf counted).  `nd`
+// holds the current node's record on entry and the entered child's on
+// return: both children are loaded while the slab test runs, so the next
+// step does not wait for its load.
 template <class Anc>
-BT_HD bool descendStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc) {
-  const uint2 nd = s.node[r.node];
+BT_HD bool descendStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc,
+                       uint2& nd) {
   if (isLeaf(nd)) {
     r.cursor = 0;
     st.leafVisits++;
@@ -224,6 +227,7 @@ BT_HD bool descendStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam
   const bool pos = !((B.neg >> a) & 1);
   const float Ns = (pos ? 1.f : -1.f) * (sp - comp(q.P.O, a));
   const uint32_t left = r.node + 1, right = nd.y >> 2;
+  const uint2 ndLeft = s.node[left], ndRight = s.node[right];
   const uint32_t cs = pos ? right : left, co = pos ? left : right;
   int dec = kFar;
   if (Ns > 0) dec = decide(q, B, a, Ns, w.box);
@@ -231,6 +235,7 @@ BT_HD bool descendStep(const SceneDev& s, const Query& q, const Beam& B, SubBeam
   const bool goRight = dec == kFar ? pos : !pos;
   if (dec == kBoth) r.trail |= 1ull << d;
   r.node = dec == kFar ? cs : co;
+  nd = goRight ? ndRight : ndLeft;
   if (goRight)
     boxSetLo(w.box, a, sp);
   else
@@ -282,7 +287,8 @@ template <class Anc>
 BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, Walk& w, Stats& st, Anc& anc) {
   for (;;) {
     if (w.phase == kPhDescend) {
-      while (!descendStep(s, q, B, r, w, st, anc)) {
+      uint2 nd = s.node[r.node];
+      while (!descendStep(s, q, B, r, w, st, anc, nd)) {
       }
       w.phase = kPhTest;
     }
