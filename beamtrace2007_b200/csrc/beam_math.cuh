@@ -171,6 +171,22 @@ struct Line {
 
 // Normalised line; a line ~1e9 extents away (or parallel) becomes the
 // constant sign(c) (beam_geom.h:65-76).
+// |D| > kDegRel * length(m) * length(r), computed in float exactly as the
+// triangle setup computes it (beam_core.h:260-286).  The square roots are
+// needed only when the two sides lie within 1e-4 of each other: comparing
+// squares (relative error below 1e-6) decides every other case the same way.
+BT_HD bool notEdgeOn(float D, V3 m, V3 r) {
+  const float mm = dot(m, m), rr = dot(r, r);
+  const float D2 = D * D;
+  const float T = (kDegRel * kDegRel) * mm * rr;
+  if (T > 1e-30f && T < 1e30f && D2 < 1e30f) {
+    if (D2 > T * 1.0001f) return true;
+    if (D2 < T * 0.9999f) return false;
+  }
+  const float scale = sqrtf(mm) * sqrtf(rr);
+  return (D < 0 ? -D : D) > kDegRel * scale;
+}
+
 BT_HD Line makeLine(float a, float b, float c, float ext) {
   Line L{0, 0, 0};
   float nrm = sqrtf(a * a + b * b);

@@ -367,8 +367,7 @@ BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats&
   ti.r[2] = sub(t.v2, q.P.O);
   const V3 m0 = edgePlane(ti.r, t.vi, 0, 1);
   const float D = dot(ti.r[2], m0);
-  const float scale = length(m0) * length(ti.r[2]);
-  if (!((D < 0 ? -D : D) > kDegRel * scale)) return kStepContinue;  // edge-on: not a test
+  if (!notEdgeOn(D, m0, ti.r[2])) return kStepContinue;  // edge-on: not a test
   if (q.cull && D > 0) return kStepContinue;                        // back-facing
   st.triTests++;
   if (B.hit == t.tri) return kStepContinue;
