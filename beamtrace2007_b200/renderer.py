@@ -241,7 +241,8 @@ class GpuRenderer:
             jobs[j] = N.SoftJob(cam, L, N.SoftOpts(int(exact), float(offset)), t[0].data_ptr(), t[1].data_ptr(),
                                 t[2].data_ptr(), t[3].data_ptr())
         info = N.RunInfo()
-        torch.cuda.synchronize(dev)
+        # (the engine runs on its own stream and returns when its outputs
+        # are written; nothing of torch's writes to these buffers)
         check(N.lib().bt_gpu_batch_soft(self._h, len(cams), jobs, C.byref(info)))
         rec = self._record(info)
         if device_outputs:

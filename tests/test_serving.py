@@ -1,0 +1,103 @@
+"""The serving loop (beamtrace2007_b200/serving.py): admission by memory
+budget and continuous batching (CPU, with a stand-in engine), and on the
+GPU a mixed Poisson stream over three resident scenes whose every result is
+bitwise the result of the same request run alone."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from conftest import scene
+
+
+class FakeEngine:
+    """Stands in for a GpuRenderer: records what ran together."""
+    log = []
+    lock = threading.Lock()
+
+    def __init__(self, ps, capacity):
+        self.ps = ps
+
+    def _note(self, what):
+        with FakeEngine.lock:
+            FakeEngine.log.append(what)
+        time.sleep(0.02)
+
+    def batch_soft(self, cams, lights, exact=True):
+        self._note(("batch", len(cams)))
+        from beamtrace2007_b200.renderer import SoftResult
+        return [SoftResult(np.zeros(c.W * c.H, np.int32), np.full(c.W * c.H, float(L[0]), np.float32),
+                           np.zeros(c.W * c.H, np.float32), np.zeros(c.W * c.H, np.float32)) for c, L in
+                zip(cams, lights)]
+
+    def soft_shadows(self, cam, L, exact=True):
+        return self.batch_soft([cam], [L], exact)[0]
+
+    def primary(self, cam, tile=16):
+        self._note(("primary", cam.W))
+        return None
+
+    def point_shadows(self, cam, prim, light):
+        return None
+
+    def raster(self, cam, prim, sh):
+        return np.full(cam.W * cam.H, cam.W, np.int32), np.zeros(cam.W * cam.H, np.uint8)
+
+    def close(self):
+        pass
+
+
+def test_admission_and_batching(native_lib):
+    from beamtrace2007_b200.serving import Request, Server, request_bytes
+    s, ps = scene("room")
+    scenes = {"a": s, "b": s}
+    FakeEngine.log = []
+    # a budget that holds the resident part and about eight 128^2 soft requests
+    probe = Request("soft", "a", 128, 128)
+    with Server(scenes, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine) as srv:
+        srv.budget = srv.resident + 8 * request_bytes(probe)
+        peak = [0]
+        reqs = []
+        for i in range(24):
+            r = Request("soft" if i % 3 else "primary", "ab"[i % 2], 128, 128, light_scale=1.0 + i)
+            reqs.append(srv.submit(r))
+            peak[0] = max(peak[0], srv.in_use)
+        for r in reqs:
+            assert r.event.wait(30)
+        assert srv.in_use == 0
+    assert peak[0] <= 8 * request_bytes(probe)
+    assert all(r.error is None and r.done >= r.arrival for r in reqs)
+    # soft requests that waited together ran as one batch at least once
+    assert any(k == "batch" and n > 1 for k, n in FakeEngine.log)
+    for r in reqs:
+        if r.kind == "soft":
+            assert r.result.vis[0] == np.float32(r.result.vis[0])
+
+
+@pytest.mark.gpu
+def test_mixed_stream_same_as_alone(gpu):
+    from beamtrace2007_b200.serving import Server, poisson_stream
+    scenes = {"room": scene("room")[0], "plant": scene("plant")[0],
+              "building": scene("building", floors=1, furniture=2)[0]}
+    with Server(scenes, memory_budget_gb=8.0) as srv:
+        reqs, summary = poisson_stream(srv, rate=200.0, n=30, sizes=(64, 96, 128), seed=3)
+        assert summary["errors"] == 0, [r.error for r in reqs if r.error]
+        assert summary["p99_ms"] >= summary["p50_ms"] > 0
+        # each request again, alone, on the same resident scene
+        for r in reqs:
+            slot = srv.slots[r.scene]
+            cam = srv._camera(slot, r)
+            if r.kind == "soft":
+                alone = slot.engine.soft_shadows(cam, slot.data.light_array(r.light_scale), exact=r.exact)
+                for k in ("tri", "vis", "E", "Eu"):
+                    assert np.array_equal(getattr(r.result, k), getattr(alone, k)), (r.kind, k)
+            else:
+                prim = slot.engine.primary(cam, tile=16)
+                if r.kind == "primary":
+                    tri, _ = slot.engine.raster(cam, prim, None)
+                    assert np.array_equal(r.result, tri)
+                else:
+                    sh = slot.engine.point_shadows(cam, prim, np.asarray(slot.data.point_light, np.float32))
+                    _, flag = slot.engine.raster(cam, prim, sh)
+                    assert np.array_equal(r.result, flag)
