@@ -138,6 +138,11 @@ SIGNATURES = {
                             C.POINTER(RunInfo)]),
     "bt_gpu_point": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, _P, C.POINTER(Polys), C.POINTER(_I64),
                           C.POINTER(RunInfo)]),
+    "bt_gpu_primary_ids": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, C.POINTER(RunInfo)]),
+    "bt_gpu_primary_ids_device": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, C.POINTER(RunInfo)]),
+    "bt_gpu_point_mask": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, _P, _P, C.POINTER(RunInfo)]),
+    "bt_gpu_point_mask_device": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, _P, _P,
+                                      C.POINTER(RunInfo)]),
     "bt_gpu_raster": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, C.POINTER(Polys), _I64, _P, _P]),
 }
 

@@ -833,6 +833,25 @@ __global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
   c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
 }
 
+// Hit polygons of the final attempts (tri >= 0), compacted as point-shadow
+// roots (any order: the outputs built from them do not depend on it).
+__global__ void compactHitsKernel(const float* ox, const float* oy, const int32_t* on, const int32_t* otri,
+                                  const int32_t* oroot, const int32_t* oatt, int64_t n, const int32_t* rootState,
+                                  const int32_t* rootAttempt, float* hx, float* hy, int32_t* hn, int32_t* htri,
+                                  int* count) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int r = oroot[i];
+  if (otri[i] < 0 || rootState[r] != kRootTraced || oatt[i] != rootAttempt[r]) return;
+  const int k = atomicAdd(count, 1);
+  for (int j = 0; j < 4; ++j) {
+    hx[4 * k + j] = ox[4 * i + j];
+    hy[4 * k + j] = oy[4 * i + j];
+  }
+  hn[k] = on[i];
+  htri[k] = otri[i];
+}
+
 // Roots abandoned in a pass, compacted for the retry pass.
 __global__ void collectKilledKernel(const int32_t* state, const int32_t* list, int n, int32_t* out, int* count) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -993,10 +1012,19 @@ __global__ void __launch_bounds__(128) primaryRaysKernel(SceneDev s, bt_camera c
 // src/render/render.cpp:49-95, one sample at the pixel centre): one thread
 // per polygon; among polygons covering a centre (shared edges) the higher
 // triangle id wins, so the result does not depend on polygon order.
+// With `proot`, polygons straight from the engine's output buffers: only
+// those of a root's final attempt count (the host-side filter of
+// downloadPolys, done here).
 __global__ void rasterKernel(bt_camera cam, const float* px_, const float* py_, const int32_t* pn, const int32_t* ptri,
-                             int64_t np, int shadow, int32_t* triBuf, uint8_t* flagBuf) {
+                             int64_t np, int shadow, int32_t* triBuf, uint8_t* flagBuf, const int32_t* proot = nullptr,
+                             const int32_t* patt = nullptr, const int32_t* rootState = nullptr,
+                             const int32_t* rootAttempt = nullptr) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= np) return;
+  if (proot) {
+    const int r = proot[i];
+    if (rootState[r] != kRootTraced || patt[i] != rootAttempt[r]) return;
+  }
   const int n = pn[i], tri = ptri[i];
   if (!shadow && tri < 0) return;
   if (n < 3 || n > 4) return;
@@ -1098,6 +1126,13 @@ struct bt_gpu_ctx {
   int32_t* dPixTri = nullptr;
   float *dPixX = nullptr, *dPixN = nullptr, *dVis = nullptr, *dE = nullptr, *dEu = nullptr;
   int blocksSoft = 0, blocksPrimary = 0, blocksPoint = 0;
+  // device-resident primary ids / point masks: compacted hit polygons
+  int64_t hitCap = 0;
+  float *dHx = nullptr, *dHy = nullptr;
+  int32_t *dHn = nullptr, *dHt = nullptr;
+  int* dHitCount = nullptr;
+  uint8_t* dFlag = nullptr;  // host-output variants: the mask in device memory
+  int64_t flagCap = 0;
   // batched soft shadows: per-job parameter table and root offsets
   AppParams* dJobs = nullptr;
   int32_t* dJobStart = nullptr;
@@ -1592,7 +1627,8 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
                   c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
-                  c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart};
+                  c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart, c->dHx, c->dHy, c->dHn,
+                  c->dHt, c->dHitCount, c->dFlag};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& ev : c->ev)
@@ -1892,6 +1928,92 @@ int downloadPolys(bt_gpu_ctx* c, int64_t produced, int R, bt_polys* out, int64_t
   return BT_OK;
 }
 
+int ensureHits(bt_gpu_ctx* c, int64_t n) {
+  if (!c->dHitCount) {
+    int e = devAlloc(&c->dHitCount, 1);
+    if (e) return e;
+  }
+  if (c->hitCap >= n) return BT_OK;
+  cudaFree(c->dHx);
+  cudaFree(c->dHy);
+  cudaFree(c->dHn);
+  cudaFree(c->dHt);
+  c->hitCap = 0;
+  int e;
+  if ((e = devAlloc(&c->dHx, size_t(4 * n))) || (e = devAlloc(&c->dHy, size_t(4 * n))) ||
+      (e = devAlloc(&c->dHn, size_t(n))) || (e = devAlloc(&c->dHt, size_t(n))))
+    return e;
+  c->hitCap = n;
+  return BT_OK;
+}
+
+int ensureFlag(bt_gpu_ctx* c, int64_t n) {
+  if (c->flagCap >= n) return BT_OK;
+  cudaFree(c->dFlag);
+  c->flagCap = 0;
+  int e = devAlloc(&c->dFlag, size_t(n));
+  if (e) return e;
+  c->flagCap = n;
+  return BT_OK;
+}
+
+void addInfo(bt_run_info* a, const bt_run_info& b) {
+  a->kd_steps += b.kd_steps;
+  a->leaf_visits += b.leaf_visits;
+  a->tri_tests += b.tri_tests;
+  a->hits += b.hits;
+  a->splits += b.splits;
+  a->beams += b.beams;
+  a->root_beams += b.root_beams;
+  a->presplit_beams += b.presplit_beams;
+  a->five_splits += b.five_splits;
+  a->climbs += b.climbs;
+  a->dropped_area += b.dropped_area;
+  a->ms_round += b.ms_round;
+  a->launches += b.launches;
+  a->round_launches += b.round_launches;
+  a->passes += b.passes;
+  a->retried_roots += b.retried_roots;
+  a->max_spill = std::max(a->max_spill, b.max_spill);
+  a->roots += b.roots;
+  a->rounds += b.rounds;
+  a->tail_rounds += b.tail_rounds;
+  a->ms_kernel_trace += b.ms_kernel_trace;
+}
+
+// Primary visibility roots (tile x tile pixels) through the engine; on
+// return the visible polygons are in the output buffers (*produced of them,
+// filtered by attempt tags) and the roots' state in dState/dAttempt.
+int runPrimary(bt_gpu_ctx* c, const bt_camera* cam, int cull, int tile, bt_run_info* info, int64_t* produced,
+               int* Rout) {
+  const int tilesW = (cam->W + tile - 1) / tile, tilesH = (cam->H + tile - 1) / tile;
+  const int R = tilesW * tilesH;
+  int64_t cap = std::max<int64_t>(int64_t(1) << 16, int64_t(cam->W) * cam->H * 2);
+  for (;;) {
+    int e = ensureOut(c, cap);
+    if (e) return e;
+    AppParams a = baseApp(c, cam);
+    a.tile = tile;
+    a.tilesW = tilesW;
+    a.cull = cull ? 1 : 0;
+    bt_run_info ri;
+    memset(&ri, 0, sizeof ri);
+    e = runRoots<kAppPrimary>(c, a, R, c->cfg.primary_budget, &ri);
+    if (e) return e;
+    Counters hc;
+    CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (hc.outCount > c->outCap) {
+      cap = int64_t(hc.outCount) + hc.outCount / 4;
+      continue;
+    }
+    if (info) addInfo(info, ri);
+    *produced = hc.outCount;
+    *Rout = R;
+    return BT_OK;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1950,22 +2072,14 @@ int bt_gpu_point(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* hits, int6
       setErr("bt_gpu_point: hit polygon %lld is invalid", (long long)i);
       return BT_ERR_INVALID;
     }
-  float *dhx, *dhy;
-  int32_t *dhn, *dht;
-  int e;
-  if ((e = devAlloc(&dhx, size_t(4 * nh))) || (e = devAlloc(&dhy, size_t(4 * nh))) ||
-      (e = devAlloc(&dhn, size_t(nh))) || (e = devAlloc(&dht, size_t(nh))))
-    return e;
-  struct Free {
-    void* p[4];
-    ~Free() {
-      for (void* q : p) cudaFree(q);
-    }
-  } guard{{dhx, dhy, dhn, dht}};
-  CK(cudaMemcpy(dhx, hits->x, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dhy, hits->y, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dhn, hits->n, sizeof(int32_t) * nh, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dht, hits->tri, sizeof(int32_t) * nh, cudaMemcpyHostToDevice));
+  int e = ensureHits(c, nh);
+  if (e) return e;
+  float *dhx = c->dHx, *dhy = c->dHy;
+  int32_t *dhn = c->dHn, *dht = c->dHt;
+  CK(cudaMemcpyAsync(dhx, hits->x, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dhy, hits->y, sizeof(float) * 4 * nh, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dhn, hits->n, sizeof(int32_t) * nh, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(dht, hits->tri, sizeof(int32_t) * nh, cudaMemcpyHostToDevice, c->stream));
   int64_t cap = std::max<int64_t>(int64_t(1) << 16, nh * 4);
   for (;;) {
     if ((e = ensureOut(c, cap))) return e;
@@ -2005,20 +2119,11 @@ int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int
   CK(cudaSetDevice(c->device));
   const int64_t npix = int64_t(cam->W) * cam->H;
   const int64_t m = std::max(np, ns);
-  float *dx, *dy;
-  int32_t *dn, *dt, *dtri;
-  uint8_t* dflag;
   int e;
-  if ((e = devAlloc(&dx, size_t(4 * std::max<int64_t>(m, 1)))) || (e = devAlloc(&dy, size_t(4 * std::max<int64_t>(m, 1)))) ||
-      (e = devAlloc(&dn, size_t(std::max<int64_t>(m, 1)))) || (e = devAlloc(&dt, size_t(std::max<int64_t>(m, 1)))) ||
-      (e = devAlloc(&dtri, size_t(npix))) || (e = devAlloc(&dflag, size_t(npix))))
-    return e;
-  struct Free {
-    void* p[6];
-    ~Free() {
-      for (void* q : p) cudaFree(q);
-    }
-  } guard{{dx, dy, dn, dt, dtri, dflag}};
+  if ((e = ensureHits(c, std::max<int64_t>(m, 1))) || (e = ensurePix(c, npix)) || (e = ensureFlag(c, npix))) return e;
+  float *dx = c->dHx, *dy = c->dHy;
+  int32_t *dn = c->dHn, *dt = c->dHt, *dtri = c->dPixTri;
+  uint8_t* dflag = c->dFlag;
   fillKernel<<<(npix + 255) / 256, 256, 0, c->stream>>>(dtri, npix, -1);
   CK(cudaMemsetAsync(dflag, 0, size_t(npix), c->stream));
   for (int pass = 0; pass < 2; ++pass) {
@@ -2034,6 +2139,143 @@ int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int
   }
   if (tri) CK(cudaMemcpyAsync(tri, dtri, sizeof(int32_t) * npix, cudaMemcpyDeviceToHost, c->stream));
   if (flag) CK(cudaMemcpyAsync(flag, dflag, size_t(npix), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+int bt_gpu_primary_ids_device(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t tile, int32_t* d_tri,
+                              bt_run_info* info) {
+  if (!c || !camOk(cam) || tile <= 0 || !d_tri) {
+    setErr("bt_gpu_primary_ids_device: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  const int64_t npix = int64_t(cam->W) * cam->H;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  int64_t produced = 0;
+  int R = 0;
+  int e = runPrimary(c, cam, cull, tile, info, &produced, &R);
+  if (e) return e;
+  fillKernel<<<int((npix + 255) / 256), 256, 0, c->stream>>>(d_tri, npix, -1);
+  if (produced > 0)
+    rasterKernel<<<int((produced + 127) / 128), 128, 0, c->stream>>>(*cam, c->dOx, c->dOy, c->dOn, c->dOtri, produced,
+                                                                     0, d_tri, nullptr, c->dOroot, c->dOatt,
+                                                                     c->dState, c->dAttempt);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float t = 0;
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+    info->ms_trace = info->ms_total = t;
+    info->launches += 2;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_point_mask_device(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t tile, const float* light,
+                             int32_t* d_tri, uint8_t* d_mask, bt_run_info* info) {
+  if (!c || !camOk(cam) || tile <= 0 || !light || !d_mask) {
+    setErr("bt_gpu_point_mask_device: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  if (info) memset(info, 0, sizeof *info);
+  const int64_t npix = int64_t(cam->W) * cam->H;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  int64_t produced = 0;
+  int R = 0;
+  int e = runPrimary(c, cam, cull, tile, info, &produced, &R);
+  if (e) return e;
+  if (d_tri) {
+    fillKernel<<<int((npix + 255) / 256), 256, 0, c->stream>>>(d_tri, npix, -1);
+    if (produced > 0)
+      rasterKernel<<<int((produced + 127) / 128), 128, 0, c->stream>>>(*cam, c->dOx, c->dOy, c->dOn, c->dOtri,
+                                                                       produced, 0, d_tri, nullptr, c->dOroot,
+                                                                       c->dOatt, c->dState, c->dAttempt);
+  }
+  // the final hit polygons become the point-shadow roots
+  if ((e = ensureHits(c, std::max<int64_t>(produced, 1)))) return e;
+  CK(cudaMemsetAsync(c->dHitCount, 0, sizeof(int), c->stream));
+  if (produced > 0)
+    compactHitsKernel<<<int((produced + 255) / 256), 256, 0, c->stream>>>(
+        c->dOx, c->dOy, c->dOn, c->dOtri, c->dOroot, c->dOatt, produced, c->dState, c->dAttempt, c->dHx, c->dHy,
+        c->dHn, c->dHt, c->dHitCount);
+  CK(cudaMemsetAsync(d_mask, 0, size_t(npix), c->stream));
+  int nh = 0;
+  CK(cudaMemcpyAsync(&nh, c->dHitCount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (nh > 0) {
+    int64_t cap = std::max<int64_t>(int64_t(1) << 16, int64_t(nh) * 4);
+    Counters hc;
+    for (;;) {
+      if ((e = ensureOut(c, cap))) return e;
+      AppParams a = baseApp(c, cam);
+      a.pointLight = mk(light[0], light[1], light[2]);
+      a.hx = c->dHx;
+      a.hy = c->dHy;
+      a.hn = c->dHn;
+      a.htri = c->dHt;
+      bt_run_info ri;
+      memset(&ri, 0, sizeof ri);
+      e = runRoots<kAppPoint>(c, a, nh, c->cfg.budget, &ri);
+      if (e) return e;
+      CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (hc.outCount > c->outCap) {
+        cap = int64_t(hc.outCount) + hc.outCount / 4;
+        continue;
+      }
+      if (info) addInfo(info, ri);
+      break;
+    }
+    if (hc.outCount > 0)
+      rasterKernel<<<int((hc.outCount + 127) / 128), 128, 0, c->stream>>>(
+          *cam, c->dOx, c->dOy, c->dOn, c->dOtri, hc.outCount, 1, nullptr, d_mask, c->dOroot, c->dOatt, c->dState,
+          c->dAttempt);
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info) {
+    float t = 0;
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+    info->ms_trace = info->ms_total = t;
+    info->launches += 4;
+  }
+  return BT_OK;
+}
+
+int bt_gpu_primary_ids(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t tile, int32_t* tri,
+                       bt_run_info* info) {
+  if (!c || !camOk(cam) || !tri) {
+    setErr("bt_gpu_primary_ids: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t npix = int64_t(cam->W) * cam->H;
+  int e = ensurePix(c, npix);
+  if (e) return e;
+  if ((e = bt_gpu_primary_ids_device(c, cam, cull, tile, c->dPixTri, info))) return e;
+  CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * npix, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BT_OK;
+}
+
+int bt_gpu_point_mask(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t tile, const float* light, int32_t* tri,
+                      uint8_t* mask, bt_run_info* info) {
+  if (!c || !camOk(cam) || !light || !mask) {
+    setErr("bt_gpu_point_mask: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  const int64_t npix = int64_t(cam->W) * cam->H;
+  int e;
+  if ((e = ensurePix(c, npix)) || (e = ensureFlag(c, npix))) return e;
+  if ((e = bt_gpu_point_mask_device(c, cam, cull, tile, light, tri ? c->dPixTri : nullptr, c->dFlag, info))) return e;
+  if (tri) CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * npix, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(mask, c->dFlag, size_t(npix), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return BT_OK;
 }

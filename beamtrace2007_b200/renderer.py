@@ -293,6 +293,25 @@ class GpuRenderer:
                 return out.head(cnt.value)
             cap = cnt.value
 
+    def primary_ids(self, cam: N.Camera, cull: bool = False, tile: int = 16) -> np.ndarray:
+        """Per-pixel hit-triangle ids, polygons kept on the GPU (bt_gpu_primary_ids)."""
+        tri = np.zeros(cam.W * cam.H, np.int32)
+        info = N.RunInfo()
+        check(N.lib().bt_gpu_primary_ids(self._h, C.byref(cam), int(cull), int(tile), ptr(tri), C.byref(info)))
+        self._record(info)
+        return tri
+
+    def point_mask(self, cam: N.Camera, light, cull: bool = False, tile: int = 16):
+        """(ids, shadow mask) of a point light, all on the GPU (bt_gpu_point_mask)."""
+        light = np.ascontiguousarray(light, np.float32)
+        tri = np.zeros(cam.W * cam.H, np.int32)
+        mask = np.zeros(cam.W * cam.H, np.uint8)
+        info = N.RunInfo()
+        check(N.lib().bt_gpu_point_mask(self._h, C.byref(cam), int(cull), int(tile), ptr(light), ptr(tri), ptr(mask),
+                                        C.byref(info)))
+        self._record(info)
+        return tri, mask
+
     def raster(self, cam: N.Camera, prim: PolyList, shadow: PolyList | None = None):
         tri = np.zeros(cam.W * cam.H, np.int32)
         flag = np.zeros(cam.W * cam.H, np.uint8)

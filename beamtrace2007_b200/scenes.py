@@ -312,6 +312,18 @@ def icosphere(subdiv: int, radius: float = 1.0, center=(0.0, 0.0, 0.0), displace
     return SceneData(f"icosphere{subdiv}", P.astype(np.float32), F.astype(np.uint32))
 
 
+def displaced_sphere(subdiv: int = 7, seed: int = 3) -> SceneData:
+    """The served sphere: icosahedron subdivided `subdiv` times (7: 327,680
+    triangles), radius 1, seeded fractal displacement of amplitude 0.1; the
+    relief shadows itself.  Camera at 3 m, lights above and to the side."""
+    s = icosphere(subdiv, 1.0, displace=0.1, seed=seed)
+    s.up = (0.0, 1.0, 0.0)
+    s.views = [View((1.8, 1.2, 2.2), (0.0, 0.0, 0.0), 45.0)]
+    s.point_light = (2.5, 3.0, 1.0)
+    s.area_light = ((2.0, 3.0, 1.5), (0.6, 0.0, 0.0), (0.0, 0.0, 0.6))
+    return s
+
+
 def torus(nu: int, nv: int, R: float = 1.0, r: float = 0.35, center=(0.0, 0.0, 0.0)) -> SceneData:
     """Torus around +y with nu x nv quads (2 * nu * nv triangles)."""
     u = 2 * np.pi * np.arange(nu) / nu
@@ -472,4 +484,5 @@ def meeting_room(seed: int = 5, tables: int = 12, chairs: int = 120) -> SceneDat
                      area_light=((10.0, 3.4, 7.0), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0)))
 
 
-SCENES = {"room": room, "plant": plant, "analytic": analytic, "building": building, "meeting": meeting_room}
+SCENES = {"room": room, "plant": plant, "analytic": analytic, "building": building, "meeting": meeting_room,
+          "sphere": displaced_sphere}

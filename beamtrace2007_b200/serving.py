@@ -184,14 +184,10 @@ class Server:
             if r.kind == "soft":
                 continue
             cam = self._camera(slot, r)
-            prim = slot.engine.primary(cam, tile=16)
             if r.kind == "primary":
-                tri, _ = slot.engine.raster(cam, prim, None)
-                r.result = tri
+                r.result = slot.engine.primary_ids(cam, tile=16)
             else:
-                sh = slot.engine.point_shadows(cam, prim, np.asarray(slot.data.point_light, np.float32))
-                _, flag = slot.engine.raster(cam, prim, sh)
-                r.result = flag
+                r.result = slot.engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=16)[1]
             r.done = time.perf_counter()
 
     def close(self):

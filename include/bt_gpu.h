@@ -282,6 +282,25 @@ BT_API int bt_gpu_primary(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, i
 BT_API int bt_gpu_point(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_polys* hits, int64_t num_hits,
                         const float* light, bt_polys* out, int64_t* count, bt_run_info* info);
 
+/* Primary visibility to per-pixel hit-triangle ids (-1 background) with the
+ * polygons kept in device memory: the engine's tile roots, then the pixel-
+ * centre raster of the final polygons on the GPU (rasterize,
+ * render.cpp:49-95, at aa = 1; a pixel centre on a shared edge takes the
+ * larger id).  Host output (W*H) / device output (_device). */
+BT_API int bt_gpu_primary_ids(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, int32_t tile, int32_t* tri,
+                              bt_run_info* info);
+BT_API int bt_gpu_primary_ids_device(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, int32_t tile,
+                                     int32_t* d_tri, bt_run_info* info);
+
+/* Point-light shadow mask (1 = in shadow) of the primary hits, all in device
+ * memory: primary roots, their final hit polygons as point-shadow roots,
+ * the shadowed polygons rasterised at pixel centres; optionally the ids
+ * too (tri / d_tri may be NULL).  Host outputs (W*H) / device (_device). */
+BT_API int bt_gpu_point_mask(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, int32_t tile, const float* light,
+                             int32_t* tri, uint8_t* mask, bt_run_info* info);
+BT_API int bt_gpu_point_mask_device(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, int32_t tile,
+                                    const float* light, int32_t* d_tri, uint8_t* d_mask, bt_run_info* info);
+
 /* Rasterises polygons at pixel centres (rasterize, render.cpp:49-95, aa = 1)
  * on the GPU: prim polygons write tri ids (-1 elsewhere), shadow polygons
  * set flag = 1.  tri and flag are host buffers of W*H. */

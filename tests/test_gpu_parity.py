@@ -204,3 +204,24 @@ def test_soft_points_vs_golden_and_restatement(gpu, k):
                          g["N"].astype(np.float64))
     assert np.abs(res.vis.astype(np.float64) - vr).max() <= VIS_TOL
     assert np.abs(res.E.astype(np.float64) - Er).max() <= E_REL * np.abs(Er).max()
+
+
+@pytest.mark.parametrize("name,kw", [("room", {}), ("plant", {}), ("building", dict(floors=1, furniture=3))])
+def test_device_ids_and_masks_equal_host_path(name, kw, gpu):
+    """bt_gpu_primary_ids / bt_gpu_point_mask (polygons never leave the GPU)
+    give bitwise the ids and masks of the host polygon path (bt_gpu_primary,
+    bt_gpu_point, bt_gpu_raster), which the tests above pin to the reference."""
+    from beamtrace2007_b200.renderer import make_camera
+    s, ps = scene(name, **kw)
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 200, 150)
+    light = np.array(s.point_light, np.float32)
+    with _renderer(ps) as g:
+        ids = g.primary_ids(cam)
+        ids2, mask = g.point_mask(cam, light)
+        prim = g.primary(cam, tile=16)
+        sh = g.point_shadows(cam, prim, light)
+        tri_h, flag_h = g.raster(cam, prim, sh)
+    assert np.array_equal(ids, tri_h)
+    assert np.array_equal(ids2, tri_h)
+    assert np.array_equal(mask, flag_h)

@@ -38,6 +38,14 @@ class FakeEngine:
         self._note(("primary", cam.W))
         return None
 
+    def primary_ids(self, cam, tile=16):
+        self._note(("primary", cam.W))
+        return np.full(cam.W * cam.H, cam.W, np.int32)
+
+    def point_mask(self, cam, light, tile=16):
+        self._note(("point", cam.W))
+        return np.full(cam.W * cam.H, cam.W, np.int32), np.zeros(cam.W * cam.H, np.uint8)
+
     def point_shadows(self, cam, prim, light):
         return None
 
@@ -93,6 +101,7 @@ def test_mixed_stream_same_as_alone(gpu):
                 for k in ("tri", "vis", "E", "Eu"):
                     assert np.array_equal(getattr(r.result, k), getattr(alone, k)), (r.kind, k)
             else:
+                # alone, and through the host polygon path
                 prim = slot.engine.primary(cam, tile=16)
                 if r.kind == "primary":
                     tri, _ = slot.engine.raster(cam, prim, None)
