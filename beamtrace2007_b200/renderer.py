@@ -299,7 +299,7 @@ class GpuRenderer:
         info = N.RunInfo()
         check(N.lib().bt_gpu_primary_ids(self._h, C.byref(cam), int(cull), int(tile), ptr(tri), C.byref(info)))
         self._record(info)
-        return tri
+        return tri.reshape(cam.H, cam.W)
 
     def point_mask(self, cam: N.Camera, light, cull: bool = False, tile: int = 16):
         """(ids, shadow mask) of a point light, all on the GPU (bt_gpu_point_mask)."""
@@ -310,7 +310,7 @@ class GpuRenderer:
         check(N.lib().bt_gpu_point_mask(self._h, C.byref(cam), int(cull), int(tile), ptr(light), ptr(tri), ptr(mask),
                                         C.byref(info)))
         self._record(info)
-        return tri, mask
+        return tri.reshape(cam.H, cam.W), mask.reshape(cam.H, cam.W)
 
     def raster(self, cam: N.Camera, prim: PolyList, shadow: PolyList | None = None):
         tri = np.zeros(cam.W * cam.H, np.int32)

@@ -40,11 +40,11 @@ class FakeEngine:
 
     def primary_ids(self, cam, tile=16):
         self._note(("primary", cam.W))
-        return np.full(cam.W * cam.H, cam.W, np.int32)
+        return np.full((cam.H, cam.W), cam.W, np.int32)
 
     def point_mask(self, cam, light, tile=16):
         self._note(("point", cam.W))
-        return np.full(cam.W * cam.H, cam.W, np.int32), np.zeros(cam.W * cam.H, np.uint8)
+        return np.full((cam.H, cam.W), cam.W, np.int32), np.zeros((cam.H, cam.W), np.uint8)
 
     def point_shadows(self, cam, prim, light):
         return None
