@@ -66,6 +66,13 @@ def request_bytes(r: Request) -> int:
     return px * (2 * 44 + 16) + (px // 256 + 1) * 164
 
 
+def primary_tile(r: Request) -> int:
+    """Pixels per side of a primary root: 16 (the reference's tile) from 512
+    pixels up; 8 below, where 16 leaves too few roots to fill the GPU
+    (measured on the served scenes: 69 vs 142 ms at 256^2)."""
+    return 16 if min(r.W, r.H) >= 512 else 8
+
+
 class _SceneSlot:
     def __init__(self, name, scene_data, engine):
         self.name = name
@@ -184,10 +191,11 @@ class Server:
             if r.kind == "soft":
                 continue
             cam = self._camera(slot, r)
+            tile = primary_tile(r)
             if r.kind == "primary":
-                r.result = slot.engine.primary_ids(cam, tile=16)
+                r.result = slot.engine.primary_ids(cam, tile=tile)
             else:
-                r.result = slot.engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=16)[1]
+                r.result = slot.engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=tile)[1]
             r.done = time.perf_counter()
 
     def close(self):

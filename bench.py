@@ -228,6 +228,63 @@ def run_reference_arm(args):
     return 0
 
 
+def batched_measure(g, s, N, lib, C, steps):
+    """A light-scale sweep of 8 frames (0.25-4x, the plant workload's sweep)
+    as one batch (bt_gpu_batch_soft) against the same frames one by one
+    (bt_gpu_soft_device); device time from the engine's CUDA events."""
+    import torch
+    from beamtrace2007_b200.renderer import make_camera
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, W, H)
+    scales = [float(x) for x in np.geomspace(0.25, 4.0, 8)]
+    lights = [s.light_array(k) for k in scales]
+    npx = W * H
+    outs = [(torch.empty(npx, dtype=torch.int32, device="cuda"),) +
+            tuple(torch.empty(npx, dtype=torch.float32, device="cuda") for _ in range(3)) for _ in scales]
+    info = N.RunInfo()
+    opts = N.SoftOpts(1, 0.0)
+    jobs = (N.SoftJob * len(scales))()
+    for j, L in enumerate(lights):
+        o = outs[j]
+        jobs[j] = N.SoftJob(cam, N.AreaLight.from_array(L), opts, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(),
+                            o[3].data_ptr())
+    plain, batch = [], []
+    for rep in range(steps + 1):
+        t = 0.0
+        for j, L in enumerate(lights):
+            o = outs[j]
+            N.check(lib.bt_gpu_soft_device(g._h, C.byref(cam), C.byref(N.AreaLight.from_array(L)), C.byref(opts),
+                                           o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(), o[3].data_ptr(),
+                                           C.byref(info)))
+            t += info.ms_total
+        N.check(lib.bt_gpu_batch_soft(g._h, len(scales), jobs, C.byref(info)))
+        if rep:  # the first pair warms up
+            plain.append(t)
+            batch.append(info.ms_total)
+    px = npx * len(scales)
+    pb, pp = float(np.median(batch)), float(np.median(plain))
+    return {"value": px / pb * 1e3, "unit": "px/s", "plain_value": px / pp * 1e3, "ratio_vs_plain": pp / pb,
+            "frames_per_batch": len(scales), "light_scales": [round(x, 3) for x in scales],
+            "ms_per_batch": pb, "ms_frames_one_by_one": pp, "steps": steps}
+
+
+def serving_measure():
+    """The served stream: three resident scenes (displaced sphere 327,680
+    triangles, meeting room 178,176, office building 2.1M), Poisson arrivals,
+    60% primary / 25% point / 15% soft, 256-1024 px square; p50/p99 latency
+    at a sustainable rate and px/s at saturation."""
+    from beamtrace2007_b200 import scenes
+    from beamtrace2007_b200.serving import Server, poisson_stream
+    sc = {"sphere": scenes.displaced_sphere(), "meeting": scenes.meeting_room(), "building": scenes.building()}
+    out = {"scenes": {k: int(len(v.tris)) for k, v in sc.items()}, "memory_budget_gb": 8.0}
+    with Server(sc, memory_budget_gb=8.0) as srv:
+        poisson_stream(srv, rate=50.0, n=6, sizes=(256,), seed=11)  # warm-up
+        for label, rate, n in (("steady", 10.0, 60), ("saturated", 200.0, 80)):
+            _, summ = poisson_stream(srv, rate=rate, n=n, sizes=(256, 512, 1024), seed=7)
+            out[label] = summ
+    return out
+
+
 def trace_traffic():
     """DRAM bytes per trace-kernel launch from the committed ncu capture."""
     tp = os.path.join(ROOT, "profiles", "trace_kernel_plant512_traffic.json")
@@ -244,6 +301,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--capacity", type=int, default=0,
                     help="sub-beam records per queue (0: the engine's default); small values for profiler captures")
     args = ap.parse_args()
@@ -349,6 +407,9 @@ def main():
                                                "rounds", "passes", "retried_roots", "max_spill")},
             "ms_primary": float(np.mean([d["ms_primary"] for d in infos])),
             "ms_trace": float(np.mean([d["ms_trace"] for d in infos]))}
+    if not args.no_extras:
+        line["batched"] = batched_measure(g, s, N, lib, C, steps=3)
+        line["serving"] = serving_measure()
     if not args.no_cpu_baseline and ws == 1:
         c = cpu_reference(s, 3, 1)
         if c:

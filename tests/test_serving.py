@@ -102,7 +102,8 @@ def test_mixed_stream_same_as_alone(gpu):
                     assert np.array_equal(getattr(r.result, k), getattr(alone, k)), (r.kind, k)
             else:
                 # alone, and through the host polygon path
-                prim = slot.engine.primary(cam, tile=16)
+                from beamtrace2007_b200.serving import primary_tile
+                prim = slot.engine.primary(cam, tile=primary_tile(r))
                 if r.kind == "primary":
                     tri, _ = slot.engine.raster(cam, prim, None)
                     assert np.array_equal(r.result, tri)
