@@ -30,6 +30,7 @@ max-over-ranks time (weak scaling).
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -295,6 +296,7 @@ def trace_traffic():
 
 
 def main():
+    faulthandler.enable()  # a fatal signal prints the Python stack
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

@@ -94,14 +94,16 @@ class RefTracer:
         self.lib = _lib(prec)
         pos = np.ascontiguousarray(pos, np.float32)
         tris = np.ascontiguousarray(tris, np.uint32)
-        self.h = self.lib.btr_create(_ptr(pos), len(pos), _ptr(tris), len(tris), float(cost_intersect),
-                                     int(single_leaf))
+        # a c_void_p, so that calls without declared argument types still pass
+        # the whole 64-bit pointer (a bare int would go as a 32-bit C int)
+        self.h = C.c_void_p(self.lib.btr_create(_ptr(pos), len(pos), _ptr(tris), len(tris), float(cost_intersect),
+                                                int(single_leaf)))
         self.num_tris = int(self.lib.btr_num_tris(self.h))
 
     def close(self):
-        if self.h:
+        if self.h is not None and self.h.value:
             self.lib.btr_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
