@@ -80,7 +80,7 @@ class SoftOpts(C.Structure):
 
 class SoftJob(C.Structure):
     _fields_ = [("cam", Camera), ("light", AreaLight), ("opts", SoftOpts), ("d_tri", C.c_void_p),
-                ("d_vis", C.c_void_p), ("d_E", C.c_void_p), ("d_Eu", C.c_void_p)]
+                ("d_vis", C.c_void_p), ("d_E", C.c_void_p), ("d_Eu", C.c_void_p), ("scene", C.c_int32)]
 
 
 class RunInfo(C.Structure):
@@ -121,6 +121,7 @@ SIGNATURES = {
     "bt_gpu_available": (_I, [C.POINTER(GpuInfo)]),
     "bt_gpu_create": (_I, [C.POINTER(SceneDesc), C.POINTER(KdDesc), C.POINTER(GpuConfig), C.POINTER(_P)]),
     "bt_gpu_destroy": (_I, [_P]),
+    "bt_gpu_add_scene": (_I, [_P, C.POINTER(SceneDesc), C.POINTER(KdDesc), C.POINTER(C.c_int32)]),
     "bt_gpu_soft": (_I, [_P, C.POINTER(Camera), C.POINTER(AreaLight), C.POINTER(SoftOpts), _P, _P, _P, _P,
                          C.POINTER(RunInfo)]),
     "bt_gpu_soft_points": (_I, [_P, C.POINTER(AreaLight), C.POINTER(SoftOpts), _I64, _P, _P, _P, _P, _P, _P,

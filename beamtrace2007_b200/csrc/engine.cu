@@ -129,6 +129,10 @@ struct AppParams {
   const AppParams* jobs;
   const int32_t* jobStart;
   int numJobs;
+  // a job's scene in the context's scene pool: kd root, its box, first triangle id
+  Box rootBox;
+  uint32_t rootNode;
+  int triBase;
   // point shadows
   V3 pointLight;
   const float* hx;
@@ -397,6 +401,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   Poly<8> poly;
   poly.clear();
   lightArea = 0;
+  SceneDev sj = p.s;  // the root's scene: the pool's first, or its job's
   if (App == kAppSoft) {
     p.app.missFx[k] = 0;
     p.app.gFx[k] = 0;
@@ -414,6 +419,8 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
       }
       ap = &p.app.jobs[lo];
       kl = k - p.app.jobStart[lo];
+      sj.bounds = ap->rootBox;
+      sj.rootNode = ap->rootNode;
     }
     const AppParams& a = *ap;
     int pix;
@@ -484,7 +491,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   storeRoot(&p.roots[k], q, lightArea, att);
   p.state[k] = kRootTraced;
   AdmitEnv<App> env{&p, &q, lightArea, k, &st, 0};
-  const bool ok = admitRoot(p.s, q, poly, k, env, st);
+  const bool ok = admitRoot(sj, q, poly, k, env, st);
   p.live[k] = env.queued;  // the pieces are traced by a later kernel
   if (!ok || env.queued > p.budget) killRoot(p, k);
   if (env.queued == 0) rootDone(p);
@@ -945,7 +952,7 @@ __global__ void __launch_bounds__(128) primaryRaysKernel(SceneDev s, bt_camera c
   };
   Entry stk[64];
   int sp = 0;
-  uint32_t node = 0;
+  uint32_t node = s.rootNode;
   float best = kInf;
   int bestTri = -1;
   const float tieEps = 4 * 1.1920928955078125e-07f;
@@ -1071,6 +1078,12 @@ __global__ void rasterKernel(bt_camera cam, const float* px_, const float* py_, 
   }
 }
 
+// Pool triangle ids to a scene's own (background -1 stays).
+__global__ void rebaseKernel(int32_t* p, int64_t n, int32_t base) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n && p[i] >= 0) p[i] -= base;
+}
+
 __global__ void fillKernel(int32_t* p, int64_t n, int32_t v) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -1092,6 +1105,15 @@ int devAlloc(T** p, size_t n) {
 
 // ------------------------------------------------------------------ context
 
+// One scene of a context's pool.
+struct PoolScene {
+  uint32_t rootNode;
+  int triBase;
+  int64_t numTris;
+  Box box;
+  float offset;
+};
+
 struct bt_gpu_ctx {
   int device = 0;
   int sms = 1;
@@ -1103,9 +1125,10 @@ struct bt_gpu_ctx {
   uint32_t* dParent = nullptr;
   float4* dRef = nullptr;
   float4* dTriNV = nullptr;
-  SceneDev s;
-  float offset = 0;  // |scene diagonal| * kEpsRel
-  int64_t numTris = 0;
+  SceneDev s;        // the whole scene pool; bounds and rootNode are the first scene's
+  float offset = 0;  // |first scene's diagonal| * kEpsRel
+  int64_t numTris = 0, numRefs = 0;
+  std::vector<PoolScene> pool;
   // engine
   SubBeam* dQ[3] = {nullptr, nullptr, nullptr};  // trace queues 0, 1 and the clip queue
   int capacity = 0;
@@ -1417,30 +1440,66 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   return BT_OK;
 }
 
+// Grows a device array to n elements, keeping the first `keep` (the pool's
+// earlier scenes).
+template <class T>
+int growArray(T** p, size_t keep, size_t n) {
+  T* q = nullptr;
+  int e = devAlloc(&q, n);
+  if (e) return e;
+  if (keep && *p) {
+    cudaError_t ce = cudaMemcpy(q, *p, keep * sizeof(T), cudaMemcpyDeviceToDevice);
+    if (ce != cudaSuccess) {
+      cudaFree(q);
+      setErr("cudaMemcpy: %s", cudaGetErrorString(ce));
+      return BT_ERR_CUDA;
+    }
+  }
+  cudaFree(*p);
+  *p = q;
+  return BT_OK;
+}
+
+// Appends a scene and its kd-tree to the context's scene pool: nodes,
+// references and triangles go after the earlier scenes', with child, leaf,
+// parent and triangle indices offset to the pool's numbering, so that one
+// SceneDev serves every scene and a root only needs its scene's kd root.
 int uploadScene(bt_gpu_ctx* c, const bt_scene_desc* sc, const bt_kd_desc* kd) {
   const int64_t nn = kd->num_nodes, nr = kd->num_refs, nt = sc->num_tris;
+  const uint32_t nodeBase = c->s.numNodes, triBase = uint32_t(c->numTris);
+  const int64_t refBase = c->numRefs;
+  if (int64_t(nodeBase) + nn >= (int64_t(1) << 30) || int64_t(triBase) + nt >= (int64_t(1) << 31) ||
+      refBase + nr >= (int64_t(1) << 32)) {
+    setErr("the scene pool would exceed 2^30 kd nodes, 2^31 triangles or 2^32 references");
+    return BT_ERR_TOO_LARGE;
+  }
   std::vector<uint2> node(static_cast<size_t>(nn));
   std::vector<float4> box(static_cast<size_t>(2 * nn));
+  std::vector<uint32_t> parent(static_cast<size_t>(nn));
   for (int64_t i = 0; i < nn; ++i) {
     const uint32_t d = kd->data[i];
-    uint32_t x;
+    uint32_t x, dd = d;
     if ((d & 3u) == 3u) {
       x = kd->offset[i];
       if (int64_t(x) + int64_t(d >> 2) > nr) {
         setErr("kd leaf %lld points past the reference list", (long long)i);
         return BT_ERR_INVALID;
       }
+      x += uint32_t(refBase);
     } else {
       memcpy(&x, &kd->split[i], 4);
       if (int64_t(d >> 2) >= nn) {
         setErr("kd node %lld has an invalid child", (long long)i);
         return BT_ERR_INVALID;
       }
+      dd = (((d >> 2) + nodeBase) << 2) | (d & 3u);
     }
-    node[size_t(i)] = make_uint2(x, d);
+    node[size_t(i)] = make_uint2(x, dd);
     const float* b = kd->node_box + 6 * i;
     box[size_t(2 * i)] = make_float4(b[0], b[1], b[2], b[3]);
     box[size_t(2 * i + 1)] = make_float4(b[4], b[5], 0.f, 0.f);
+    const uint32_t par = kd->parent[i];
+    parent[size_t(i)] = par == ~0u ? ~0u : par + nodeBase;
   }
   std::vector<float4> ref(static_cast<size_t>(4 * nr));
   for (int64_t k = 0; k < nr; ++k) {
@@ -1455,7 +1514,7 @@ int uploadScene(bt_gpu_ctx* c, const bt_scene_desc* sc, const bt_kd_desc* kd) {
     const float* p2 = sc->pos + 3 * size_t(vi[2]);
     const float* n = sc->tri_normals + 3 * size_t(t);
     float w[4];
-    uint32_t u[4] = {vi[0], vi[1], vi[2], t};
+    uint32_t u[4] = {vi[0], vi[1], vi[2], t + triBase};
     memcpy(w, u, 16);
     ref[size_t(4 * k)] = make_float4(p0[0], p0[1], p0[2], p1[0]);
     ref[size_t(4 * k + 1)] = make_float4(p1[1], p1[2], p2[0], p2[1]);
@@ -1469,31 +1528,45 @@ int uploadScene(bt_gpu_ctx* c, const bt_scene_desc* sc, const bt_kd_desc* kd) {
     tnv[size_t(2 * t)] = make_float4(n[0], n[1], n[2], 0.f);
     tnv[size_t(2 * t + 1)] = make_float4(p0[0], p0[1], p0[2], 0.f);
   }
+  const size_t NN = size_t(nodeBase) + size_t(nn), NR = size_t(refBase) + size_t(nr),
+               NT = size_t(triBase) + size_t(nt);
   int e;
-  if ((e = devAlloc(&c->dNode, size_t(nn))) || (e = devAlloc(&c->dBox, size_t(2 * nn))) ||
-      (e = devAlloc(&c->dParent, size_t(nn))) || (e = devAlloc(&c->dRef, size_t(4 * nr))) ||
-      (e = devAlloc(&c->dTriNV, size_t(2 * nt))))
+  if ((e = growArray(&c->dNode, nodeBase, NN)) || (e = growArray(&c->dBox, 2 * size_t(nodeBase), 2 * NN)) ||
+      (e = growArray(&c->dParent, nodeBase, NN)) || (e = growArray(&c->dRef, 4 * size_t(refBase), 4 * NR + 4)) ||
+      (e = growArray(&c->dTriNV, 2 * size_t(triBase), 2 * NT)))
     return e;
-  CK(cudaMemcpy(c->dNode, node.data(), sizeof(uint2) * node.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->dBox, box.data(), sizeof(float4) * box.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->dParent, kd->parent, sizeof(uint32_t) * size_t(nn), cudaMemcpyHostToDevice));
-  if (nr) CK(cudaMemcpy(c->dRef, ref.data(), sizeof(float4) * ref.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->dTriNV, tnv.data(), sizeof(float4) * tnv.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dNode + nodeBase, node.data(), sizeof(uint2) * node.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dBox + 2 * size_t(nodeBase), box.data(), sizeof(float4) * box.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dParent + nodeBase, parent.data(), sizeof(uint32_t) * parent.size(), cudaMemcpyHostToDevice));
+  if (nr)
+    CK(cudaMemcpy(c->dRef + 4 * size_t(refBase), ref.data(), sizeof(float4) * ref.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->dTriNV + 2 * size_t(triBase), tnv.data(), sizeof(float4) * tnv.size(), cudaMemcpyHostToDevice));
   c->s.node = c->dNode;
   c->s.box = c->dBox;
   c->s.parent = c->dParent;
   c->s.ref = c->dRef;
   c->s.triNV = c->dTriNV;
+  PoolScene ps;
+  ps.rootNode = nodeBase;
+  ps.triBase = int(triBase);
+  ps.numTris = nt;
   for (int a = 0; a < 3; ++a) {
-    c->s.bounds.lo[a] = kd->bounds[a];
-    c->s.bounds.hi[a] = kd->bounds[3 + a];
+    ps.box.lo[a] = kd->bounds[a];
+    ps.box.hi[a] = kd->bounds[3 + a];
   }
-  c->s.numTris = int(nt);
-  c->s.numNodes = uint32_t(nn);
-  c->numTris = nt;
   // offset = length(scene.bounds.diag()) * kEpsRel (render.cpp:348)
   V3 dg = mk(sc->bounds[3] - sc->bounds[0], sc->bounds[4] - sc->bounds[1], sc->bounds[5] - sc->bounds[2]);
-  c->offset = length(dg) * kEpsRel;
+  ps.offset = length(dg) * kEpsRel;
+  if (c->pool.empty()) {  // the first scene: what the single-scene entry points trace
+    c->s.bounds = ps.box;
+    c->s.rootNode = 0;
+    c->offset = ps.offset;
+  }
+  c->pool.push_back(ps);
+  c->s.numTris = int(NT);
+  c->s.numNodes = uint32_t(NN);
+  c->numTris = int64_t(NT);
+  c->numRefs = int64_t(NR);
   return BT_OK;
 }
 
@@ -1642,6 +1715,19 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
   return BT_OK;
 }
 
+int bt_gpu_add_scene(bt_gpu_ctx* c, const bt_scene_desc* scene, const bt_kd_desc* kd, int32_t* scene_id) {
+  if (!c || !scene || !kd || scene->num_tris <= 0 || kd->num_nodes <= 0) {
+    setErr("bt_gpu_add_scene: empty scene or tree");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));  // nothing in flight reads the arrays being replaced
+  const int e = uploadScene(c, scene, kd);
+  if (e) return e;
+  if (scene_id) *scene_id = int32_t(c->pool.size() - 1);
+  return BT_OK;
+}
+
 int bt_gpu_primary_rays_device(bt_gpu_ctx* c, const bt_camera* cam, int32_t* dTri, float* dX, float* dN) {
   if (!c || !camOk(cam) || !dTri || !dX || !dN) return BT_ERR_INVALID;
   CK(cudaSetDevice(c->device));
@@ -1733,6 +1819,10 @@ int bt_gpu_batch_soft(bt_gpu_ctx* c, int32_t n, const bt_soft_job* jobs, bt_run_
       setErr("bt_gpu_batch_soft: job %d has a bad camera", j);
       return BT_ERR_INVALID;
     }
+    if (jobs[j].scene < 0 || size_t(jobs[j].scene) >= c->pool.size()) {
+      setErr("bt_gpu_batch_soft: job %d names scene %d of %zu", j, jobs[j].scene, c->pool.size());
+      return BT_ERR_INVALID;
+    }
     totPix += int64_t(jobs[j].cam.W) * jobs[j].cam.H;
   }
   CK(cudaSetDevice(c->device));
@@ -1755,14 +1845,21 @@ int bt_gpu_batch_soft(bt_gpu_ctx* c, int32_t n, const bt_soft_job* jobs, bt_run_
   for (int j = 0; j < n; ++j) {
     const bt_soft_job& J = jobs[j];
     const bt_camera& cam = J.cam;
+    const PoolScene& ps = c->pool[size_t(J.scene)];
     int32_t* tri = J.d_tri ? J.d_tri : c->dPixTri + off;
+    SceneDev sj = c->s;
+    sj.bounds = ps.box;
+    sj.rootNode = ps.rootNode;
     dim3 bs(16, 8), gs((cam.W + 15) / 16, (cam.H + 7) / 8);
-    primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, cam, tri, c->dPixX + 3 * off, c->dPixN + 3 * off);
+    primaryRaysKernel<<<gs, bs, 0, c->stream>>>(sj, cam, tri, c->dPixX + 3 * off, c->dPixN + 3 * off);
     AppParams a = baseApp(c, &cam);
+    a.rootBox = ps.box;
+    a.rootNode = ps.rootNode;
+    a.triBase = ps.triBase;
     a.Lc = mk(J.light.c[0], J.light.c[1], J.light.c[2]);
     a.LU = mk(J.light.U[0], J.light.U[1], J.light.U[2]);
     a.LV = mk(J.light.V[0], J.light.V[1], J.light.V[2]);
-    a.offset = J.opts.offset > 0 ? J.opts.offset : c->offset;
+    a.offset = J.opts.offset > 0 ? J.opts.offset : ps.offset;
     a.exact = J.opts.exact;
     anyExact |= J.opts.exact;
     a.pixTri = tri;
@@ -1803,6 +1900,10 @@ int bt_gpu_batch_soft(bt_gpu_ctx* c, int32_t n, const bt_soft_job* jobs, bt_run_
     a.gFx = c->dG + start[size_t(j)];
     const int Rj = start[size_t(j) + 1] - start[size_t(j)];
     softFinalizeKernel<<<(Rj + 255) / 256, 256, 0, c->stream>>>(a, c->dState + start[size_t(j)], Rj);
+    // triangle ids of the pool back to the job's scene
+    const int64_t np = int64_t(jobs[j].cam.W) * jobs[j].cam.H;
+    if (a.triBase != 0 && jobs[j].d_tri)
+      rebaseKernel<<<int((np + 255) / 256), 256, 0, c->stream>>>(jobs[j].d_tri, np, a.triBase);
   }
   CK(cudaGetLastError());
   if (info) info->launches += n;
@@ -2587,6 +2688,7 @@ int bt_gpu_soft_points_noalloc(const bt_scene_desc* sc, const bt_kd_desc* kd, co
   }
   c.s.numTris = int(sc->num_tris);
   c.s.numNodes = uint32_t(kd->num_nodes);
+  c.s.rootNode = 0;
   c.numTris = sc->num_tris;
   V3 dg = mk(sc->bounds[3] - sc->bounds[0], sc->bounds[4] - sc->bounds[1], sc->bounds[5] - sc->bounds[2]);
   c.offset = length(dg) * kEpsRel;

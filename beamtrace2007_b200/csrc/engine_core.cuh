@@ -36,9 +36,10 @@ struct SceneDev {
   const uint32_t* parent;
   const float4* ref;
   const float4* triNV;
-  Box bounds;
+  Box bounds;         // the kd root's box
   int numTris;
   uint32_t numNodes;
+  uint32_t rootNode;  // where traversal starts (scenes after the first of a pool start further on)
 };
 
 // A queued sub-beam: 64 bytes, self-contained (corners on the root's plane,
@@ -594,7 +595,7 @@ struct AdmitEmit {
     SubBeam r;
     storeGeom(b, r);
     r.trail = 0;
-    r.node = 0;
+    r.node = s->rootNode;
     r.root = root;
     r.hit = -1;
     r.cursor = -1;

@@ -223,11 +223,22 @@ class GpuRenderer:
                                   ptr(Eu), C.byref(info)))
         return SoftResult(tri, vis, E, Eu, self._record(info))
 
-    def batch_soft(self, cams, lights, exact: bool = True, offset: float = 0.0, device_outputs: bool = False):
-        """Soft shadows of several images of this scene in one engine run
-        (bt_gpu_batch_soft).  Returns one SoftResult per job (host arrays),
-        or, with device_outputs, (tri, vis, E, Eu) CUDA tensors per job and
-        the run info."""
+    def add_scene(self, scene: "PreparedScene") -> int:
+        """Adds a scene to this context's pool (bt_gpu_add_scene); returns its id."""
+        sd, kd = scene.descs()
+        sid = C.c_int32()
+        check(N.lib().bt_gpu_add_scene(self._h, C.byref(sd), C.byref(kd), C.byref(sid)))
+        self._pool = getattr(self, "_pool", [self.scene]) + [scene]
+        return sid.value
+
+    def batch_soft(self, cams, lights, exact: bool = True, offset: float = 0.0, device_outputs: bool = False,
+                   scenes=None):
+        """Soft shadows of several images in one engine run
+        (bt_gpu_batch_soft); `scenes` gives each job's scene id in this
+        context's pool (default: all the context's own scene, id 0).
+        Returns one SoftResult per job (host arrays), or, with
+        device_outputs, (tri, vis, E, Eu) CUDA tensors per job and the run
+        info."""
         import torch
         dev = torch.device("cuda", self.config.device)
         jobs = (N.SoftJob * max(len(cams), 1))()
@@ -239,7 +250,7 @@ class GpuRenderer:
             outs.append(t)
             L = light if isinstance(light, N.AreaLight) else N.AreaLight.from_array(light)
             jobs[j] = N.SoftJob(cam, L, N.SoftOpts(int(exact), float(offset)), t[0].data_ptr(), t[1].data_ptr(),
-                                t[2].data_ptr(), t[3].data_ptr())
+                                t[2].data_ptr(), t[3].data_ptr(), int(scenes[j]) if scenes is not None else 0)
         info = N.RunInfo()
         # (the engine runs on its own stream and returns when its outputs
         # are written; nothing of torch's writes to these buffers)

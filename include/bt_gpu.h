@@ -172,6 +172,12 @@ BT_API int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const
                          bt_gpu_ctx** out);
 BT_API int bt_gpu_destroy(bt_gpu_ctx* ctx);
 
+/* Adds another finalised scene and its kd-tree to the context's scene pool
+ * (no counterpart in the reference); *scene_id names it in batch jobs.  The
+ * scene of bt_gpu_create is id 0 and stays the one the single-image entry
+ * points render. */
+BT_API int bt_gpu_add_scene(bt_gpu_ctx* ctx, const bt_scene_desc* scene, const bt_kd_desc* kd, int32_t* scene_id);
+
 /* Exact soft shadows of a W x H image: GPU primary rays (tri, shading point,
  * normal per pixel centre), then one shadow-beam root per covered pixel.
  * Outputs (host, W*H each, any may be NULL): tri (-1 background), vis
@@ -245,8 +251,9 @@ BT_API int bt_gpu_soft_device(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_ar
                               const bt_soft_opts* opts, int32_t* d_tri, float* d_vis, float* d_E, float* d_Eu,
                               bt_run_info* info);
 
-/* One soft-shadow job of a batch: an image W x H from cam, its light and
- * options, and its outputs in device memory (W*H each; any may be NULL). */
+/* One soft-shadow job of a batch: an image W x H from cam of one scene of
+ * the context's pool, its light and options, and its outputs in device
+ * memory (W*H each; any may be NULL; tri ids are the scene's own). */
 typedef struct {
   bt_camera cam;
   bt_area_light light;
@@ -255,6 +262,7 @@ typedef struct {
   float* d_vis;
   float* d_E;
   float* d_Eu;
+  int32_t scene;            /* 0: the context's own scene; else an id from bt_gpu_add_scene */
 } bt_soft_job;
 
 /* bt_gpu_soft_device for num_jobs images of the context's scene in one

@@ -203,6 +203,7 @@ EMU_API void* emu_create(const bt_scene_desc* sc, const bt_kd_desc* kd) {
   }
   e->s.numTris = int(nt);
   e->s.numNodes = uint32_t(nn);
+  e->s.rootNode = 0;
   return e;
 }
 
