@@ -62,7 +62,10 @@ constexpr int kWarps = 4;
 constexpr int kThreads = 32 * kWarps;
 constexpr double kFixVis = 1099511627776.0;         // 2^40: visible fraction, fixed point
 constexpr double kFixG = 1152921504606846976.0;     // 2^60: Lambert integral, fixed point
-constexpr int kMaxLaunches = 20000;  // launches per call before BT_ERR_TIMEOUT
+// Launches per call before BT_ERR_TIMEOUT: a guard against a run that stops
+// making progress, far above what long batches need (a 64-job batch of
+// 100-200K-triangle scenes with large lights takes thousands of rounds).
+constexpr int kMaxLaunches = 1000000;
 
 enum App { kAppSoft = 0, kAppPrimary = 1, kAppPoint = 2 };
 enum RootState { kRootNone = 0, kRootTraced = 1, kRootKilled = 2 };

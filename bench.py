@@ -269,6 +269,51 @@ def batched_measure(g, s, N, lib, C, steps):
             "ms_per_batch": pb, "ms_frames_one_by_one": pp, "steps": steps}
 
 
+def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: int = 200_000, reps: int = 1,
+                         seed: int = 2024):
+    """The batched-jobs workload: receiver/occluder pairs (icosphere or
+    torus, meshes log-uniform between 100 and `max_tris` triangles, plus a
+    ground quad), square resolutions from `sizes`, light scale U[0.25, 4],
+    exact; all jobs in one engine run (scene pool, bt_gpu_batch_soft)
+    against the same jobs one by one; device time from the engine's CUDA
+    events."""
+    from beamtrace2007_b200 import scenes
+    from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
+    rng = np.random.default_rng(seed)
+    specs = [(int(np.exp(rng.uniform(np.log(100), np.log(max_tris)))), int(rng.choice(list(sizes))),
+              float(rng.uniform(0.25, 4.0))) for _ in range(n_jobs)]
+    t0 = time.perf_counter()
+    jobs = []
+    for i, (tris, res, scale) in enumerate(specs):
+        sd = scenes.shadow_job(100 + i, tris)
+        jobs.append((sd, PreparedScene(sd.pos, sd.tris), res, scale))
+    prep_s = time.perf_counter() - t0
+    g = GpuRenderer(jobs[0][1])
+    ids = [0] + [g.add_scene(ps) for _, ps, _, _ in jobs[1:]]
+    cams, lights = [], []
+    for sd, ps, res, scale in jobs:
+        v = sd.views[0]
+        cams.append(make_camera(v.eye, v.target, v.fov, sd.up, res, res))
+        lights.append(sd.light_array(scale))
+    px = sum(c.W * c.H for c in cams)
+    batch, plain = [], []
+    for rep in range(reps + 1):
+        _, info = g.batch_soft(cams, lights, exact=True, scenes=ids, device_outputs=True)
+        t = 0.0
+        for k in range(len(cams)):
+            _, i1 = g.batch_soft([cams[k]], [lights[k]], exact=True, scenes=[ids[k]], device_outputs=True)
+            t += i1["ms_total"]
+        if rep:  # the first pass warms up
+            batch.append(info["ms_total"])
+            plain.append(t)
+    g.close()
+    pb, pp = float(np.median(batch)), float(np.median(plain))
+    return {"jobs": len(jobs), "triangles": int(sum(ps.num_tris for _, ps, _, _ in jobs)), "pixels": int(px),
+            "sizes": list(sizes), "max_tris": max_tris,
+            "value": px / pb * 1e3, "unit": "px/s", "one_by_one_value": px / pp * 1e3, "ratio_vs_one_by_one": pp / pb,
+            "ms_batch": pb, "ms_one_by_one": pp, "host_prep_s": prep_s}
+
+
 def serving_measure():
     """The served stream: three resident scenes (displaced sphere 327,680
     triangles, meeting room 178,176, office building 2.1M), Poisson arrivals,
@@ -411,6 +456,9 @@ def main():
             "ms_trace": float(np.mean([d["ms_trace"] for d in infos]))}
     if not args.no_extras:
         line["batched"] = batched_measure(g, s, N, lib, C, steps=3)
+        # the batched-jobs workload at bounded size (the full 64 jobs of up to
+        # 200K triangles at up to 512^2 take minutes per batch)
+        line["batched_jobs"] = batched_jobs_measure(n_jobs=32, max_tris=20_000, sizes=(64, 128))
         line["serving"] = serving_measure()
     if not args.no_cpu_baseline and ws == 1:
         c = cpu_reference(s, 3, 1)
