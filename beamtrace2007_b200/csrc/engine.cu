@@ -512,6 +512,8 @@ __device__ __forceinline__ void addStats(Stats& a, const Stats& b) {
   a.presplitBeams += b.presplitBeams;
   a.fiveSplits += b.fiveSplits;
   a.climbs += b.climbs;
+  a.epsBand += b.epsBand;
+  a.epsFlip += b.epsFlip;
   a.dropped += b.dropped;
 }
 
@@ -526,6 +528,17 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
   double d = st.dropped;
   for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(kFull, d, o);
   if (laneId() == 0 && d != 0) atomicAdd(reinterpret_cast<double*>(&p.stats[kStDropped]), d);
+  if (__any_sync(kFull, st.epsBand != 0)) {  // logging kernels only
+    unsigned long long b = st.epsBand, f = st.epsFlip;
+    for (int o = 16; o > 0; o >>= 1) {
+      b += __shfl_down_sync(kFull, b, o);
+      f += __shfl_down_sync(kFull, f, o);
+    }
+    if (laneId() == 0) {
+      atomicAdd(&p.stats[kStEpsBand], b);
+      if (f) atomicAdd(&p.stats[kStEpsFlip], f);
+    }
+  }
 }
 
 // Clips one buffered record (a triangle at its cursor needs it): the pieces
@@ -638,7 +651,7 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // Records needing a clip are compacted into the clip queue.
 // (At least 3 CTAs per SM: lets the compiler keep the lane's state in up to
 // 170 registers; at 4 CTAs it spills, which costs more than the warps gain.)
-template <int App, bool Fused>
+template <int App, bool Fused, bool EpsLog = false>
 __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
@@ -696,7 +709,7 @@ __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant
       int occ = -1;
       if (res == kStepContinue) {
         for (;;) {
-          res = testOne(p.s, q, r, b, st, occ);
+          res = testOne<EpsLog>(p.s, q, r, b, st, occ);
           if (res != kStepContinue || !moreInLeaf(p.s, q, r)) break;
         }
       }
@@ -1181,6 +1194,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->kernel_timing = 0;
   c->max_retries = 4;
   c->tail_records = 0;
+  c->eps_stats = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1328,8 +1342,12 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   p.ctr = c->dCtr;
   p.stats = c->dStats;
   p.app = app;
-  const int gA = gridFor(c, admitKernel<App>), gT = gridFor(c, traceKernel<App, false>),
-            gC = gridFor(c, clipKernel<App>), gF = gridFor(c, traceKernel<App, true>);
+  // eps_stats: the trace kernels that also log the fuzzy-band votes
+  const bool epsLog = c->cfg.eps_stats != 0;
+  const int gA = gridFor(c, admitKernel<App>),
+            gT = epsLog ? gridFor(c, traceKernel<App, false, true>) : gridFor(c, traceKernel<App, false>),
+            gC = gridFor(c, clipKernel<App>),
+            gF = epsLog ? gridFor(c, traceKernel<App, true, true>) : gridFor(c, traceKernel<App, true>);
   // tail rounds: every root admitted and fewer queued records than this
   const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads;
   static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
@@ -1368,14 +1386,20 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
         p.cur = round & 1;
         if (tail) {
           if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
-          traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
+          if (epsLog)
+            traceKernel<App, true, true><<<gF, kThreads, 0, c->stream>>>(p);
+          else
+            traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
           if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
           launches += 2;
           tailRounds++;
         } else {
           admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
           if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
-          traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
+          if (epsLog)
+            traceKernel<App, false, true><<<gT, kThreads, 0, c->stream>>>(p);
+          else
+            traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
           if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
           clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
           launches += 4;

@@ -59,9 +59,11 @@ struct __align__(16) SubBeam {
 // Per-lane counters (TraceStats, src/util/stats.h:8-42).
 struct Stats {
   uint32_t kdSteps, leafVisits, triTests, hits, splits, beams, rootBeams, presplitBeams, fiveSplits, climbs;
+  uint32_t epsBand, epsFlip;  // edge votes in the fuzzy band; of those, outside it in FP64 (logging only)
   double dropped;
   BT_HD void clear() {
     kdSteps = leafVisits = triTests = hits = splits = beams = rootBeams = presplitBeams = fiveSplits = climbs = 0;
+    epsBand = epsFlip = 0;
     dropped = 0;
   }
 };
@@ -352,6 +354,47 @@ BT_HD V3 edgePlane(const V3* r, const uint32_t* T, int i, int j) {
   return T[i] < T[j] ? cross(r[i], r[j]) : neg(cross(r[j], r[i]));
 }
 
+// Disagreement logging for one edge vote: corners whose float distance to
+// the edge line falls inside the fuzzy band (+-eps, where the vote counts
+// neither side) and, of those, corners that the same line evaluated in
+// FP64 -- from the float vertices and apex, in the same canonical
+// orientation -- places outside the band.  Decisions stay the float ones;
+// the FP64 line is computed only when a corner is in the band.
+BT_HD void logBand(const Query& q, const Beam& B, const Line& L, const TriRec& t, int i, int j, float sg, Stats& st) {
+  int band = 0;
+  bool in[4];
+  for (int k = 0; k < 4; ++k) {
+    const float dv = B.qx[k] * L.a + B.qy[k] * L.b + L.c;
+    in[k] = k < B.n && !(dv > q.eps) && !(dv < -q.eps);
+    band += in[k];
+  }
+  if (!band) return;
+  st.epsBand += uint32_t(band);
+  const V3 vf[3] = {t.v0, t.v1, t.v2};
+  double ri[3], rj[3];
+  for (int a = 0; a < 3; ++a) {
+    ri[a] = double(comp(vf[i], a)) - double(comp(q.P.O, a));
+    rj[a] = double(comp(vf[j], a)) - double(comp(q.P.O, a));
+  }
+  const bool fwd = t.vi[i] < t.vi[j];
+  const double* p0 = fwd ? ri : rj;
+  const double* p1 = fwd ? rj : ri;
+  double m[3] = {p0[1] * p1[2] - p0[2] * p1[1], p0[2] * p1[0] - p0[0] * p1[2], p0[0] * p1[1] - p0[1] * p1[0]};
+  if (!fwd)
+    for (int a = 0; a < 3; ++a) m[a] = -m[a];
+  const double a = sg * (m[0] * q.P.u.x + m[1] * q.P.u.y + m[2] * q.P.u.z);
+  const double b = sg * (m[0] * q.P.v.x + m[1] * q.P.v.y + m[2] * q.P.v.z);
+  const double c = sg * (m[0] * q.P.d.x + m[1] * q.P.d.y + m[2] * q.P.d.z);
+  const double nrm = sqrt(a * a + b * b);
+  if (!(nrm > 0)) return;
+  for (int k = 0; k < 4; ++k) {
+    if (!in[k]) continue;
+    const double dv = (double(B.qx[k]) * a + double(B.qy[k]) * b + c) / nrm;
+    if (dv > double(q.eps) || dv < -double(q.eps)) st.epsFlip++;
+  }
+}
+
+template <bool EpsLog = false>
 BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats& st, int& occluder) {
   const uint2 leaf = s.node[r.node];
   const uint32_t i = uint32_t(r.cursor);
@@ -375,12 +418,15 @@ BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats&
   const float sg = D > 0 ? 1.f : -1.f;
   bool allIn = true;
   ti.edge[0] = makeLine(sg * dot(m0, q.P.u), sg * dot(m0, q.P.v), sg * dot(m0, q.P.d), q.ext);
+  if (EpsLog) logBand(q, B, ti.edge[0], t, 0, 1, sg, st);
   if (!voteLine(q, B, ti.edge[0], allIn)) return kStepContinue;
   const V3 m1 = edgePlane(ti.r, t.vi, 1, 2);
   ti.edge[1] = makeLine(sg * dot(m1, q.P.u), sg * dot(m1, q.P.v), sg * dot(m1, q.P.d), q.ext);
+  if (EpsLog) logBand(q, B, ti.edge[1], t, 1, 2, sg, st);
   if (!voteLine(q, B, ti.edge[1], allIn)) return kStepContinue;
   const V3 m2 = edgePlane(ti.r, t.vi, 2, 0);
   ti.edge[2] = makeLine(sg * dot(m2, q.P.u), sg * dot(m2, q.P.v), sg * dot(m2, q.P.d), q.ext);
+  if (EpsLog) logBand(q, B, ti.edge[2], t, 2, 0, sg, st);
   if (!voteLine(q, B, ti.edge[2], allIn)) return kStepContinue;
   ti.n = t.n;
   ti.A[0] = dot(t.n, q.P.u);

@@ -163,7 +163,7 @@ class GpuRenderer:
 
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
                  capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
-                 tail_records: int = 0):
+                 tail_records: int = 0, eps_stats: bool = False):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -174,6 +174,7 @@ class GpuRenderer:
         cfg.blocks_per_sm = blocks_per_sm
         cfg.kernel_timing = int(kernel_timing)
         cfg.tail_records = int(tail_records)
+        cfg.eps_stats = int(eps_stats)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()

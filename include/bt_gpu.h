@@ -111,6 +111,9 @@ typedef struct {
   int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
   int64_t tail_records;     /* tail rounds (one fused trace-and-clip kernel) below this many queued
                                records once every root is admitted; 0 = the trace grid's lanes, < 0 = never */
+  int32_t eps_stats;        /* nonzero: trace kernels that also count the edge votes in the fuzzy band
+                               and their FP64 re-evaluation (eps_band_corners, eps_fp64_flips); results
+                               are the same, the kernels are slower */
 } bt_gpu_config;
 
 typedef struct {
@@ -122,8 +125,8 @@ typedef struct {
 typedef struct {
   uint64_t kd_steps, leaf_visits, tri_tests, hits, splits, beams, root_beams, presplit_beams, five_splits, climbs;
   double dropped_area;
-  uint64_t eps_band_corners;  /* corner votes that fell inside the fuzzy band */
-  uint64_t eps_fp64_flips;    /* of those, votes whose FP64 re-evaluation lies outside the band */
+  uint64_t eps_band_corners;  /* eps_stats: edge-vote corners inside the fuzzy band (traced records) */
+  uint64_t eps_fp64_flips;    /* of those, corners whose FP64 re-evaluation lies outside the band */
   double ms_primary, ms_trace, ms_total;
   double ms_round;            /* summed device time of the persistent round kernels */
   int32_t launches;           /* kernels launched by the call */

@@ -225,3 +225,27 @@ def test_device_ids_and_masks_equal_host_path(name, kw, gpu):
     assert np.array_equal(ids, tri_h)
     assert np.array_equal(ids2, tri_h)
     assert np.array_equal(mask, flag_h)
+
+
+def test_eps_band_logging(gpu):
+    """eps_stats: the trace kernels that count the edge votes inside the
+    fuzzy band and how many of them an FP64 re-evaluation places outside it.
+    Decisions stay the float ones, so the results are bitwise those of the
+    plain kernels; the counts are per record, so they repeat exactly."""
+    from beamtrace2007_b200.renderer import make_camera
+    s, ps = scene("plant")
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 160, 120)
+    L = s.light_array(2.0)
+    with _renderer(ps) as g:
+        plain = g.soft_shadows(cam, L, exact=True)
+    with _renderer(ps, eps_stats=True) as g:
+        a = g.soft_shadows(cam, L, exact=True)
+        b = g.soft_shadows(cam, L, exact=True)
+    for f in ("tri", "vis", "E", "Eu"):
+        assert np.array_equal(getattr(a, f), getattr(plain, f))
+    assert plain.info["eps_band_corners"] == 0
+    band, flips = a.info["eps_band_corners"], a.info["eps_fp64_flips"]
+    assert (band, flips) == (b.info["eps_band_corners"], b.info["eps_fp64_flips"])
+    assert band > 0 and 0 <= flips <= band
+    assert a.info["tri_tests"] == plain.info["tri_tests"]
