@@ -29,7 +29,12 @@
 #define BT_COLD __attribute__((noinline))
 #endif
 
-constexpr int kPolyMax = 8;  // vertices of a clip polygon (kMaxPoly, beam_geom.h:12)
+// Vertices of a clip polygon.  The reference sizes its lists for 8
+// (kMaxPoly, beam_geom.h:12), but the clip only ever splits polygons of at
+// most 4 corners (beams, and pentagons are split into 4 + 3 before the next
+// line), so a piece has at most 5; 6 keeps the splitter's overflow check
+// unreachable and the clip's local arrays small.
+constexpr int kPolyMax = 6;
 
 namespace btg {
 
