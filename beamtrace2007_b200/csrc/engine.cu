@@ -541,8 +541,10 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
   }
 }
 
-// Clips one buffered record (a triangle at its cursor needs it): the pieces
-// go to the ring in consecutive positions.  Returns true if nothing
+// Clips one record of the clip queue (a triangle at its cursor needs it):
+// the pieces go to the next round's trace queue in consecutive slots (or,
+// in tail rounds, the first one back to the calling lane, `keep`).
+// Returns true if nothing
 // measurable changed and the record (updated in place) continues at the next
 // triangle.  Works on its own query and beam: the caller's stay in registers.
 template <int App>

@@ -195,8 +195,10 @@ BT_API int bt_gpu_soft_points(bt_gpu_ctx* ctx, const bt_area_light* light, const
                               const int32_t* tri, const float* X, const float* N, float* vis, float* E, float* Eu,
                               bt_run_info* info);
 
-/* The same on device-resident buffers (device pointers; the caller's
- * stream is the legacy default stream).  For benchmarks and batching. */
+/* The same on device-resident buffers (device pointers).  The work runs on
+ * the context's own stream, which does not wait for other streams: the
+ * inputs must be complete when the call is made (synchronise the stream
+ * that wrote them first); the call returns when the outputs are written. */
 BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light, const bt_soft_opts* opts, int64_t n,
                                      const int32_t* d_tri, const float* d_X, const float* d_N, float* d_vis,
                                      float* d_E, float* d_Eu, bt_run_info* info);
