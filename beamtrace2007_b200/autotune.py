@@ -1,0 +1,63 @@
+"""Autotuner (no counterpart in the reference): picks the engine's launch
+settings for a workload by timing a probe of it on the GPU.
+
+Two kinds of setting:
+
+* per context (`bt_gpu_config`): CTAs per SM of the persistent grids
+  (`blocks_per_sm`, i.e. warps per SM; 0 = as many as fit), the queue
+  length below which rounds become fused tail rounds (`tail_records`), and
+  the sub-beam queue capacity -- `tune_engine` builds a context for each
+  candidate and times soft-shadow frames;
+* per call: the primary-visibility tile (pixels per side of a root) --
+  `tune_tile` times `bt_gpu_primary_ids` per candidate on an existing
+  context.  Fewer, larger tiles mean less re-traversal and fewer splits at
+  tile borders; more, smaller tiles keep the GPU busy on small images.
+
+Results do not depend on the context settings (the engine is deterministic
+and exact for any of them); the tile changes which polygons are produced,
+so a caller that compares images must use the same tile (the reference's
+own is 16).
+"""
+from __future__ import annotations
+
+import itertools
+import time
+
+import numpy as np
+
+
+def _best(timings: dict):
+    return min(timings, key=timings.get)
+
+
+def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, -1),
+                capacities=(0,), reps: int = 2, device: int = 0):
+    """Times `reps` soft-shadow frames (after one warm-up) for every
+    combination of the candidate settings; returns (best settings as
+    GpuRenderer keyword arguments, {settings tuple: best ms})."""
+    from .renderer import GpuRenderer
+    timings = {}
+    for bps, tail, cap in itertools.product(blocks_per_sm, tail_records, capacities):
+        with GpuRenderer(scene, device=device, blocks_per_sm=bps, tail_records=tail, capacity=cap) as g:
+            g.soft_shadows(cam, light, exact=exact)
+            ms = []
+            for _ in range(reps):
+                ms.append(g.soft_shadows(cam, light, exact=exact).info["ms_total"])
+        timings[(bps, tail, cap)] = min(ms)
+    bps, tail, cap = _best(timings)
+    return {"blocks_per_sm": bps, "tail_records": tail, "capacity": cap}, timings
+
+
+def tune_tile(renderer, cam, tiles=(8, 16, 32), reps: int = 2):
+    """The primary tile that gives the fastest `primary_ids` for this
+    camera; returns (tile, {tile: best seconds})."""
+    timings = {}
+    for tile in tiles:
+        renderer.primary_ids(cam, tile=tile)
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            renderer.primary_ids(cam, tile=tile)
+            ts.append(time.perf_counter() - t)
+        timings[tile] = float(np.min(ts))
+    return _best(timings), timings

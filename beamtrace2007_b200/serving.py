@@ -41,6 +41,7 @@ class Request:
     view: int = 0
     light_scale: float = 1.0  # soft: area light scale
     exact: bool = True        # soft: Lambert integral over the visible light
+    tile: int = 0             # primary / point: the tile it ran with (set by the server)
     arrival: float = 0.0      # perf_counter seconds, set by submit
     done: float = 0.0
     result: object = None
@@ -106,6 +107,7 @@ class Server:
         if self.resident > self.budget:
             raise ValueError(f"resident scenes and queues need {self.resident / 2**30:.2f} GiB, "
                              f"over the {memory_budget_gb} GiB budget")
+        self.tiles: dict = {}   # (scene, W, H) -> primary tile chosen by `tune`
         self.in_use = 0
         self.lock = threading.Lock()
         self.waiting: collections.deque[Request] = collections.deque()
@@ -113,6 +115,20 @@ class Server:
         for slot in self.slots.values():
             slot.thread = threading.Thread(target=self._worker, args=(slot,), daemon=True)
             slot.thread.start()
+
+    def tune(self, sizes=(256, 512, 1024), tiles=(8, 16, 32)):
+        """Autotunes the primary tile of every resident scene at each square
+        size (autotune.tune_tile); call before the stream starts (it uses the
+        scenes' contexts).  Untuned sizes use `primary_tile`."""
+        from .autotune import tune_tile
+        out = {}
+        for name, slot in self.slots.items():
+            for W in sizes:
+                r = Request("primary", name, W, W)
+                best, t = tune_tile(slot.engine, self._camera(slot, r), tiles)
+                self.tiles[(name, W, W)] = best
+                out[f"{name}/{W}"] = {"tile": best, "ms": {k: round(v * 1e3, 2) for k, v in t.items()}}
+        return out
 
     # ---- admission ----
     def submit(self, r: Request) -> Request:
@@ -191,7 +207,7 @@ class Server:
             if r.kind == "soft":
                 continue
             cam = self._camera(slot, r)
-            tile = primary_tile(r)
+            tile = r.tile = self.tiles.get((r.scene, r.W, r.H)) or primary_tile(r)
             if r.kind == "primary":
                 r.result = slot.engine.primary_ids(cam, tile=tile)
             else:

@@ -324,6 +324,7 @@ def serving_measure():
     sc = {"sphere": scenes.displaced_sphere(), "meeting": scenes.meeting_room(), "building": scenes.building()}
     out = {"scenes": {k: int(len(v.tris)) for k, v in sc.items()}, "memory_budget_gb": 8.0}
     with Server(sc, memory_budget_gb=8.0) as srv:
+        out["tuned_tiles"] = srv.tune(sizes=(256, 512, 1024))  # the autotuner, before the stream
         poisson_stream(srv, rate=50.0, n=6, sizes=(256,), seed=11)  # warm-up
         for label, rate, n in (("steady", 10.0, 60), ("saturated", 200.0, 80)):
             _, summ = poisson_stream(srv, rate=rate, n=n, sizes=(256, 512, 1024), seed=7)

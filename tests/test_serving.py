@@ -89,6 +89,8 @@ def test_mixed_stream_same_as_alone(gpu):
     scenes = {"room": scene("room")[0], "plant": scene("plant")[0],
               "building": scene("building", floors=1, furniture=2)[0]}
     with Server(scenes, memory_budget_gb=8.0) as srv:
+        tuned = srv.tune(sizes=(64, 128), tiles=(8, 16))
+        assert set(tuned) == {f"{s}/{w}" for s in scenes for w in (64, 128)}
         reqs, summary = poisson_stream(srv, rate=200.0, n=30, sizes=(64, 96, 128), seed=3)
         assert summary["errors"] == 0, [r.error for r in reqs if r.error]
         assert summary["p99_ms"] >= summary["p50_ms"] > 0
@@ -102,8 +104,7 @@ def test_mixed_stream_same_as_alone(gpu):
                     assert np.array_equal(getattr(r.result, k), getattr(alone, k)), (r.kind, k)
             else:
                 # alone, and through the host polygon path
-                from beamtrace2007_b200.serving import primary_tile
-                prim = slot.engine.primary(cam, tile=primary_tile(r))
+                prim = slot.engine.primary(cam, tile=r.tile)
                 if r.kind == "primary":
                     tri, _ = slot.engine.raster(cam, prim, None)
                     assert np.array_equal(r.result, tri)
@@ -111,3 +112,21 @@ def test_mixed_stream_same_as_alone(gpu):
                     sh = slot.engine.point_shadows(cam, prim, np.asarray(slot.data.point_light, np.float32))
                     _, flag = slot.engine.raster(cam, prim, sh)
                     assert np.array_equal(r.result, flag)
+
+
+@pytest.mark.gpu
+def test_autotune_engine_settings(gpu):
+    """tune_engine times each candidate context and returns the fastest; the
+    frame it renders is the same for every candidate."""
+    from beamtrace2007_b200.autotune import tune_engine
+    from beamtrace2007_b200.renderer import GpuRenderer, make_camera
+    s, ps = scene("plant")
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 96, 96)
+    best, timings = tune_engine(ps, cam, s.light_array(), blocks_per_sm=(0, 1), tail_records=(0, -1), reps=1)
+    assert len(timings) == 4 and all(t > 0 for t in timings.values())
+    assert (best["blocks_per_sm"], best["tail_records"], best["capacity"]) == min(timings, key=timings.get)
+    with GpuRenderer(ps, **best) as g1, GpuRenderer(ps, blocks_per_sm=1, tail_records=-1) as g2:
+        a = g1.soft_shadows(cam, s.light_array(), exact=True)
+        b = g2.soft_shadows(cam, s.light_array(), exact=True)
+    assert np.array_equal(a.vis, b.vis) and np.array_equal(a.E, b.E)
