@@ -63,6 +63,14 @@ class KdParams(C.Structure):
                 ("clip_bounds", C.c_int32), ("single_leaf", C.c_int32)]
 
 
+class SceneFileInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 128), ("num_verts", C.c_int64), ("num_tris", C.c_int64),
+                ("num_materials", C.c_int64), ("num_views", C.c_int64), ("cull_backfaces", C.c_int32),
+                ("has_point_light", C.c_int32), ("has_area_light", C.c_int32), ("up", C.c_float * 3),
+                ("point_light", C.c_float * 3), ("light_c", C.c_float * 3), ("light_u", C.c_float * 3),
+                ("light_v", C.c_float * 3), ("light_intensity", C.c_float), ("background", C.c_float * 3)]
+
+
 class GpuInfo(C.Structure):
     _fields_ = [("name", C.c_char * 256), ("sm_count", C.c_int32), ("mem_gb", C.c_double), ("cc_major", C.c_int32),
                 ("cc_minor", C.c_int32)]
@@ -72,7 +80,7 @@ class GpuConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("budget", C.c_int32), ("primary_budget", C.c_int32),
                 ("capacity", C.c_int64), ("blocks_per_sm", C.c_int32), ("kernel_timing", C.c_int32),
                 ("max_retries", C.c_int32), ("tail_records", C.c_int64),
-                ("eps_stats", C.c_int32)]
+                ("eps_stats", C.c_int32), ("yield_pct", C.c_int32)]
 
 
 class SoftOpts(C.Structure):
@@ -93,7 +101,7 @@ class RunInfo(C.Structure):
                 ("ms_round", C.c_double), ("launches", C.c_int32), ("round_launches", C.c_int32),
                 ("passes", C.c_int32), ("retried_roots", C.c_int32), ("max_spill", C.c_int32),
                 ("roots", C.c_int64), ("rounds", C.c_int32), ("tail_rounds", C.c_int32), ("ms_kernel_admit", C.c_double),
-                ("ms_kernel_trace", C.c_double), ("ms_kernel_clip", C.c_double)]
+                ("ms_kernel_trace", C.c_double), ("ms_kernel_clip", C.c_double), ("yields", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -118,6 +126,11 @@ SIGNATURES = {
     "bt_kd_sizes": (None, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_kd_view": (None, [_P, C.POINTER(KdDesc)]),
     "bt_kd_free": (None, [_P]),
+    "bt_scene_load_config": (_I, [C.c_char_p, C.POINTER(_P)]),
+    "bt_scene_parse_config": (_I, [C.c_char_p, C.POINTER(_P)]),
+    "bt_scene_file_info_get": (None, [_P, C.POINTER(SceneFileInfo)]),
+    "bt_scene_file_arrays": (None, [_P, _P, _P, _P, _P, _P]),
+    "bt_scene_file_free": (None, [_P]),
     "bt_camera_make": (None, [_P, _P, C.c_float, _P, C.c_int32, C.c_int32, C.POINTER(Camera)]),
     "bt_gpu_available": (_I, [C.POINTER(GpuInfo)]),
     "bt_gpu_create": (_I, [C.POINTER(SceneDesc), C.POINTER(KdDesc), C.POINTER(GpuConfig), C.POINTER(_P)]),

@@ -5,9 +5,11 @@ Two kinds of setting:
 
 * per context (`bt_gpu_config`): CTAs per SM of the persistent grids
   (`blocks_per_sm`, i.e. warps per SM; 0 = as many as fit), the queue
-  length below which rounds become fused tail rounds (`tail_records`), and
-  the sub-beam queue capacity -- `tune_engine` builds a context for each
-  candidate and times soft-shadow frames;
+  length below which rounds become fused tail rounds (`tail_records`), the
+  share of exited trace warps at which the records still in flight are
+  handed on to the next round (`yield_pct`), and the sub-beam queue
+  capacity -- `tune_engine` builds a context for each candidate and times
+  soft-shadow frames;
 * per call: the primary-visibility tile (pixels per side of a root) --
   `tune_tile` times `bt_gpu_primary_ids` per candidate on an existing
   context.  Fewer, larger tiles mean less re-traversal and fewer splits at
@@ -31,21 +33,22 @@ def _best(timings: dict):
 
 
 def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, -1),
-                capacities=(0,), reps: int = 2, device: int = 0):
+                capacities=(0,), yield_pcts=(0,), reps: int = 2, device: int = 0):
     """Times `reps` soft-shadow frames (after one warm-up) for every
     combination of the candidate settings; returns (best settings as
     GpuRenderer keyword arguments, {settings tuple: best ms})."""
     from .renderer import GpuRenderer
     timings = {}
-    for bps, tail, cap in itertools.product(blocks_per_sm, tail_records, capacities):
-        with GpuRenderer(scene, device=device, blocks_per_sm=bps, tail_records=tail, capacity=cap) as g:
+    for bps, tail, cap, yp in itertools.product(blocks_per_sm, tail_records, capacities, yield_pcts):
+        with GpuRenderer(scene, device=device, blocks_per_sm=bps, tail_records=tail, capacity=cap,
+                         yield_pct=yp) as g:
             g.soft_shadows(cam, light, exact=exact)
             ms = []
             for _ in range(reps):
                 ms.append(g.soft_shadows(cam, light, exact=exact).info["ms_total"])
-        timings[(bps, tail, cap)] = min(ms)
-    bps, tail, cap = _best(timings)
-    return {"blocks_per_sm": bps, "tail_records": tail, "capacity": cap}, timings
+        timings[(bps, tail, cap, yp)] = min(ms)
+    bps, tail, cap, yp = _best(timings)
+    return {"blocks_per_sm": bps, "tail_records": tail, "capacity": cap, "yield_pct": yp}, timings
 
 
 def tune_tile(renderer, cam, tiles=(8, 16, 32), reps: int = 2):

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -82,7 +83,9 @@ struct __align__(128) Counters {
   int maxQueue;                 // largest trace queue
   int done;                     // set by roundEnd: every root of the pass is done
   int rounds;
-  int pad0[6];
+  int warpsOut;                 // trace warps that have exited in this round
+  int yields;                   // records handed on unfinished (all rounds of the pass)
+  int pad0[4];
   int count[2];                 // records in trace queue 0 / 1
   int head;                     // fetch cursor of the trace queue being drained
   int pad1[13];
@@ -155,6 +158,7 @@ struct RoundParams {
   int reserve;  // queue slots reserved per root: max(budget, 32) (a root's pre-split pieces always fit)
   int numRoots;
   int rootCap;  // size of the per-root arrays
+  int yieldAt;  // exited trace warps at which the rest hand their records on (INT_MAX: never)
   const int32_t* rootList;
   RootRec* roots;  // per-root query records
   int32_t* live;
@@ -672,6 +676,33 @@ __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant
   Stats st;
   st.clear();
   for (;;) {
+    // Once the queue is drained and enough warps have exited, the records
+    // still in flight go to the next round's queue as they stand (at the top
+    // of this loop a lane's position -- node, trail, depth, cursor, hit -- is
+    // all in its record), so that the round does not wait on a few long
+    // walks with most of the GPU idle.  Tail rounds run to completion.
+    int warpsOut = 0;
+    if (!Fused && exhausted && lane == 0) warpsOut = *(volatile int*)&p.ctr->warpsOut;
+    if (!Fused && exhausted && __shfl_sync(kFull, warpsOut, 0) >= p.yieldAt) {
+      const unsigned y = __ballot_sync(kFull, phase == kTrace);
+      if (y) {
+        int base = 0;
+        if (lane == 0) {
+          base = atomicAdd(&p.ctr->count[p.cur ^ 1], __popc(y));
+          atomicAdd(&p.ctr->yields, __popc(y));
+        }
+        base = __shfl_sync(kFull, base, 0);
+        if (phase == kTrace) {
+          const int at = base + __popc(y & ltMask);
+          if (at < p.capacity)
+            p.tq[p.cur ^ 1][at] = r;
+          else
+            atomicExch(&p.ctr->error, 1);
+          phase = kIdle;
+        }
+      }
+      break;
+    }
     const unsigned idle = __ballot_sync(kFull, phase == kIdle);
     if (idle && !exhausted) {
       const int ni = __popc(idle);
@@ -784,6 +815,7 @@ __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant
       }
     }
   }
+  if (!Fused && lane == 0) atomicAdd(&p.ctr->warpsOut, 1);
   flushStats(p, st);
 }
 
@@ -854,6 +886,7 @@ __global__ void roundEndKernel(Counters* c, int cur, int numRoots) {
   c->clipCount = 0;
   c->clipHead = 0;
   c->outQ = 0;
+  c->warpsOut = 0;
   c->rounds++;
   c->done = (c->rootNext >= numRoots && c->inflight == 0 && c->count[nxt] == 0) ? 1 : 0;
 }
@@ -1183,6 +1216,10 @@ struct bt_gpu_ctx {
   cudaEvent_t kev[32] = {};  // kernel_timing: 2 per round of a batch, around the trace kernel
 };
 
+// For the host-side modules of the library (ingest.cpp): sets the message
+// bt_gpu_last_error returns on this thread.
+void btSetError(const char* msg) { setErr("%s", msg); }
+
 extern "C" {
 
 const char* bt_gpu_last_error(void) { return g_err; }
@@ -1197,6 +1234,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->max_retries = 4;
   c->tail_records = 0;
   c->eps_stats = 0;
+  c->yield_pct = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1352,11 +1390,14 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
             gF = epsLog ? gridFor(c, traceKernel<App, true, true>) : gridFor(c, traceKernel<App, true>);
   // tail rounds: every root admitted and fewer queued records than this
   const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads;
+  const int yieldPct = c->cfg.yield_pct == 0 ? 50 : std::min(c->cfg.yield_pct, 100);
+  const int yieldAt = yieldPct < 0 ? INT_MAX : std::max(1, int(int64_t(gT) * kWarps * yieldPct / 100));
   static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
   const bool ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
   // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
   FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
   int launches = 0, passes = 0, retried = 0, roundsRun = 0, tailRounds = 0;
+  int64_t yieldsRun = 0;
   const int32_t* list = nullptr;
   int n = R;
   Counters hc;
@@ -1370,6 +1411,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     }
     p.numRoots = n;
     p.rootList = list;
+    p.yieldAt = yieldAt;
     if (pass > 0) {
       // per-pass state; the output count carries over
       Counters z;
@@ -1425,8 +1467,8 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
           }
       }
       if (roundLog)
-        fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d ms %.3f\n", pass, hc.rounds,
-                hc.inflight, hc.rootNext, n, hc.count[round & 1], ms);
+        fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d yields %d ms %.3f\n", pass,
+                hc.rounds, hc.inflight, hc.rootNext, n, hc.count[round & 1], hc.yields, ms);
       if (hc.error) {
         setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam queue overflow (capacity %d)", c->capacity);
         return BT_ERR_CAPACITY;
@@ -1439,6 +1481,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     }
     if (info) info->max_spill = std::max(info->max_spill, hc.maxQueue);
     roundsRun += hc.rounds;
+    yieldsRun += hc.yields;
     if (hc.killed == 0) break;
     if (pass >= c->cfg.max_retries) {
       setErr("%d roots still over budget %d after %d retries", hc.killed, budget, pass);
@@ -1460,6 +1503,7 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
   if (info) {
     info->rounds += roundsRun;
     info->tail_rounds += tailRounds;
+    info->yields += yieldsRun;
     info->launches += launches;
     info->passes += passes;
     info->retried_roots += retried;

@@ -68,6 +68,14 @@ def make_camera(eye, target, fov: float, up, W: int, H: int) -> N.Camera:
     return cam
 
 
+def kd_params_default(cost_intersect: float = 0.4) -> dict:
+    """The kd-tree build parameters PreparedScene uses by default."""
+    kp = N.KdParams()
+    N.lib().bt_kd_params_default(C.byref(kp))
+    kp.cost_intersect = cost_intersect
+    return {k: getattr(kp, k) for k, _ in kp._fields_}
+
+
 class PreparedScene:
     """A finalised scene and its kd-tree, as host arrays."""
 
@@ -120,6 +128,33 @@ class PreparedScene:
         finally:
             L.bt_kd_free(h)
 
+    # the arrays that make up a prepared scene (saved and restored by the
+    # resident-scene cache, beamtrace2007_b200.ingest.SceneCache)
+    ARRAYS = ("pos", "tris", "tri_normals", "tri_area", "bounds", "kd_split", "kd_data", "kd_offset", "kd_parent",
+              "kd_box", "kd_tri_indices", "kd_bounds")
+
+    def to_arrays(self) -> dict:
+        d = {k: getattr(self, k) for k in self.ARRAYS}
+        d["kd_sizes"] = np.array([self.kd_leaves, self.kd_max_depth], np.int64)
+        return d
+
+    @classmethod
+    def from_arrays(cls, d) -> "PreparedScene":
+        """A scene prepared earlier (to_arrays), without finalising or
+        building again."""
+        ps = cls.__new__(cls)
+        dtypes = dict(pos=np.float32, tris=np.uint32, tri_normals=np.float32, tri_area=np.float32,
+                      bounds=np.float32, kd_split=np.float32, kd_data=np.uint32, kd_offset=np.uint32,
+                      kd_parent=np.uint32, kd_box=np.float32, kd_tri_indices=np.uint32, kd_bounds=np.float32)
+        for k in cls.ARRAYS:
+            setattr(ps, k, np.ascontiguousarray(d[k], dtypes[k]))
+        n = len(ps.kd_split)
+        if not (len(ps.kd_data) == len(ps.kd_offset) == len(ps.kd_parent) == len(ps.kd_box) == n
+                and ps.tris.ndim == 2 and len(ps.tri_normals) == len(ps.tris) == len(ps.tri_area)):
+            raise ValueError("inconsistent prepared-scene arrays")
+        ps.kd_leaves, ps.kd_max_depth = (int(x) for x in d["kd_sizes"])
+        return ps
+
     @property
     def num_tris(self) -> int:
         return len(self.tris)
@@ -163,7 +198,7 @@ class GpuRenderer:
 
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
                  capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
-                 tail_records: int = 0, eps_stats: bool = False):
+                 tail_records: int = 0, eps_stats: bool = False, yield_pct: int = 0):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -175,6 +210,7 @@ class GpuRenderer:
         cfg.kernel_timing = int(kernel_timing)
         cfg.tail_records = int(tail_records)
         cfg.eps_stats = int(eps_stats)
+        cfg.yield_pct = int(yield_pct)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()

@@ -18,6 +18,9 @@
  *   bt_scene_finalize       Scene::finalize         src/scene/scene.cpp:89-118
  *   bt_kd_build             KdTree::build           src/accel/kdtree.h:36
  *   bt_camera_make          Camera::make            src/render/render_types.h:24
+ * and scene ingest (configs, OBJ/PLY meshes, procedural scenes):
+ *   bt_scene_load_config    loadConfig + buildScene src/scene/scene.h:58-61
+ *   bt_scene_parse_config   parseConfig + buildScene src/scene/scene.h:60-61
  * Batching (no counterpart in the reference): bt_gpu_batch_soft.
  */
 #ifndef BT_GPU_H
@@ -114,6 +117,9 @@ typedef struct {
   int32_t eps_stats;        /* nonzero: trace kernels that also count the edge votes in the fuzzy band
                                and their FP64 re-evaluation (eps_band_corners, eps_fp64_flips); results
                                are the same, the kernels are slower */
+  int32_t yield_pct;        /* once a round's trace queue is drained and this percentage of the trace
+                               warps has exited, the records still in flight go on in the next round
+                               instead of holding the round (results are the same); 0 = 50, < 0 = never */
 } bt_gpu_config;
 
 typedef struct {
@@ -137,6 +143,7 @@ typedef struct {
   int32_t tail_rounds;        /* of those, tail rounds (fused trace and clip, bookkeeping) */
   /* summed device time of the trace launches (kernel_timing only, else 0); admit and clip reserved (0) */
   double ms_kernel_admit, ms_kernel_trace, ms_kernel_clip;
+  int64_t yields;             /* records handed on unfinished to the next round (yield_pct) */
 } bt_run_info;
 
 /* Beam cross-sections on a query plane (OutBeam, beam_types.h:68-73):
@@ -168,6 +175,37 @@ BT_API void bt_kd_view(const bt_kd_tree* t, bt_kd_desc* d);
 BT_API void bt_kd_free(bt_kd_tree* t);
 BT_API void bt_camera_make(const float* eye, const float* target, float fov_y, const float* up, int32_t W, int32_t H,
                            bt_camera* cam);
+
+/* ---- scene ingest (SceneConfig and Scene, src/scene/scene.h:13-61) ----
+ * A config is lines of `key values` (# comments): name, mesh (obj PATH |
+ * ply PATH | procedural NAME [key=value ...], with optional `scale s`,
+ * `translate x y z`, `color r g b`), cull_backfaces, up, view (eye target
+ * fov), orbit, walk, point_light, area_light (centre and full edge
+ * vectors), light_intensity, background.  Mesh paths are taken as written
+ * (relative ones from the working directory).  The scene is the one the
+ * reference builds from the same config, float for float, with its
+ * degenerate triangles removed (bt_scene_finalize's rule).  Errors:
+ * BT_ERR_INVALID with the reason in bt_gpu_last_error(). */
+typedef struct bt_scene_file bt_scene_file;
+typedef struct {
+  char name[128];
+  int64_t num_verts, num_tris, num_materials, num_views;
+  int32_t cull_backfaces, has_point_light, has_area_light;
+  float up[3];
+  float point_light[3];
+  float light_c[3], light_u[3], light_v[3];
+  float light_intensity;
+  float background[3];
+} bt_scene_file_info;
+BT_API int bt_scene_load_config(const char* path, bt_scene_file** out);
+BT_API int bt_scene_parse_config(const char* text, bt_scene_file** out);
+BT_API void bt_scene_file_info_get(const bt_scene_file* f, bt_scene_file_info* info);
+/* pos: 3 x num_verts; tris: 3 x num_tris; tri_mat: num_tris; mat_color:
+ * 3 x num_materials; views: 7 x num_views (eye, target, fov in degrees).
+ * Any pointer may be NULL. */
+BT_API void bt_scene_file_arrays(const bt_scene_file* f, float* pos, uint32_t* tris, uint16_t* tri_mat,
+                                 float* mat_color, float* views);
+BT_API void bt_scene_file_free(bt_scene_file* f);
 
 /* ---- device ---- */
 BT_API int bt_gpu_available(bt_gpu_info* info);

@@ -123,10 +123,12 @@ def test_autotune_engine_settings(gpu):
     s, ps = scene("plant")
     v = s.views[0]
     cam = make_camera(v.eye, v.target, v.fov, s.up, 96, 96)
-    best, timings = tune_engine(ps, cam, s.light_array(), blocks_per_sm=(0, 1), tail_records=(0, -1), reps=1)
-    assert len(timings) == 4 and all(t > 0 for t in timings.values())
-    assert (best["blocks_per_sm"], best["tail_records"], best["capacity"]) == min(timings, key=timings.get)
-    with GpuRenderer(ps, **best) as g1, GpuRenderer(ps, blocks_per_sm=1, tail_records=-1) as g2:
+    best, timings = tune_engine(ps, cam, s.light_array(), blocks_per_sm=(0, 1), tail_records=(0, -1),
+                                yield_pcts=(0, -1), reps=1)
+    assert len(timings) == 8 and all(t > 0 for t in timings.values())
+    assert (best["blocks_per_sm"], best["tail_records"], best["capacity"], best["yield_pct"]) == min(
+        timings, key=timings.get)
+    with GpuRenderer(ps, **best) as g1, GpuRenderer(ps, blocks_per_sm=1, tail_records=-1, yield_pct=-1) as g2:
         a = g1.soft_shadows(cam, s.light_array(), exact=True)
         b = g2.soft_shadows(cam, s.light_array(), exact=True)
     assert np.array_equal(a.vis, b.vis) and np.array_equal(a.E, b.E)
