@@ -19,6 +19,12 @@ released when it completes.
 
 Results do not depend on what else is in flight: the engine accumulates in
 fixed point and the batch path is bitwise the single-job path.
+
+Scenes are given as generated scenes, prepared scenes, or paths of the
+reference's scene configs; configs go through a SceneCache
+(beamtrace2007_b200.ingest), so a scene ingested and prepared once -- its
+kd-tree build is the host work that gates admission -- is admitted again
+from the cache directory.
 """
 from __future__ import annotations
 
@@ -89,8 +95,10 @@ class Server:
     builds a context (GpuRenderer by default; tests may pass a stand-in)."""
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 21,
-                 engine_factory=None):
+                 engine_factory=None, cache=None):
+        from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
+        self.cache = cache if cache is not None else SceneCache()
         self.budget = int(memory_budget_gb * (1 << 30))
         self.device = device
         if engine_factory is None:
@@ -99,7 +107,10 @@ class Server:
         self.slots: dict[str, _SceneSlot] = {}
         self.resident = 0
         for name, sd in scenes.items():
-            ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris)
+            if isinstance(sd, str):  # a scene config: ingested and prepared through the cache
+                sd, ps = self.cache.get(sd)
+            else:
+                ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris)
             self.resident += 44 * len(ps.kd_split) + 64 * len(ps.kd_tri_indices) + 32 * ps.num_tris
             self.resident += 3 * 64 * queue_records
             slot = _SceneSlot(name, sd, engine_factory(ps, queue_records))

@@ -300,3 +300,32 @@ class RefGpu:
         if self.h:
             self.lib.btrg_destroy(self.h)
             self.h = None
+
+
+def ref_config(text: str, prec: str = "f") -> dict:
+    """The reference's parseConfig + buildScene on config text: its scene
+    (pos, tris, tri_mat, mat_color), views (eye, target, fov per row) and
+    lights, as float64 copies of its Real values.  Raises ValueError with
+    the reference's message when it rejects the config."""
+    lib = _lib(prec)
+    lib.btr_config_build.restype = _P
+    lib.btr_config_build.argtypes = [C.c_char_p]
+    lib.btr_config_error.restype = C.c_char_p
+    lib.btr_config_free.argtypes = [_P]
+    lib.btr_config_counts.argtypes = [_P, _P]
+    lib.btr_config_arrays.argtypes = [_P] * 7
+    h = lib.btr_config_build(text.encode())
+    if not h:
+        raise ValueError(lib.btr_config_error().decode(errors="replace"))
+    h = C.c_void_p(h)
+    try:
+        n = np.zeros(7, np.int64)
+        lib.btr_config_counts(h, _ptr(n))
+        nv, nt, nm, nview = (int(x) for x in n[:4])
+        out = dict(pos=np.zeros((nv, 3)), tris=np.zeros((nt, 3), np.uint32), tri_mat=np.zeros(nt, np.uint16),
+                   mat_color=np.zeros((nm, 3)), views=np.zeros((nview, 7)), lights=np.zeros(22))
+        lib.btr_config_arrays(h, *(_ptr(out[k]) for k in ("pos", "tris", "tri_mat", "mat_color", "views", "lights")))
+        out.update(cull_backfaces=bool(n[4]), has_point_light=bool(n[5]), has_area_light=bool(n[6]))
+        return out
+    finally:
+        lib.btr_config_free(h)

@@ -12,6 +12,7 @@
 // reference has for them (render.cpp, gpu_render.cu) so that per-root output
 // and counters can be read back.
 #include <atomic>
+#include <string>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -455,4 +456,73 @@ BTR_API void btr_tolerances(double* out) {
   out[0] = double(kEpsRel);
   out[1] = double(kKdRel);
   out[2] = double(kDegRel);
+}
+
+// ---- scene ingest: the reference's parseConfig + buildScene (scene.cpp) ----
+namespace {
+struct RefConfig {
+  SceneConfig cfg;
+  Scene scene;
+  std::string err;
+};
+}  // namespace
+
+// Parses `text` and builds its scene; returns a handle, or null with the
+// reason in btr_config_error.  The handle is freed by btr_config_free.
+thread_local std::string g_cfgErr;
+BTR_API void* btr_config_build(const char* text) {
+  auto* r = new RefConfig();
+  std::string err;
+  if (!parseConfig(text, r->cfg, err) || !buildScene(r->cfg, r->scene, err)) {
+    g_cfgErr = err;
+    delete r;
+    return nullptr;
+  }
+  return r;
+}
+BTR_API const char* btr_config_error() { return g_cfgErr.c_str(); }
+BTR_API void btr_config_free(void* h) { delete static_cast<RefConfig*>(h); }
+
+// counts: verts, tris, materials, views, cull, has point light, has area light
+BTR_API void btr_config_counts(void* h, int64_t* out) {
+  const auto* r = static_cast<RefConfig*>(h);
+  out[0] = int64_t(r->scene.pos.size());
+  out[1] = int64_t(r->scene.tris.size());
+  out[2] = int64_t(r->scene.matColor.size());
+  out[3] = int64_t(r->cfg.views.size());
+  out[4] = r->cfg.cullBackfaces;
+  out[5] = r->cfg.hasPointLight;
+  out[6] = r->cfg.hasAreaLight;
+}
+
+// pos (3/vert), tris (3/tri), triMat, matColor (3/material), views (7/view:
+// eye, target, fov), lights (up, point, c, U, V, intensity, background: 22)
+BTR_API void btr_config_arrays(void* h, double* pos, uint32_t* tris, uint16_t* mat, double* color, double* views,
+                               double* lights) {
+  const auto* r = static_cast<RefConfig*>(h);
+  const Scene& s = r->scene;
+  auto put = [](double* d, const Vec3& v) {
+    d[0] = double(v.x);
+    d[1] = double(v.y);
+    d[2] = double(v.z);
+  };
+  for (size_t i = 0; i < s.pos.size(); ++i) put(pos + 3 * i, s.pos[i]);
+  for (size_t i = 0; i < s.tris.size(); ++i)
+    for (int k = 0; k < 3; ++k) tris[3 * i + size_t(k)] = s.tris[i][size_t(k)];
+  for (size_t i = 0; i < s.triMat.size(); ++i) mat[i] = s.triMat[i];
+  for (size_t i = 0; i < s.matColor.size(); ++i) put(color + 3 * i, s.matColor[i]);
+  for (size_t i = 0; i < r->cfg.views.size(); ++i) {
+    put(views + 7 * i, r->cfg.views[i].eye);
+    put(views + 7 * i + 3, r->cfg.views[i].target);
+    views[7 * i + 6] = double(r->cfg.views[i].fovY);
+  }
+  const SceneConfig& c = r->cfg;
+  put(lights, c.up);
+  put(lights + 3, c.pointLight);
+  put(lights + 6, c.lightC);
+  put(lights + 9, c.lightU);
+  put(lights + 12, c.lightV);
+  lights[15] = double(c.lightIntensity);
+  put(lights + 16, c.background);
+  lights[19] = lights[20] = lights[21] = 0;
 }

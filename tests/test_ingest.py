@@ -1,0 +1,219 @@
+"""Scene ingest (bt_scene_load_config / bt_scene_parse_config) and the
+resident-scene cache.
+
+Parity: the scene built from a config is the reference's, bitwise -- float
+positions, triangles after the degeneracy rule, their materials, the
+colours and the views -- against digests the reference itself produced
+(tests/golden/ingest_digests.json, made by tests/golden/make_ingest_golden.py)
+and, where the reference is compiled here, against its parseConfig +
+buildScene array by array, the full-size building config included.
+Configs the reference rejects are rejected with the same reason."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import ingest_cases as cases
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ingest_digests.json")
+
+
+@pytest.fixture(scope="module")
+def mesh_paths(tmp_path_factory):
+    return cases.write_meshes(str(tmp_path_factory.mktemp("meshes")))
+
+
+def _views(sf):
+    return np.array([[*v.eye, *v.target, v.fov] for v in sf.views], np.float32).reshape(-1, 7)
+
+
+def _digest(sf):
+    return cases.digest(sf.pos, sf.tris, sf.tri_mat, sf.mat_color, _views(sf))
+
+
+def test_ingest_matches_reference_digests(native_lib, mesh_paths):
+    from beamtrace2007_b200.ingest import parse_config
+    with open(GOLDEN) as f:
+        golden = json.load(f)
+    texts = cases.configs(mesh_paths)
+    assert set(golden) == set(texts)
+    for name, text in texts.items():
+        sf = parse_config(text)
+        assert (len(sf.tris), len(sf.views)) == (golden[name]["tris"], golden[name]["views"]), name
+        assert _digest(sf) == golden[name]["digest"], name
+
+
+def _same_as_reference(sf, r):
+    assert np.array_equal(sf.pos.astype(np.float64), r["pos"])
+    assert np.array_equal(sf.tris, r["tris"])
+    assert np.array_equal(sf.tri_mat, r["tri_mat"])
+    assert np.array_equal(sf.mat_color.astype(np.float64), r["mat_color"])
+    assert np.array_equal(_views(sf).astype(np.float64), r["views"])
+    L = r["lights"]
+    assert sf.up == tuple(L[0:3])
+    assert (sf.point_light is not None) == r["has_point_light"]
+    if sf.point_light is not None:
+        assert sf.point_light == tuple(L[3:6])
+    assert (sf.area_light is not None) == r["has_area_light"]
+    if sf.area_light is not None:
+        assert sf.area_light == (tuple(L[6:9]), tuple(L[9:12]), tuple(L[12:15]))
+    assert sf.light_intensity == L[15] and sf.background == tuple(L[16:19])
+    assert sf.cull_backfaces == r["cull_backfaces"]
+
+
+def test_ingest_matches_reference_arrays(native_lib, oracle_ready, mesh_paths):
+    from ref import ref_config
+    from beamtrace2007_b200.ingest import parse_config
+    for name, text in cases.configs(mesh_paths).items():
+        _same_as_reference(parse_config(text), ref_config(text))
+
+
+def test_full_building_config_matches_reference(native_lib, oracle_ready):
+    """The reference's own building config: 7 floors of 8 x 8 offices
+    (~2.2M triangles), the camera walking along a corridor."""
+    from ref import ref_config
+    from beamtrace2007_b200.ingest import parse_config
+    text = ("name building\nmesh procedural building floors=7 rooms=8 detail=33\nup 0 1 0\n"
+            "walk 1.0 4.6 17.5  39 4.4 17.5  12 70\npoint_light 2.5 5.6 18.5\n"
+            "area_light 2.5 5.75 17.5  0.8 0 0  0 0 0.8\n")
+    sf = parse_config(text)
+    assert len(sf.tris) > 2_000_000
+    _same_as_reference(sf, ref_config(text))
+
+
+@pytest.mark.parametrize("text,phrase", list(cases.ERRORS.items()))
+def test_rejected_configs(native_lib, text, phrase):
+    from beamtrace2007_b200._native import BtError
+    from beamtrace2007_b200.ingest import parse_config
+    with pytest.raises(BtError) as e:
+        parse_config(text)
+    assert phrase in str(e.value)
+
+
+@pytest.mark.parametrize("text,phrase", list(cases.ERRORS.items()))
+def test_reference_rejects_the_same_configs(oracle_ready, text, phrase):
+    from ref import ref_config
+    with pytest.raises(ValueError) as e:
+        ref_config(text)
+    assert phrase in str(e.value)
+
+
+def test_bad_mesh_files(native_lib, tmp_path):
+    from beamtrace2007_b200._native import BtError
+    from beamtrace2007_b200.ingest import load_config, parse_config
+    bad = tmp_path / "bad.ply"
+    bad.write_text("solid x\nend_header\n")
+    with pytest.raises(BtError, match="not a PLY file"):
+        parse_config(f"mesh ply {bad}\n")
+    odd = tmp_path / "odd.ply"
+    odd.write_text("ply\nformat binary_middle_endian 1.0\nelement vertex 0\nend_header\n")
+    with pytest.raises(BtError, match="unsupported PLY format"):
+        parse_config(f"mesh ply {odd}\n")
+    empty = tmp_path / "empty.obj"
+    empty.write_text("# nothing\n")
+    with pytest.raises(BtError, match="no vertices"):
+        parse_config(f"mesh obj {empty}\n")
+    with pytest.raises(BtError, match="cannot open config"):
+        load_config(str(tmp_path / "missing.cfg"))
+
+
+def test_load_config_reads_the_file(native_lib, mesh_paths, tmp_path):
+    from beamtrace2007_b200.ingest import load_config, parse_config
+    text = cases.configs(mesh_paths)["mixed"]
+    cfg = tmp_path / "mixed.cfg"
+    cfg.write_text(text)
+    a, b = load_config(str(cfg)), parse_config(text)
+    assert a.path == str(cfg) and a.name == "mixed"
+    assert _digest(a) == _digest(b)
+
+
+def test_scene_cache(native_lib, mesh_paths, tmp_path):
+    """A prepared scene comes back from the cache directory with the arrays
+    a fresh preparation gives; a changed mesh file is a new entry; a damaged
+    entry is rebuilt."""
+    from beamtrace2007_b200.ingest import SceneCache
+    from beamtrace2007_b200.renderer import PreparedScene
+    obj = tmp_path / "part.obj"
+    with open(mesh_paths["obj"]) as f:
+        obj.write_text(f.read())
+    cfg = tmp_path / "scene.cfg"
+    cfg.write_text(f"name cached\nmesh procedural plant\nmesh obj {obj} translate 0 3 0\n"
+                   "view 2.6 1.7 3.4  0 0.55 0  45\narea_light 0.9 2.8 0.7  0.4 0 0  0 0 0.4\n")
+    store = str(tmp_path / "cache")
+    c1 = SceneCache(store)
+    sf1, ps1 = c1.get(str(cfg))
+    assert (c1.misses, c1.disk_hits, c1.hits) == (1, 0, 0)
+    assert c1.get(str(cfg))[1] is ps1 and c1.hits == 1
+    fresh = PreparedScene(sf1.pos, sf1.tris)
+    c2 = SceneCache(store)
+    sf2, ps2 = c2.get(str(cfg))
+    assert (c2.misses, c2.disk_hits) == (0, 1)
+    for k in PreparedScene.ARRAYS:
+        assert np.array_equal(getattr(ps2, k), getattr(fresh, k)), k
+    assert (ps2.kd_leaves, ps2.kd_max_depth) == (fresh.kd_leaves, fresh.kd_max_depth)
+    assert _digest(sf2) == _digest(sf1)
+    assert sf2.area_light == sf1.area_light and sf2.name == "cached"
+    assert np.array_equal(sf2.light_array(2.0), sf1.light_array(2.0))
+    # a changed mesh file: a new key, built again
+    key = SceneCache.key(str(cfg))
+    with open(obj, "a") as f:
+        f.write("v 9 9 9\nv 9 8 9\nv 8 9 9\nf -1 -2 -3\n")
+    assert SceneCache.key(str(cfg)) != key
+    c3 = SceneCache(store)
+    _, ps3 = c3.get(str(cfg))
+    assert c3.misses == 1 and ps3.num_tris == ps1.num_tris + 1
+    # a damaged entry: rebuilt
+    entry = os.path.join(store, SceneCache.key(str(cfg)) + ".npz")
+    with open(entry, "wb") as f:
+        f.write(b"not an archive")
+    c4 = SceneCache(store)
+    _, ps4 = c4.get(str(cfg))
+    assert c4.misses == 1 and np.array_equal(ps4.kd_split, ps3.kd_split)
+
+
+REF_ROOM = ("name room\nmesh procedural room\ncull_backfaces 0\nup 0 1 0\norbit 4 1.2 4  2.8 0.7 8 70\n"
+            "point_light 5.5 2.6 2.5\narea_light 4 2.95 4  1 0 0  0 0 1\n")
+REF_PLANT = ("name plant\nmesh procedural plant\nup 0 1 0\nview 2.6 1.7 3.4  0 0.55 0  45\n"
+             "orbit 0 0.7 0  3.8 1.0 12 45\npoint_light 1.0 3.0 0.8\narea_light 0.9 2.8 0.7  0.4 0 0  0 0 0.4\n")
+
+
+@pytest.mark.gpu
+def test_reference_configs_render_as_the_reference(gpu, oracle_ready):
+    """The reference's room and plant configs, ingested, on the GPU: primary
+    hit polygons and point-shadow pieces bitwise the reference float
+    build's; exact soft-shadow visibility within 1e-4 of its FP64 build."""
+    from conftest import piece_keys, to_f32
+    from ref import RefTracer
+    from beamtrace2007_b200.ingest import parse_config
+    from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
+    room = parse_config(REF_ROOM)
+    ps = PreparedScene(room.pos, room.tris)
+    rf = RefTracer(room.pos, room.tris, "f")
+    W = 128
+    light = np.array(room.point_light, np.float32)
+    with GpuRenderer(ps) as g:
+        for v in room.views[:3]:
+            cam = make_camera(v.eye, v.target, v.fov, room.up, W, W)
+            prim = g.primary(cam, tile=16)
+            sh = g.point_shadows(cam, prim, light)
+            pr, _ = rf.primary_tiles(cam.as_array(), W, W, tile=16)
+            hits = to_f32(pr).select(to_f32(pr).tri >= 0)
+            assert np.array_equal(piece_keys(prim, True), piece_keys(hits, True))
+            sr, _ = rf.point_shadows(cam.as_array(), W, W, light.astype(np.float64), prim)
+            assert np.array_equal(piece_keys(sh), piece_keys(to_f32(sr)))
+    plant = parse_config(REF_PLANT)
+    ps = PreparedScene(plant.pos, plant.tris)
+    rf = RefTracer(plant.pos, plant.tris, "f")
+    rd = RefTracer(plant.pos, plant.tris, "d")
+    v = plant.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, plant.up, 96, 72)
+    L = plant.light_array()
+    with GpuRenderer(ps) as g:
+        res = g.soft_shadows(cam, L, exact=True)
+    tri, X, N, _ = rf.primary_rays(cam.as_array(), 96, 72, threads=8)
+    assert np.array_equal(res.tri, tri)
+    vd, _, _, _ = rd.soft_points(L, ps.offset, tri, X, N, exact=True, threads=16)
+    m = tri >= 0
+    assert m.mean() > 0.2
+    assert np.abs(res.vis.astype(np.float64) - vd)[m].max() <= 1e-4

@@ -83,6 +83,32 @@ def test_admission_and_batching(native_lib):
             assert r.result.vis[0] == np.float32(r.result.vis[0])
 
 
+def test_config_scenes_through_the_cache(native_lib, tmp_path):
+    """Scenes given as the reference's configs are ingested and prepared
+    once; a second server on the same cache directory admits them from the
+    stored arrays.  Requests use the config's views and lights."""
+    from beamtrace2007_b200.ingest import SceneCache
+    from beamtrace2007_b200.serving import Request, Server
+    cfg = tmp_path / "room.cfg"
+    cfg.write_text("name room\nmesh procedural room\nup 0 1 0\norbit 4 1.2 4  2.8 0.7 8 70\n"
+                   "point_light 5.5 2.6 2.5\narea_light 4 2.95 4  1 0 0  0 0 1\n")
+    store = str(tmp_path / "cache")
+    results = []
+    for run in range(2):
+        cache = SceneCache(store)
+        with Server({"room": str(cfg)}, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine,
+                    cache=cache) as srv:
+            slot = srv.slots["room"]
+            assert len(slot.data.views) == 8
+            assert np.array_equal(np.float32(slot.data.point_light), np.float32([5.5, 2.6, 2.5]))
+            reqs = [srv.submit(Request(k, "room", 64, 48, view=3)) for k in ("primary", "point", "soft")]
+            for r in reqs:
+                assert r.event.wait(30) and r.error is None
+            results.append([r.result for r in reqs])
+        assert (cache.misses, cache.disk_hits) == ((1, 0) if run == 0 else (0, 1))
+    assert np.array_equal(results[0][0], results[1][0])
+
+
 @pytest.mark.gpu
 def test_mixed_stream_same_as_alone(gpu):
     from beamtrace2007_b200.serving import Server, poisson_stream
