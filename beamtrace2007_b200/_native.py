@@ -126,6 +126,8 @@ SIGNATURES = {
     "bt_kd_sizes": (None, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_kd_view": (None, [_P, C.POINTER(KdDesc)]),
     "bt_kd_free": (None, [_P]),
+    "bt_kd_build_gpu": (_I, [_P, _I64, _P, _P, _I64, _P, C.POINTER(KdParams), C.c_int32, C.POINTER(_P),
+                             C.POINTER(C.c_double)]),
     "bt_scene_load_config": (_I, [C.c_char_p, C.POINTER(_P)]),
     "bt_scene_parse_config": (_I, [C.c_char_p, C.POINTER(_P)]),
     "bt_scene_file_info_get": (None, [_P, C.POINTER(SceneFileInfo)]),

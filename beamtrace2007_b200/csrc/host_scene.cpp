@@ -16,6 +16,8 @@
 #include <vector>
 
 #include "bt_gpu.h"
+#include "kd_rules.h"
+#include "kd_tree.h"
 
 namespace {
 
@@ -74,74 +76,31 @@ struct KdBuild {
     return f3(p[0], p[1], p[2]);
   }
 
-  // Bounds of triangle t clipped to `box` in double, rounded outward, never
-  // beyond `box` or `fallback` (clippedTriangleBounds, kdtree.cpp:77-134).
+  // Bounds of triangle t clipped to `box`, never beyond `box` or `fallback`
+  // (clippedTriangleBounds, kdtree.cpp:77-134; kd_rules.h).
   Aabb clipped(uint32_t t, const Aabb& box, const Aabb& fallback) const {
-    double poly[2][12][3];
-    int n = 3;
-    for (int k = 0; k < 3; ++k) {
-      F3 p = v(t, k);
-      poly[0][k][0] = p.x;
-      poly[0][k][1] = p.y;
-      poly[0][k][2] = p.z;
-    }
-    int cur = 0;
-    for (int axis = 0; axis < 3 && n > 0; ++axis) {
-      for (int side = 0; side < 2 && n > 0; ++side) {
-        double plane = side == 0 ? double(box.lo[axis]) : double(box.hi[axis]);
-        double sign = side == 0 ? 1.0 : -1.0;
-        int m = 0;
-        for (int i = 0; i < n; ++i) {
-          const double* a = poly[cur][i];
-          const double* b = poly[cur][(i + 1) % n];
-          double da = sign * (a[axis] - plane), db = sign * (b[axis] - plane);
-          if (da >= 0) {
-            for (int c = 0; c < 3; ++c) poly[1 - cur][m][c] = a[c];
-            ++m;
-          }
-          if ((da >= 0) != (db >= 0)) {
-            double tt = da / (da - db);
-            for (int c = 0; c < 3; ++c) poly[1 - cur][m][c] = a[c] + tt * (b[c] - a[c]);
-            poly[1 - cur][m][axis] = plane;
-            ++m;
-          }
-        }
-        n = m;
-        cur = 1 - cur;
-      }
-    }
-    if (n == 0) return fallback;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int i = 0; i < n; ++i)
-      for (int c = 0; c < 3; ++c) {
-        lo[c] = std::min(lo[c], poly[cur][i][c]);
-        hi[c] = std::max(hi[c], poly[cur][i][c]);
-      }
-    Aabb r;
-    const double ulp = double(std::numeric_limits<float>::epsilon());
+    const float* v[3];
+    for (int k = 0; k < 3; ++k) v[k] = pos + 3 * size_t(tris[3 * size_t(t) + size_t(k)]);
+    const kdr::Box r = kdr::clippedBounds(v[0], v[1], v[2], toBox(box), toBox(fallback));
+    Aabb a;
     for (int c = 0; c < 3; ++c) {
-      double pad = 4 * ulp * (std::fabs(lo[c]) + std::fabs(hi[c]) + double(box.hi[c] - box.lo[c]));
-      r.lo[c] = float(lo[c] - pad);
-      r.hi[c] = float(hi[c] + pad);
+      a.lo[c] = r.lo[c];
+      a.hi[c] = r.hi[c];
     }
-    for (int a = 0; a < 3; ++a) {
-      float blo = box.lo[a] > fallback.lo[a] ? box.lo[a] : fallback.lo[a];
-      float bhi = box.hi[a] < fallback.hi[a] ? box.hi[a] : fallback.hi[a];
-      r.lo[a] = r.lo[a] > blo ? r.lo[a] : blo;
-      r.hi[a] = r.hi[a] < bhi ? r.hi[a] : bhi;
-      if (r.lo[a] > r.hi[a]) r.lo[a] = r.hi[a];
+    return a;
+  }
+
+  static kdr::Box toBox(const Aabb& b) {
+    kdr::Box r;
+    for (int c = 0; c < 3; ++c) {
+      r.lo[c] = b.lo[c];
+      r.hi[c] = b.hi[c];
     }
     return r;
   }
 
   float sahCost(const Aabb& box, int axis, float s, size_t nl, size_t nr) const {
-    Aabb l = box, r = box;
-    l.hi[axis] = s;
-    r.lo[axis] = s;
-    float inv = 1 / box.surfaceArea();
-    float cost = costTraverse + costIntersect * (l.surfaceArea() * inv * float(nl) + r.surfaceArea() * inv * float(nr));
-    if (nl == 0 || nr == 0) cost *= emptyBonus;
-    return cost;
+    return kdr::sahCost(kdr::Costs{costTraverse, costIntersect, emptyBonus}, toBox(box), axis, s, nl, nr);
   }
 
   // Binned SAH above binThreshold references, exact event sweep below
@@ -158,18 +117,14 @@ struct KdBuild {
         std::vector<size_t> starts(size_t(B), 0), ends(size_t(B), 0);
         float scale = float(B) / (hi - lo);
         for (const TriBox& r : refs) {
-          int bs = int((r.b.lo[axis] - lo) * scale);
-          int be = int((r.b.hi[axis] - lo) * scale);
-          bs = bs < 0 ? 0 : (bs > B - 1 ? B - 1 : bs);
-          be = be < 0 ? 0 : (be > B - 1 ? B - 1 : be);
-          starts[size_t(bs)]++;
-          ends[size_t(be)]++;
+          starts[size_t(kdr::binOf(r.b.lo[axis], lo, scale, B))]++;
+          ends[size_t(kdr::binOf(r.b.hi[axis], lo, scale, B))]++;
         }
         size_t nl = 0, nr = N;
         for (int k = 1; k < B; ++k) {
           nl += starts[size_t(k - 1)];
           nr -= ends[size_t(k - 1)];
-          float s = lo + (hi - lo) * float(k) / float(B);
+          float s = kdr::binPlane(lo, hi, k, B);
           float c = sahCost(box, axis, s, nl, nr);
           if (c < bestCost) {
             bestCost = c;
@@ -261,11 +216,8 @@ struct KdBuild {
     left.reserve(N / 2 + 1);
     right.reserve(N / 2 + 1);
     for (const TriBox& r : refs) {
-      float lo = r.b.lo[bestAxis], hi = r.b.hi[bestAxis];
-      bool planar = lo == hi && lo == bestSplit;
-      bool goLeft = planar || lo < bestSplit;
-      bool goRight = planar || hi > bestSplit;
-      if (!goLeft && !goRight) goLeft = goRight = true;
+      bool goLeft, goRight, planar;
+      kdr::sides(r.b.lo[bestAxis], r.b.hi[bestAxis], bestSplit, goLeft, goRight, planar);
       if (goLeft && goRight && !planar && clipBounds) {
         left.push_back({r.tri, clipped(r.tri, lbox, r.b)});
         right.push_back({r.tri, clipped(r.tri, rbox, r.b)});
@@ -286,13 +238,43 @@ struct KdBuild {
 
 }  // namespace
 
-struct bt_kd_tree {
-  std::vector<float> split;
-  std::vector<uint32_t> data, offset, parent, triIndices;
-  std::vector<float> nodeBox;  // 6 per node: lo xyz, hi xyz
-  float bounds[6];
-  int numLeaves, maxDepth;
-};
+void kdRootAndDepth(const float* sceneBounds, const bt_kd_params& p, int64_t numTris, kdr::Box& root, int& maxDepth) {
+  for (int a = 0; a < 3; ++a) {
+    const float lo = sceneBounds[a], hi = sceneBounds[3 + a];
+    const float pad = (hi - lo) * 1e-4f + 1e-6f;
+    root.lo[a] = lo - pad;
+    root.hi[a] = hi + pad;
+  }
+  const int N = numTris > 1 ? int(numTris) : 1;
+  maxDepth = p.max_depth >= 0 ? p.max_depth : int(8 + 1.3 * std::log2(double(N)));
+  maxDepth = std::min(maxDepth, 63);
+}
+
+void kdFinish(bt_kd_tree* t) {
+  const size_t nn = t->split.size();
+  t->parent.assign(nn, ~0u);
+  t->nodeBox.assign(6 * nn, 0.f);
+  if (!nn) return;
+  for (int a = 0; a < 6; ++a) t->nodeBox[size_t(a)] = t->bounds[a];
+  std::vector<uint32_t> stack(1, 0u);
+  while (!stack.empty()) {
+    const uint32_t i = stack.back();
+    stack.pop_back();
+    const uint32_t d = t->data[i];
+    if ((d & 3u) == 3u) continue;
+    const int a = int(d & 3u);
+    const uint32_t l = i + 1, r = d >> 2;
+    for (int k = 0; k < 6; ++k) {
+      t->nodeBox[6 * size_t(l) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
+      t->nodeBox[6 * size_t(r) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
+    }
+    t->nodeBox[6 * size_t(l) + 3 + size_t(a)] = t->split[i];
+    t->nodeBox[6 * size_t(r) + size_t(a)] = t->split[i];
+    t->parent[l] = t->parent[r] = i;
+    stack.push_back(l);
+    stack.push_back(r);
+  }
+}
 
 extern "C" {
 
@@ -355,24 +337,21 @@ int bt_kd_build(const float* pos, const uint32_t* tris, const float* triArea, in
   b.bins = p.bins;
   b.clipBounds = p.clip_bounds != 0;
   b.singleLeaf = p.single_leaf != 0;
-  // Root box: scene bounds padded by 1e-4 of the diagonal + 1e-6 (kdtree.cpp:301-305).
+  kdr::Box rb;
+  int maxDepth;
+  kdRootAndDepth(sceneBounds, p, numTris, rb, maxDepth);
   Aabb root;
   for (int a = 0; a < 3; ++a) {
-    root.lo[a] = sceneBounds[a];
-    root.hi[a] = sceneBounds[3 + a];
+    root.lo[a] = rb.lo[a];
+    root.hi[a] = rb.hi[a];
   }
-  F3 pad = (root.hi - root.lo) * 1e-4f + f3(1e-6f, 1e-6f, 1e-6f);
-  root.lo = root.lo - pad;
-  root.hi = root.hi + pad;
   std::vector<TriBox> refs(static_cast<size_t>(numTris));
   for (int64_t t = 0; t < numTris; ++t) {
     Aabb bb;
     for (int k = 0; k < 3; ++k) bb.expand(b.v(uint32_t(t), k));
     refs[size_t(t)] = {uint32_t(t), bb};
   }
-  int N = numTris > 1 ? int(numTris) : 1;
-  b.maxDepth = p.max_depth >= 0 ? p.max_depth : int(8 + 1.3 * std::log2(double(N)));
-  b.maxDepth = std::min(b.maxDepth, 63);
+  b.maxDepth = maxDepth;
   try {
     b.build(refs, root, 0);
   } catch (const std::bad_alloc&) {
@@ -380,7 +359,6 @@ int bt_kd_build(const float* pos, const uint32_t* tris, const float* triArea, in
   }
   bt_kd_tree* t = new (std::nothrow) bt_kd_tree();
   if (!t) return BT_ERR_NOMEM;
-  const size_t nn = b.split.size();
   t->split.swap(b.split);
   t->data.swap(b.data);
   t->offset.swap(b.offset);
@@ -391,28 +369,7 @@ int bt_kd_build(const float* pos, const uint32_t* tris, const float* triArea, in
     t->bounds[a] = root.lo[a];
     t->bounds[3 + a] = root.hi[a];
   }
-  // Parents and node boxes as a descent from the root computes them (kdtree.cpp:318-336).
-  t->parent.assign(nn, ~0u);
-  t->nodeBox.assign(6 * nn, 0.f);
-  for (int a = 0; a < 6; ++a) t->nodeBox[size_t(a)] = t->bounds[a];
-  std::vector<uint32_t> stack(1, 0u);
-  while (!stack.empty()) {
-    const uint32_t i = stack.back();
-    stack.pop_back();
-    const uint32_t d = t->data[i];
-    if ((d & 3u) == 3u) continue;
-    const int a = int(d & 3u);
-    const uint32_t l = i + 1, r = d >> 2;
-    for (int k = 0; k < 6; ++k) {
-      t->nodeBox[6 * size_t(l) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
-      t->nodeBox[6 * size_t(r) + size_t(k)] = t->nodeBox[6 * size_t(i) + size_t(k)];
-    }
-    t->nodeBox[6 * size_t(l) + 3 + size_t(a)] = t->split[i];
-    t->nodeBox[6 * size_t(r) + size_t(a)] = t->split[i];
-    t->parent[l] = t->parent[r] = i;
-    stack.push_back(l);
-    stack.push_back(r);
-  }
+  kdFinish(t);
   *out = t;
   return BT_OK;
 }

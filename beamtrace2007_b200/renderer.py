@@ -16,6 +16,7 @@ constructing its renderer: Scene::finalize and KdTree::build (beam SAH cost
 from __future__ import annotations
 
 import ctypes as C
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -77,9 +78,13 @@ def kd_params_default(cost_intersect: float = 0.4) -> dict:
 
 
 class PreparedScene:
-    """A finalised scene and its kd-tree, as host arrays."""
+    """A finalised scene and its kd-tree, as host arrays.  The tree is built
+    on the host (bt_kd_build) or, with `kd_device`, on that CUDA device
+    (bt_kd_build_gpu: the same tree); `kd` overrides other bt_kd_params
+    fields.  `kd_build_ms`: the build's wall-clock time."""
 
-    def __init__(self, pos: np.ndarray, tris: np.ndarray, cost_intersect: float = 0.4, single_leaf: bool = False):
+    def __init__(self, pos: np.ndarray, tris: np.ndarray, cost_intersect: float = 0.4, single_leaf: bool = False,
+                 kd_device: int | None = None, **kd):
         L = N.lib()
         pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
         tris_in = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
@@ -103,9 +108,17 @@ class PreparedScene:
         L.bt_kd_params_default(C.byref(kp))
         kp.cost_intersect = cost_intersect
         kp.single_leaf = int(single_leaf)
+        for k, v in kd.items():
+            setattr(kp, k, v)
         h = C.c_void_p()
-        check(L.bt_kd_build(ptr(self.pos), ptr(self.tris), ptr(self.tri_area), nt, ptr(self.bounds), C.byref(kp),
-                            C.byref(h)))
+        t0 = time.perf_counter()
+        if kd_device is None:
+            check(L.bt_kd_build(ptr(self.pos), ptr(self.tris), ptr(self.tri_area), nt, ptr(self.bounds), C.byref(kp),
+                                C.byref(h)))
+        else:
+            check(L.bt_kd_build_gpu(ptr(self.pos), len(self.pos), ptr(self.tris), ptr(self.tri_area), nt,
+                                    ptr(self.bounds), C.byref(kp), int(kd_device), C.byref(h), None))
+        self.kd_build_ms = (time.perf_counter() - t0) * 1e3
         try:
             d = N.KdDesc()
             L.bt_kd_view(h, C.byref(d))
@@ -153,6 +166,7 @@ class PreparedScene:
                 and ps.tris.ndim == 2 and len(ps.tri_normals) == len(ps.tris) == len(ps.tri_area)):
             raise ValueError("inconsistent prepared-scene arrays")
         ps.kd_leaves, ps.kd_max_depth = (int(x) for x in d["kd_sizes"])
+        ps.kd_build_ms = 0.0
         return ps
 
     @property

@@ -95,10 +95,12 @@ class Server:
     builds a context (GpuRenderer by default; tests may pass a stand-in)."""
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 21,
-                 engine_factory=None, cache=None):
+                 engine_factory=None, cache=None, kd_on_gpu: bool = True):
         from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
-        self.cache = cache if cache is not None else SceneCache()
+        kd_device = device if kd_on_gpu else None
+        self.cache = cache if cache is not None else SceneCache(kd_device=kd_device)
+        self.prep_ms: dict = {}   # scene -> ms to admit it (ingest, finalise, kd-tree)
         self.budget = int(memory_budget_gb * (1 << 30))
         self.device = device
         if engine_factory is None:
@@ -107,10 +109,12 @@ class Server:
         self.slots: dict[str, _SceneSlot] = {}
         self.resident = 0
         for name, sd in scenes.items():
+            t0 = time.perf_counter()
             if isinstance(sd, str):  # a scene config: ingested and prepared through the cache
                 sd, ps = self.cache.get(sd)
             else:
-                ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris)
+                ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris, kd_device=kd_device)
+            self.prep_ms[name] = (time.perf_counter() - t0) * 1e3
             self.resident += 44 * len(ps.kd_split) + 64 * len(ps.kd_tri_indices) + 32 * ps.num_tris
             self.resident += 3 * 64 * queue_records
             slot = _SceneSlot(name, sd, engine_factory(ps, queue_records))

@@ -17,6 +17,7 @@
  * and the host-side preparation the GPU path needs:
  *   bt_scene_finalize       Scene::finalize         src/scene/scene.cpp:89-118
  *   bt_kd_build             KdTree::build           src/accel/kdtree.h:36
+ *   bt_kd_build_gpu         KdTree::build on the GPU (the same tree)
  *   bt_camera_make          Camera::make            src/render/render_types.h:24
  * and scene ingest (configs, OBJ/PLY meshes, procedural scenes):
  *   bt_scene_load_config    loadConfig + buildScene src/scene/scene.h:58-61
@@ -173,6 +174,14 @@ BT_API void bt_kd_sizes(const bt_kd_tree* t, int64_t* num_nodes, int64_t* num_re
                         int32_t* max_depth);
 BT_API void bt_kd_view(const bt_kd_tree* t, bt_kd_desc* d);
 BT_API void bt_kd_free(bt_kd_tree* t);
+/* The same tree, node for node, built on CUDA device `device` (level by
+ * level: binned SAH histograms and exact event sweeps per node, partition
+ * with clipping, leaf sorting on the device; the host numbers the nodes).
+ * num_verts bounds the triangle indices.  *ms (may be NULL): wall-clock time
+ * of the call.  Free the tree with bt_kd_free. */
+BT_API int bt_kd_build_gpu(const float* pos, int64_t num_verts, const uint32_t* tris, const float* tri_area,
+                           int64_t num_tris, const float* scene_bounds, const bt_kd_params* params, int32_t device,
+                           bt_kd_tree** out, double* ms);
 BT_API void bt_camera_make(const float* eye, const float* target, float fov_y, const float* up, int32_t W, int32_t H,
                            bt_camera* cam);
 

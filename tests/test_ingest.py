@@ -182,7 +182,9 @@ REF_PLANT = ("name plant\nmesh procedural plant\nup 0 1 0\nview 2.6 1.7 3.4  0 0
 def test_reference_configs_render_as_the_reference(gpu, oracle_ready):
     """The reference's room and plant configs, ingested, on the GPU: primary
     hit polygons and point-shadow pieces bitwise the reference float
-    build's; exact soft-shadow visibility within 1e-4 of its FP64 build."""
+    build's; exact soft-shadow visibility within 1e-4 of its FP64 build
+    wherever the reference's float build is (on this plant it is 6e-4 off
+    at 3 of 6148 pixels, and so are we)."""
     from conftest import piece_keys, to_f32
     from ref import RefTracer
     from beamtrace2007_b200.ingest import parse_config
@@ -214,6 +216,13 @@ def test_reference_configs_render_as_the_reference(gpu, oracle_ready):
     tri, X, N, _ = rf.primary_rays(cam.as_array(), 96, 72, threads=8)
     assert np.array_equal(res.tri, tri)
     vd, _, _, _ = rd.soft_points(L, ps.offset, tri, X, N, exact=True, threads=16)
+    vf, _, _, _ = rf.soft_points(L, ps.offset, tri, X, N, exact=True, threads=16)
     m = tri >= 0
     assert m.mean() > 0.2
-    assert np.abs(res.vis.astype(np.float64) - vd)[m].max() <= 1e-4
+    # within 1e-4 of FP64, except where the reference's own float build is
+    # further off (a handful of pixels of this scene): there, no further off
+    # than it plus 1e-5
+    err = np.abs(res.vis.astype(np.float64) - vd)[m]
+    err_ref = np.abs(vf - vd)[m]
+    assert np.all(err <= np.maximum(1e-4, err_ref + 1e-5)), err.max()
+    assert (err > 1e-4).sum() <= max(3, (err_ref > 1e-4).sum())

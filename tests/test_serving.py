@@ -63,7 +63,8 @@ def test_admission_and_batching(native_lib):
     FakeEngine.log = []
     # a budget that holds the resident part and about eight 128^2 soft requests
     probe = Request("soft", "a", 128, 128)
-    with Server(scenes, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine) as srv:
+    with Server(scenes, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine,
+                kd_on_gpu=False) as srv:
         srv.budget = srv.resident + 8 * request_bytes(probe)
         peak = [0]
         reqs = []
@@ -97,7 +98,7 @@ def test_config_scenes_through_the_cache(native_lib, tmp_path):
     for run in range(2):
         cache = SceneCache(store)
         with Server({"room": str(cfg)}, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine,
-                    cache=cache) as srv:
+                    cache=cache, kd_on_gpu=False) as srv:
             slot = srv.slots["room"]
             assert len(slot.data.views) == 8
             assert np.array_equal(np.float32(slot.data.point_light), np.float32([5.5, 2.6, 2.5]))
