@@ -1389,7 +1389,9 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
             gC = gridFor(c, clipKernel<App>),
             gF = epsLog ? gridFor(c, traceKernel<App, true, true>) : gridFor(c, traceKernel<App, true>);
   // tail rounds: every root admitted and fewer queued records than this
-  const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads;
+  // (default: a sixth of the trace grid's lanes, about two warps' worth per SM -- the fused kernel clips
+  // inside the divergent walk, which only pays once the queue no longer fills the GPU)
+  const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads / 6;
   const int yieldPct = c->cfg.yield_pct == 0 ? 50 : std::min(c->cfg.yield_pct, 100);
   const int yieldAt = yieldPct < 0 ? INT_MAX : std::max(1, int(int64_t(gT) * kWarps * yieldPct / 100));
   static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");

@@ -114,7 +114,7 @@ typedef struct {
   int32_t kernel_timing;    /* nonzero: CUDA events around the trace kernels fill ms_kernel_trace */
   int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
   int64_t tail_records;     /* tail rounds (one fused trace-and-clip kernel) below this many queued
-                               records once every root is admitted; 0 = the trace grid's lanes, < 0 = never */
+                               records once every root is admitted; 0 = a sixth of the trace grid's lanes, < 0 = never */
   int32_t eps_stats;        /* nonzero: trace kernels that also count the edge votes in the fuzzy band
                                and their FP64 re-evaluation (eps_band_corners, eps_fp64_flips); results
                                are the same, the kernels are slower */
