@@ -333,10 +333,11 @@ struct AdmitEnv {
   __device__ void dropped(float) {}
 };
 
-// Clip emission into the next round's trace queue: pieces collect in chunks
-// of kChunk, each chunk appended with one atomic, so siblings stay adjacent
-// (wfSplitEmit, wavefront_core.h:367-422).
-constexpr int kChunk = 8;
+// Clip emission into the next round's trace queue (wfSplitEmit,
+// wavefront_core.h:367-422): the slots pass 1 counted are reserved with one
+// atomic and each piece is written straight into its own, so siblings stay
+// adjacent; slots left by slivers that beamGeom drops are filled with empty
+// records (n = -1), which the trace kernel skips.
 template <int App>
 struct SplitEnv {
   const RoundParams* p;
@@ -344,29 +345,46 @@ struct SplitEnv {
   float lightArea;
   int root;
   Stats* st;
-  int written;
-  int nbuf;
+  SubBeam* dst;   // the reserved slots
+  int reserved;
+  int filled;
   SubBeam* keep;  // tail rounds: the first piece stays with the clipping lane
   bool kept;
-  SubBeam buf[kChunk];
-  __device__ void flush() {
-    if (nbuf == 0) return;
+  __device__ void reserve(int n) {
+    reserved = 0;
+    filled = 0;
+    dst = nullptr;
+    if (n <= 0) return;
     const int nxt = p->cur ^ 1;
-    const int at = queueAppend(*p, nxt, nbuf);
-    if (at >= 0)
-      for (int i = 0; i < nbuf; ++i) p->tq[nxt][at + i] = buf[i];
-    written += nbuf;
-    nbuf = 0;
+    const int at = queueAppend(*p, nxt, n);
+    if (at < 0) return;
+    dst = p->tq[nxt] + at;
+    reserved = n;
+  }
+  // empty records in the slots no piece took; returns their number
+  __device__ int finish() {
+    for (int i = filled; i < reserved; ++i) {
+      SubBeam d;
+      for (int k = 0; k < 4; ++k) d.qx[k] = d.qy[k] = 0.f;
+      d.trail = 0;
+      d.node = 0;
+      d.root = root;
+      d.hit = -1;
+      d.cursor = 0;
+      d.depth = 0;
+      d.n = -1;
+      d.neg = 0;
+      dst[i] = d;
+    }
+    return reserved - filled;
   }
   __device__ bool queue(const SubBeam& r) {
     if (keep && !kept) {
       *keep = r;
       kept = true;
-      ++written;
       return true;
     }
-    buf[nbuf++] = r;
-    if (nbuf == kChunk) flush();
+    if (filled < reserved) dst[filled++] = r;
     return true;
   }
   __device__ void occluded(const Beam& b, int tri) { outputPiece<App>(*p, *q, lightArea, root, b, tri, *st); }
@@ -594,15 +612,17 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   env.lightArea = lightArea;
   env.root = root;
   env.st = &st;
-  env.written = 0;
-  env.nbuf = 0;
   env.keep = keep;
   env.kept = false;
+  // `slots` pieces at most: one may stay with the lane (tail rounds), the
+  // rest take reserved queue slots
+  env.reserve(keep ? slots - 1 : slots);
   splitPass2(q, rec, b, ti, L, nl, env, st, &log);
-  env.flush();
-  if (kept) *kept = env.kept;
   // slivers dropped by beamGeom were counted in `slots` but never queued
-  if (env.written < slots) liveSub(p, root, slots - env.written);
+  // (nor kept)
+  const int unused = env.finish() + (keep && !env.kept ? 1 : 0);
+  if (kept) *kept = env.kept;
+  if (unused > 0) liveSub(p, root, unused);
   return false;
 }
 
@@ -715,6 +735,8 @@ __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant
         r = queue[i];
         if (uint32_t(r.root) >= uint32_t(p.rootCap) || r.node >= p.s.numNodes || r.n > 4) {
           atomicExch(&p.ctr->error, 2);  // a malformed record: report, never index with it
+        } else if (r.n < 0) {
+          // an empty slot of a clip's reservation
         } else if (r.n == 0 || p.state[r.root] == kRootKilled) {
           liveSub(p, r.root, 1);  // a dropped sliver or an abandoned root
         } else {
