@@ -24,9 +24,15 @@
 #if defined(__CUDACC__)
 #define BT_HD __host__ __device__ __forceinline__
 #define BT_COLD __host__ __device__ __noinline__
+#define BT_UNROLL _Pragma("unroll")
+// the polygon steps of a clip: inlined into the one out-of-line clip
+// routine, so that its polygons can stay in registers
+#define BT_CLIP __host__ __device__ __forceinline__
 #else
 #define BT_HD inline
 #define BT_COLD __attribute__((noinline))
+#define BT_UNROLL
+#define BT_CLIP inline
 #endif
 
 // Vertices of a clip polygon.  The reference sizes its lists for 8
@@ -117,44 +123,70 @@ BT_HD bool planeProject(const Plane& P, V3 p, float& qx, float& qy) {
 
 // ------------------------------------------------------------ 2D polygons
 
+// A convex polygon of at most N vertices.  Every element access is either
+// at a compile-time index (loops unrolled to N, guarded by i < n) or a
+// select chain over the N slots, so that a polygon held in a local variable
+// stays in registers: a run-time array index would put it in local memory,
+// which the clip step otherwise reads and writes hundreds of times per
+// record.  The arithmetic is the same operations in the same order.
 template <int N>
 struct Poly {
   float x[N], y[N];
   int n;
+  BT_HD float X(int i) const {
+    float v = x[0];
+    BT_UNROLL for (int k = 1; k < N; ++k) v = i == k ? x[k] : v;
+    return v;
+  }
+  BT_HD float Y(int i) const {
+    float v = y[0];
+    BT_UNROLL for (int k = 1; k < N; ++k) v = i == k ? y[k] : v;
+    return v;
+  }
+  BT_HD void set(int i, float px, float py) {
+    BT_UNROLL for (int k = 0; k < N; ++k) {
+      x[k] = i == k ? px : x[k];
+      y[k] = i == k ? py : y[k];
+    }
+  }
+  // vertex after i (i < n): i + 1, or 0 at the end
+  BT_HD float nextX(int i) const { return i + 1 == n ? x[0] : x[i + 1 < N ? i + 1 : 0]; }
+  BT_HD float nextY(int i) const { return i + 1 == n ? y[0] : y[i + 1 < N ? i + 1 : 0]; }
   BT_HD void clear() { n = 0; }
   BT_HD void push(float px, float py) {
     if (n < N) {
-      x[n] = px;
-      y[n] = py;
+      set(n, px, py);
       ++n;
     }
   }
   // Signed area, accumulated as beam_geom.h:27-34 does.
   BT_HD float area() const {
     float a = 0;
-    for (int i = 0; i < n; ++i) {
-      int j = i + 1 == n ? 0 : i + 1;
-      a += x[i] * y[j] - x[j] * y[i];
+    BT_UNROLL for (int i = 0; i < N; ++i) {
+      if (i < n) a += x[i] * nextY(i) - nextX(i) * y[i];
     }
     return a * 0.5f;
   }
   BT_HD void reverse() {
-    for (int i = 0, j = n - 1; i < j; ++i, --j) {
-      float tx = x[i];
-      x[i] = x[j];
-      x[j] = tx;
-      float ty = y[i];
-      y[i] = y[j];
-      y[j] = ty;
+    float rx[N], ry[N];
+    BT_UNROLL for (int k = 0; k < N; ++k) {
+      rx[k] = k < n ? X(n - 1 - k) : x[k];
+      ry[k] = k < n ? Y(n - 1 - k) : y[k];
+    }
+    BT_UNROLL for (int k = 0; k < N; ++k) {
+      x[k] = rx[k];
+      y[k] = ry[k];
     }
   }
   BT_HD float extent() const {
     float lx = kInf, hx = -kInf, ly = kInf, hy = -kInf;
-    for (int i = 0; i < n; ++i) {
-      lx = x[i] < lx ? x[i] : lx;
-      hx = x[i] > hx ? x[i] : hx;
-      ly = y[i] < ly ? y[i] : ly;
-      hy = y[i] > hy ? y[i] : hy;
+    BT_UNROLL for (int i = 0; i < N; ++i) {
+      if (i < n) {
+        lx = x[i] < lx ? x[i] : lx;
+        hx = x[i] > hx ? x[i] : hx;
+        ly = y[i] < ly ? y[i] : ly;
+        hy = y[i] > hy ? y[i] : hy;
+      }
     }
     float ex = hx - lx, ey = hy - ly;
     return ex > ey ? ex : ey;
@@ -162,9 +194,11 @@ struct Poly {
   template <int M>
   BT_HD void copyFrom(const Poly<M>& o) {
     n = o.n < N ? o.n : N;
-    for (int i = 0; i < n; ++i) {
-      x[i] = o.x[i];
-      y[i] = o.y[i];
+    BT_UNROLL for (int i = 0; i < (N < M ? N : M); ++i) {
+      if (i < n) {
+        x[i] = o.x[i];
+        y[i] = o.y[i];
+      }
     }
   }
 };
@@ -208,34 +242,48 @@ BT_HD Line makeLine(float a, float b, float c, float ext) {
 // Fuzzy split of convex p by L; crossings computed from the
 // lexicographically smaller endpoint (beam_geom.h:83-114).
 template <int N>
-BT_COLD bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out) {
+BT_CLIP bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out) {
   in.clear();
   out.clear();
   float d[N];
   int cls[N];
   int nin = 0, nout = 0;
-  for (int i = 0; i < p.n; ++i) {
-    d[i] = L.eval(p.x[i], p.y[i]);
-    cls[i] = d[i] > eps ? 1 : (d[i] < -eps ? -1 : 0);
+  BT_UNROLL for (int i = 0; i < N; ++i) {
+    d[i] = 0.f;
+    cls[i] = 0;
+    if (i < p.n) {
+      d[i] = L.eval(p.x[i], p.y[i]);
+      cls[i] = d[i] > eps ? 1 : (d[i] < -eps ? -1 : 0);
+    }
   }
-  for (int i = 0; i < p.n; ++i) {
-    int j = i + 1 == p.n ? 0 : i + 1;
-    nin += (cls[i] >= 0) + (cls[i] * cls[j] < 0);
-    nout += (cls[i] <= 0) + (cls[i] * cls[j] < 0);
+  BT_UNROLL for (int i = 0; i < N; ++i) {
+    if (i < p.n) {
+      const int cj = i + 1 == p.n ? cls[0] : cls[i + 1 < N ? i + 1 : 0];
+      nin += (cls[i] >= 0) + (cls[i] * cj < 0);
+      nout += (cls[i] <= 0) + (cls[i] * cj < 0);
+    }
   }
   if (nin > N || nout > N) return false;
-  for (int i = 0; i < p.n; ++i) {
-    int j = i + 1 == p.n ? 0 : i + 1;
-    if (cls[i] >= 0) in.push(p.x[i], p.y[i]);
-    if (cls[i] <= 0) out.push(p.x[i], p.y[i]);
-    if (cls[i] * cls[j] < 0) {
-      bool iFirst = p.x[i] < p.x[j] || (p.x[i] == p.x[j] && p.y[i] < p.y[j]);
-      int a = iFirst ? i : j, b = iFirst ? j : i;
-      float t = d[a] / (d[a] - d[b]);
-      float X = p.x[a] + t * (p.x[b] - p.x[a]);
-      float Y = p.y[a] + t * (p.y[b] - p.y[a]);
-      in.push(X, Y);
-      out.push(X, Y);
+  BT_UNROLL for (int i = 0; i < N; ++i) {
+    if (i < p.n) {
+      const bool wrap = i + 1 == p.n;
+      const int jn = i + 1 < N ? i + 1 : 0;
+      const int cj = wrap ? cls[0] : cls[jn];
+      const float dj = wrap ? d[0] : d[jn];
+      const float xj = wrap ? p.x[0] : p.x[jn], yj = wrap ? p.y[0] : p.y[jn];
+      if (cls[i] >= 0) in.push(p.x[i], p.y[i]);
+      if (cls[i] <= 0) out.push(p.x[i], p.y[i]);
+      if (cls[i] * cj < 0) {
+        const bool iFirst = p.x[i] < xj || (p.x[i] == xj && p.y[i] < yj);
+        const float da = iFirst ? d[i] : dj, db = iFirst ? dj : d[i];
+        const float xa = iFirst ? p.x[i] : xj, xb = iFirst ? xj : p.x[i];
+        const float ya = iFirst ? p.y[i] : yj, yb = iFirst ? yj : p.y[i];
+        float t = da / (da - db);
+        float X = xa + t * (xb - xa);
+        float Y = ya + t * (yb - ya);
+        in.push(X, Y);
+        out.push(X, Y);
+      }
     }
   }
   return true;
@@ -244,7 +292,7 @@ BT_COLD bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, 
 // Welds duplicate / collinear vertices within 1e-3 of the split epsilon
 // (beam_geom.h:122-150); n = 0 if the polygon collapses.
 template <int N>
-BT_COLD void cleanPoly(Poly<N>& p, float epsSplit) {
+BT_CLIP void cleanPoly(Poly<N>& p, float epsSplit) {
   const float eps = epsSplit * 1e-3f;
   bool changed = true;
   while (changed && p.n >= 3) {
@@ -252,17 +300,21 @@ BT_COLD void cleanPoly(Poly<N>& p, float epsSplit) {
     for (int i = 0; i < p.n && p.n >= 3; ++i) {
       int h = i == 0 ? p.n - 1 : i - 1;
       int j = i + 1 == p.n ? 0 : i + 1;
-      float ex = p.x[j] - p.x[h], ey = p.y[j] - p.y[h];
-      float dx = p.x[i] - p.x[h], dy = p.y[i] - p.y[h];
+      const float xh = p.X(h), yh = p.Y(h), xi = p.X(i), yi = p.Y(i), xj = p.X(j), yj = p.Y(j);
+      float ex = xj - xh, ey = yj - yh;
+      float dx = xi - xh, dy = yi - yh;
       float len = sqrtf(ex * ex + ey * ey);
       float dist2 = dx * dx + dy * dy;
       float cr = fabs_(ex * dy - ey * dx);
       bool dup = dist2 <= eps * eps;
       bool collinear = cr <= eps * len;
       if (dup || collinear) {
-        for (int k = i; k + 1 < p.n; ++k) {
-          p.x[k] = p.x[k + 1];
-          p.y[k] = p.y[k + 1];
+        // drop vertex i: the later ones move down one slot
+        BT_UNROLL for (int k = 0; k + 1 < N; ++k) {
+          if (k >= i && k + 1 < p.n) {
+            p.x[k] = p.x[k + 1];
+            p.y[k] = p.y[k + 1];
+          }
         }
         --p.n;
         changed = true;
@@ -278,12 +330,14 @@ BT_COLD void cleanPoly(Poly<N>& p, float epsSplit) {
 template <int N>
 BT_HD int classifyPoly(const Poly<N>& p, const Line& L, float eps) {
   int c = 0;
-  for (int i = 0; i < p.n; ++i) {
-    float d = L.eval(p.x[i], p.y[i]);
-    if (d > eps)
-      c |= 1;
-    else if (d < -eps)
-      c |= 2;
+  BT_UNROLL for (int i = 0; i < N; ++i) {
+    if (i < p.n) {
+      float d = L.eval(p.x[i], p.y[i]);
+      if (d > eps)
+        c |= 1;
+      else if (d < -eps)
+        c |= 2;
+    }
   }
   return c;
 }
@@ -372,22 +426,22 @@ BT_HD void setStatus(const Query& q, Beam& b, int hit, const float* A, float C) 
 // (lanes past n repeat corner n-1, as beamGeom's l3 rule does).
 template <int N>
 BT_HD void beamCorners(const Poly<N>& c, Beam& b) {
-  int l3 = c.n > 3 ? 3 : 2;
+  const bool four = c.n > 3;
   b.qx[0] = c.x[0];
   b.qx[1] = c.x[1];
   b.qx[2] = c.x[2];
-  b.qx[3] = c.x[l3];
+  b.qx[3] = four ? c.x[3] : c.x[2];
   b.qy[0] = c.y[0];
   b.qy[1] = c.y[1];
   b.qy[2] = c.y[2];
-  b.qy[3] = c.y[l3];
+  b.qy[3] = four ? c.y[3] : c.y[2];
   b.n = c.n;
 }
 
 // Cleaned corners and axes of a piece; false (and `dropped` = |area|) for
 // slivers below minArea (BeamCtx::beamGeom, beam_core.h:200-221).
 template <int N>
-BT_COLD bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped) {
+BT_CLIP bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped) {
   Poly<N> c = p;
   cleanPoly(c, q.eps);
   float A = c.n >= 3 ? c.area() : 0.f;
@@ -638,45 +692,74 @@ BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* 
 // Clips B by L[0..nl) one line at a time, most-cutting edge first; pieces
 // outside some line go to sink.push(0, p), pieces inside every line to
 // sink.push(1, p) (BeamCtx::clipTri with orderEdges, beam_core.h:420-479).
+// Line li (run-time, < 5) of five held in registers.
+BT_HD Line lineAt(const Line* L, int li) {
+  Line r = L[0];
+  BT_UNROLL for (int k = 1; k < 5; ++k) {
+    r.a = li == k ? L[k].a : r.a;
+    r.b = li == k ? L[k].b : r.b;
+    r.c = li == k ? L[k].c : r.c;
+  }
+  return r;
+}
+
 template <int N, class Sink>
-BT_COLD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink, uint32_t& fiveSplits) {
+BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sink& sink, uint32_t& fiveSplits) {
+  Line L[5];
+  BT_UNROLL for (int k = 0; k < 5; ++k) L[k] = Lin[k];
   {
     float score[3];
-    for (int k = 0; k < 3; ++k) {
+    BT_UNROLL for (int k = 0; k < 3; ++k) {
       float pos[4];
-      for (int i = 0; i < 4; ++i) {
+      BT_UNROLL for (int i = 0; i < 4; ++i) {
         float dv = B.qx[i] * L[k].a + B.qy[i] * L[k].b + L[k].c;
         pos[i] = dv > 0.f ? dv : 0.f;
       }
       score[k] = pos[0] + pos[1] + pos[2] + (B.n == 4 ? pos[3] : 0.f);
     }
-    for (int i = 1; i < 3; ++i)
-      for (int j = i; j > 0 && score[j] < score[j - 1]; --j) {
-        float ts = score[j];
-        score[j] = score[j - 1];
-        score[j - 1] = ts;
-        Line tl = L[j];
-        L[j] = L[j - 1];
-        L[j - 1] = tl;
+    // insertion sort of the three edge lines by score (stable)
+    if (score[1] < score[0]) {
+      float ts = score[0];
+      score[0] = score[1];
+      score[1] = ts;
+      Line tl = L[0];
+      L[0] = L[1];
+      L[1] = tl;
+    }
+    if (score[2] < score[1]) {
+      float ts = score[1];
+      score[1] = score[2];
+      score[2] = ts;
+      Line tl = L[1];
+      L[1] = L[2];
+      L[2] = tl;
+      if (score[1] < score[0]) {
+        ts = score[0];
+        score[0] = score[1];
+        score[1] = ts;
+        tl = L[0];
+        L[0] = L[1];
+        L[1] = tl;
       }
+    }
   }
   bool ok = true;
+  // pending pentagon halves (LIFO), with the line each resumes at
   Poly<N> stack[8];
   int stackLine[8];
-  int sp = 1;
-  stack[0].n = B.n;
-  for (int i = 0; i < B.n; ++i) {
-    stack[0].x[i] = B.qx[i];
-    stack[0].y[i] = B.qy[i];
+  int sp = 0;
+  Poly<N> p;
+  p.n = B.n;
+  BT_UNROLL for (int i = 0; i < 4; ++i) {
+    p.x[i] = B.qx[i];
+    p.y[i] = B.qy[i];
   }
-  stackLine[0] = 0;
-  while (sp > 0) {
-    --sp;
-    Poly<N> p = stack[sp];
-    int li = stackLine[sp];
+  int li = 0;
+  for (;;) {
     bool inside = true;
     for (; li < nl; ++li) {
-      int c = classifyPoly(p, L[li], q.eps);
+      const Line Lk = lineAt(L, li);
+      int c = classifyPoly(p, Lk, q.eps);
       if (!(c & 2)) continue;
       if (!(c & 1)) {
         if (!sink.push(0, p)) ok = false;
@@ -684,7 +767,7 @@ BT_COLD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink,
         break;
       }
       Poly<N> in, out;
-      if (!splitPoly(p, L[li], q.eps, in, out)) return false;
+      if (!splitPoly(p, Lk, q.eps, in, out)) return false;
       cleanPoly(out, q.eps);
       if (out.n >= 3 && !sink.push(0, out)) ok = false;
       cleanPoly(in, q.eps);
@@ -706,6 +789,10 @@ BT_COLD bool clipTri(const Query& q, const Beam& B, Line* L, int nl, Sink& sink,
       }
     }
     if (inside && !sink.push(1, p)) ok = false;
+    if (sp == 0) break;
+    --sp;
+    p = stack[sp];
+    li = stackLine[sp];
   }
   return ok;
 }

@@ -845,7 +845,10 @@ __global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant
 // round's trace queue.  A record whose clip changes nothing measurable
 // continues at its next triangle in the next round.
 template <int App>
-__global__ void __launch_bounds__(kThreads) clipKernel(const __grid_constant__ RoundParams p) {
+// (At least 4 CTAs per SM, i.e. at most 128 registers: with its polygons
+// in registers the clip step would take 255 and run 2 CTAs per SM; 4 keeps
+// enough warps for its latency and spills little -- measured 3 and 6 too.)
+__global__ void __launch_bounds__(kThreads, 4) clipKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   // clip records fill the clip queue from the bottom, deferred outputs from
   // the top; together they are at most the round's trace records

@@ -487,34 +487,34 @@ struct EmitSink {
   int t;
   Env* env;
   Stats* st;
+  BT_HD void one(bool hitNow, bool queued, const Poly<kPolyMax>& piece) {
+    Beam nb;
+    float dropped = 0;
+    if (!beamGeom(*q, piece, parent->neg, nb, dropped)) {
+      st->dropped += double(dropped);
+      env->dropped(dropped);
+      return;
+    }
+    if (!queued) {
+      env->occluded(nb, t);
+      return;
+    }
+    SubBeam pr = *base;
+    storeGeom(nb, pr);
+    pr.hit = hitNow ? t : parent->hit;
+    env->queue(pr);
+  }
   BT_HD bool push(int l, const Poly<kPolyMax>& p0) {
     const bool hitNow = l == 1;
     const bool queued = !(hitNow && q->mode == kModeAnyHit);
-    Poly<kPolyMax> sub[2];
-    int ns = 1;
     if (p0.n == 5) {
-      splitFive(p0, sub[0], sub[1]);
+      Poly<kPolyMax> a, b;
+      splitFive(p0, a, b);
       st->fiveSplits++;
-      ns = 2;
+      one(hitNow, queued, a);
+      one(hitNow, queued, b);
     } else {
-      sub[0] = p0;
-    }
-    for (int j = 0; j < ns; ++j) {
-      Beam nb;
-      float dropped = 0;
-      if (!beamGeom(*q, sub[j], parent->neg, nb, dropped)) {
-        st->dropped += double(dropped);
-        env->dropped(dropped);
-        continue;
-      }
-      if (!queued) {
-        env->occluded(nb, t);
-        continue;
-      }
-      SubBeam pr = *base;
-      storeGeom(nb, pr);
-      pr.hit = hitNow ? t : parent->hit;
-      env->queue(pr);
+      one(hitNow, queued, p0);
     }
     return true;
   }
@@ -532,7 +532,7 @@ struct PieceLog {
     if (count < kPieceLog) {
       level[count] = int8_t(l);
       n[count] = int8_t(p.n);
-      for (int i = 0; i < 5; ++i) {
+      BT_UNROLL for (int i = 0; i < 5; ++i) {
         x[count][i] = i < p.n ? p.x[i] : 0.f;
         y[count][i] = i < p.n ? p.y[i] : 0.f;
       }
@@ -564,20 +564,18 @@ struct ClipSink {
 // lists (the root must be abandoned), else the slots pass 2 will use
 // (0 if nothing changes: the record continues unchanged at cursor + 1).
 template <class Env>
-BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
+BT_CLIP int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
                        Line* L, int& nl, bool& commit, PieceLog* log = nullptr) {
   const uint2 leaf = s.node[r.node];
   setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
   classifyTri(q, B, ti, L, nl);
-  Line Lc[5];
-  for (int i = 0; i < nl; ++i) Lc[i] = L[i];
   ClipSink<Env> sink;
   sink.emitting = 0;
   sink.area = AreaSink{0.f, 0, 0};
   sink.log = log;
   if (log) log->count = 0;
   uint32_t five = 0;
-  if (!clipTri<kPolyMax>(q, B, Lc, nl, sink, five)) return -1;
+  if (!clipTri<kPolyMax>(q, B, L, nl, sink, five)) return -1;
   st.fiveSplits += five;
   commit = sink.area.newArea >= q.minArea;
   if (!commit) return 0;
@@ -585,7 +583,7 @@ BT_COLD int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, cons
 }
 
 template <class Env>
-BT_COLD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
+BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
                         Stats& st, const PieceLog* log = nullptr) {
   st.splits++;
   SubBeam base = r;
@@ -596,7 +594,7 @@ BT_COLD void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const T
     for (int k = 0; k < log->count; ++k) {
       Poly<kPolyMax> p;
       p.n = log->n[k];
-      for (int i = 0; i < kPolyMax; ++i) {
+      BT_UNROLL for (int i = 0; i < kPolyMax; ++i) {
         p.x[i] = i < 5 ? log->x[k][i] : 0.f;
         p.y[i] = i < 5 ? log->y[k][i] : 0.f;
       }
