@@ -124,6 +124,12 @@ struct AppParams {
   const int32_t* pixTri;
   const float* pixX;
   const float* pixN;
+  // fused primary rays: admission traces each pixel's eye ray itself and
+  // writes tri, X, N here (instead of reading them from a primary-ray pass)
+  int fusedPrimary;
+  int32_t* pixTriOut;
+  float* pixXOut;
+  float* pixNOut;
   float *vis, *E, *Eu;
   unsigned long long* missFx;
   unsigned long long* gFx;
@@ -313,6 +319,117 @@ __device__ __forceinline__ int queueAppend(const RoundParams& p, int q, int n) {
   return at;
 }
 
+// ------------------------------------------------------------ primary rays
+
+// Moller-Trumbore (rayHitTri, src/ray/ray_core.h:22-37).
+__device__ __forceinline__ float rayHit(V3 o, V3 d, V3 v0, V3 v1, V3 v2) {
+  V3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+  V3 pv = cross(d, e2);
+  float det = dot(e1, pv);
+  if (det == 0) return kInf;
+  float inv = 1 / det;
+  V3 tv = sub(o, v0);
+  float u = dot(tv, pv) * inv;
+  if (u < 0 || u > 1) return kInf;
+  V3 qv = cross(tv, e1);
+  float v = dot(d, qv) * inv;
+  if (v < 0 || u + v > 1) return kInf;
+  return dot(e2, qv) * inv;
+}
+
+// The eye ray through the centre of pixel (x, y), nearest hit with coplanar
+// ties to the lower id (rayTraverse<false>, src/ray/ray_core.h:42-132):
+// returns the triangle (-1: none) and sets X, N (normal facing the eye; 0
+// when nothing is hit).
+__device__ __noinline__ int eyeRay(const SceneDev& s, V3 o, V3 fwd, V3 right, V3 down, float halfW, float halfH,
+                                   int W, int H, int x, int y, V3* Xo, V3* No) {
+  const float qx = (2 * (float(x) + 0.5f) / float(W) - 1) * halfW;
+  const float qy = (2 * (float(y) + 0.5f) / float(H) - 1) * halfH;
+  const V3 d = add(add(fwd, mul(right, qx)), mul(down, qy));
+  *Xo = mk(0, 0, 0);
+  *No = mk(0, 0, 0);
+  float t0 = 0, t1 = kInf;
+  float inv[3];
+  for (int a = 0; a < 3; ++a) {
+    const float da = comp(d, a), oa = comp(o, a);
+    inv[a] = 1 / da;
+    if (da == 0) {
+      if (oa < s.bounds.lo[a] || oa > s.bounds.hi[a]) return -1;
+      continue;
+    }
+    float ta = (s.bounds.lo[a] - oa) * inv[a];
+    float tb = (s.bounds.hi[a] - oa) * inv[a];
+    if (ta > tb) {
+      float tt = ta;
+      ta = tb;
+      tb = tt;
+    }
+    t0 = t0 > ta ? t0 : ta;
+    t1 = t1 < tb ? t1 : tb;
+  }
+  if (t0 > t1) return -1;
+  struct Entry {
+    uint32_t node;
+    float t0, t1;
+  };
+  Entry stk[64];
+  int sp = 0;
+  uint32_t node = s.rootNode;
+  float best = kInf;
+  int bestTri = -1;
+  const float tieEps = 4 * 1.1920928955078125e-07f;
+  for (;;) {
+    const uint2 nd = s.node[node];
+    if (!isLeaf(nd)) {
+      const int a = int(nd.y & 3u);
+      const float sp_ = splitOf(nd);
+      const float oa = comp(o, a), da = comp(d, a);
+      const bool belowFirst = oa < sp_ || (oa == sp_ && da <= 0);
+      const uint32_t first = belowFirst ? node + 1 : (nd.y >> 2);
+      const uint32_t second = belowFirst ? (nd.y >> 2) : node + 1;
+      if (da == 0) {
+        node = first;
+        continue;
+      }
+      const float tp = (sp_ - oa) * inv[a];
+      if (tp > t1 || tp <= 0) {
+        node = first;
+      } else if (tp < t0) {
+        node = second;
+      } else {
+        if (sp < 64) stk[sp++] = Entry{second, tp, t1};
+        node = first;
+        t1 = tp;
+      }
+      continue;
+    }
+    const uint32_t cnt = nd.y >> 2;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      const TriRec t = loadRef(s, nd.x + i);
+      const float th = rayHit(o, d, t.v0, t.v1, t.v2);
+      if (!(th > 0 && th < kInf)) continue;
+      const float tol = bestTri < 0 ? 0.f : best * tieEps;
+      if (bestTri < 0 || th < best - tol || (th <= best + tol && t.tri < bestTri)) {
+        best = th;
+        bestTri = t.tri;
+      }
+    }
+    if (bestTri >= 0 && best <= t1) break;
+    if (sp == 0) break;
+    --sp;
+    node = stk[sp].node;
+    t0 = stk[sp].t0;
+    t1 = stk[sp].t1;
+  }
+  if (bestTri < 0) return -1;
+  *Xo = add(o, mul(d, best));
+  V3 nT, v0;
+  triNV(s, bestTri, nT, v0);
+  if (dot(nT, d) > 0) nT = neg(nT);
+  *No = nT;
+  return bestTri;
+}
+
 // Admission: every pre-split piece goes to the round's trace queue.
 template <int App>
 struct AdmitEnv {
@@ -453,7 +570,20 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
       rootDone(p);
       return false;
     }
-    const int T = a.pixTri[pix];
+    int T;
+    V3 x, ns;
+    if (a.fusedPrimary) {
+      T = eyeRay(sj, a.eye, a.fwd, a.right, a.down, a.halfW, a.halfH, a.W, a.H, pix % a.W, pix / a.W, &x, &ns);
+      a.pixTriOut[pix] = T;
+      a.pixXOut[3 * pix] = x.x;
+      a.pixXOut[3 * pix + 1] = x.y;
+      a.pixXOut[3 * pix + 2] = x.z;
+      a.pixNOut[3 * pix] = ns.x;
+      a.pixNOut[3 * pix + 1] = ns.y;
+      a.pixNOut[3 * pix + 2] = ns.z;
+    } else {
+      T = a.pixTri[pix];
+    }
     if (T < 0) {
       if (a.vis) a.vis[pix] = -1;
       if (a.E) a.E[pix] = 0;
@@ -461,8 +591,10 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
       rootDone(p);
       return false;
     }
-    const V3 x = mk(a.pixX[3 * pix], a.pixX[3 * pix + 1], a.pixX[3 * pix + 2]);
-    const V3 ns = mk(a.pixN[3 * pix], a.pixN[3 * pix + 1], a.pixN[3 * pix + 2]);
+    if (!a.fusedPrimary) {
+      x = mk(a.pixX[3 * pix], a.pixX[3 * pix + 1], a.pixX[3 * pix + 2]);
+      ns = mk(a.pixN[3 * pix], a.pixN[3 * pix + 1], a.pixN[3 * pix + 2]);
+    }
     const float A = length(cross(a.LU, a.LV));
     if (a.Eu) a.Eu[pix] = A * lightCenterG(a.Lc, a.LU, a.LV, x, ns);
     if (!lightBeamSetup(a.Lc, a.LU, a.LV, x, ns, T, a.offset, q, poly, lightArea)) {
@@ -969,124 +1101,24 @@ __global__ void softFinalizeKernel(AppParams a, const int32_t* state, int R) {
 
 // ------------------------------------------------------------ primary rays
 
-// Moller-Trumbore (rayHitTri, src/ray/ray_core.h:22-37).
-__device__ __forceinline__ float rayHit(V3 o, V3 d, V3 v0, V3 v1, V3 v2) {
-  V3 e1 = sub(v1, v0), e2 = sub(v2, v0);
-  V3 pv = cross(d, e2);
-  float det = dot(e1, pv);
-  if (det == 0) return kInf;
-  float inv = 1 / det;
-  V3 tv = sub(o, v0);
-  float u = dot(tv, pv) * inv;
-  if (u < 0 || u > 1) return kInf;
-  V3 qv = cross(tv, e1);
-  float v = dot(d, qv) * inv;
-  if (v < 0 || u + v > 1) return kInf;
-  return dot(e2, qv) * inv;
-}
-
-// One ray per pixel centre, nearest hit with coplanar ties to the lower id
-// (primaryKernel + rayTraverse<false>, cuda/gpu_render.cu:222-244,
-// src/ray/ray_core.h:42-132): tri, X, N (normal facing the eye).
+// One eye ray per pixel centre (primaryKernel, cuda/gpu_render.cu:222-244):
+// eyeRay, shared with the fused soft-shadow admission.
 __global__ void __launch_bounds__(128) primaryRaysKernel(SceneDev s, bt_camera cam, int32_t* triOut, float* Xout,
                                                          float* Nout) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= cam.W || y >= cam.H) return;
   const size_t k = size_t(y) * size_t(cam.W) + size_t(x);
-  const float qx = (2 * (float(x) + 0.5f) / float(cam.W) - 1) * cam.half_w;
-  const float qy = (2 * (float(y) + 0.5f) / float(cam.H) - 1) * cam.half_h;
-  const V3 o = mk(cam.eye[0], cam.eye[1], cam.eye[2]);
-  const V3 fwd = mk(cam.fwd[0], cam.fwd[1], cam.fwd[2]), right = mk(cam.right[0], cam.right[1], cam.right[2]),
-           down = mk(cam.down[0], cam.down[1], cam.down[2]);
-  const V3 d = add(add(fwd, mul(right, qx)), mul(down, qy));
-  triOut[k] = -1;
-  Xout[3 * k] = Xout[3 * k + 1] = Xout[3 * k + 2] = 0;
-  Nout[3 * k] = Nout[3 * k + 1] = Nout[3 * k + 2] = 0;
-  float t0 = 0, t1 = kInf;
-  float inv[3];
-  for (int a = 0; a < 3; ++a) {
-    const float da = comp(d, a), oa = comp(o, a);
-    inv[a] = 1 / da;
-    if (da == 0) {
-      if (oa < s.bounds.lo[a] || oa > s.bounds.hi[a]) return;
-      continue;
-    }
-    float ta = (s.bounds.lo[a] - oa) * inv[a];
-    float tb = (s.bounds.hi[a] - oa) * inv[a];
-    if (ta > tb) {
-      float tt = ta;
-      ta = tb;
-      tb = tt;
-    }
-    t0 = t0 > ta ? t0 : ta;
-    t1 = t1 < tb ? t1 : tb;
-  }
-  if (t0 > t1) return;
-  struct Entry {
-    uint32_t node;
-    float t0, t1;
-  };
-  Entry stk[64];
-  int sp = 0;
-  uint32_t node = s.rootNode;
-  float best = kInf;
-  int bestTri = -1;
-  const float tieEps = 4 * 1.1920928955078125e-07f;
-  for (;;) {
-    const uint2 nd = s.node[node];
-    if (!isLeaf(nd)) {
-      const int a = int(nd.y & 3u);
-      const float sp_ = splitOf(nd);
-      const float oa = comp(o, a), da = comp(d, a);
-      const bool belowFirst = oa < sp_ || (oa == sp_ && da <= 0);
-      const uint32_t first = belowFirst ? node + 1 : (nd.y >> 2);
-      const uint32_t second = belowFirst ? (nd.y >> 2) : node + 1;
-      if (da == 0) {
-        node = first;
-        continue;
-      }
-      const float tp = (sp_ - oa) * inv[a];
-      if (tp > t1 || tp <= 0) {
-        node = first;
-      } else if (tp < t0) {
-        node = second;
-      } else {
-        if (sp < 64) stk[sp++] = Entry{second, tp, t1};
-        node = first;
-        t1 = tp;
-      }
-      continue;
-    }
-    const uint32_t cnt = nd.y >> 2;
-    for (uint32_t i = 0; i < cnt; ++i) {
-      const TriRec t = loadRef(s, nd.x + i);
-      const float th = rayHit(o, d, t.v0, t.v1, t.v2);
-      if (!(th > 0 && th < kInf)) continue;
-      const float tol = bestTri < 0 ? 0.f : best * tieEps;
-      if (bestTri < 0 || th < best - tol || (th <= best + tol && t.tri < bestTri)) {
-        best = th;
-        bestTri = t.tri;
-      }
-    }
-    if (bestTri >= 0 && best <= t1) break;
-    if (sp == 0) break;
-    --sp;
-    node = stk[sp].node;
-    t0 = stk[sp].t0;
-    t1 = stk[sp].t1;
-  }
-  if (bestTri < 0) return;
-  triOut[k] = bestTri;
-  const V3 X = add(o, mul(d, best));
-  V3 nT, v0;
-  triNV(s, bestTri, nT, v0);
-  if (dot(nT, d) > 0) nT = neg(nT);
+  V3 X, N;
+  const int t = eyeRay(s, mk(cam.eye[0], cam.eye[1], cam.eye[2]), mk(cam.fwd[0], cam.fwd[1], cam.fwd[2]),
+                       mk(cam.right[0], cam.right[1], cam.right[2]), mk(cam.down[0], cam.down[1], cam.down[2]),
+                       cam.half_w, cam.half_h, cam.W, cam.H, x, y, &X, &N);
+  triOut[k] = t;
   Xout[3 * k] = X.x;
   Xout[3 * k + 1] = X.y;
   Xout[3 * k + 2] = X.z;
-  Nout[3 * k] = nT.x;
-  Nout[3 * k + 1] = nT.y;
-  Nout[3 * k + 2] = nT.z;
+  Nout[3 * k] = N.x;
+  Nout[3 * k + 1] = N.y;
+  Nout[3 * k + 2] = N.z;
 }
 
 // ---------------------------------------------------------------- raster
@@ -1260,6 +1292,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->tail_records = 0;
   c->eps_stats = 0;
   c->yield_pct = 0;
+  c->fuse_primary = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1700,8 +1733,14 @@ bool camOk(const bt_camera* cam) { return cam && cam->W > 0 && cam->H > 0 && cam
 
 int softCore(bt_gpu_ctx* c, const bt_area_light* L, const bt_soft_opts* o, int64_t n, const bt_camera* cam,
              const int32_t* dTri, const float* dX, const float* dN, float* dVis, float* dE, float* dEu,
-             bt_run_info* info) {
+             bt_run_info* info, int32_t* fusedTri = nullptr, float* fusedX = nullptr, float* fusedN = nullptr) {
   AppParams a = baseApp(c, cam);
+  if (fusedTri && cam) {
+    a.fusedPrimary = 1;
+    a.pixTriOut = fusedTri;
+    a.pixXOut = fusedX;
+    a.pixNOut = fusedN;
+  }
   a.Lc = mk(L->c[0], L->c[1], L->c[2]);
   a.LU = mk(L->U[0], L->U[1], L->U[2]);
   a.LV = mk(L->V[0], L->V[1], L->V[2]);
@@ -1850,12 +1889,17 @@ int bt_gpu_soft(bt_gpu_ctx* c, const bt_camera* cam, const bt_area_light* L, con
   if (e) return e;
   if (info) memset(info, 0, sizeof *info);
   CK(cudaEventRecord(c->ev[0], c->stream));
-  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
-  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, c->dPixTri, c->dPixX, c->dPixN);
-  CK(cudaGetLastError());
+  const bool fused = c->cfg.fuse_primary != 0;
+  if (!fused) {
+    dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+    primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, c->dPixTri, c->dPixX, c->dPixN);
+    CK(cudaGetLastError());
+    if (info) info->launches++;
+  }
   CK(cudaEventRecord(c->ev[1], c->stream));
-  if (info) info->launches++;
-  e = softCore(c, L, o, np, cam, c->dPixTri, c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, info);
+  e = fused ? softCore(c, L, o, np, cam, c->dPixTri, c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, info, c->dPixTri,
+                       c->dPixX, c->dPixN)
+            : softCore(c, L, o, np, cam, c->dPixTri, c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, info);
   if (e) return e;
   CK(cudaEventRecord(c->ev[2], c->stream));
   if (tri) CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * np, cudaMemcpyDeviceToHost, c->stream));
@@ -1888,12 +1932,16 @@ int bt_gpu_soft_device(bt_gpu_ctx* c, const bt_camera* cam, const bt_area_light*
   if (e) return e;
   if (info) memset(info, 0, sizeof *info);
   CK(cudaEventRecord(c->ev[0], c->stream));
-  dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
-  primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, dTri, c->dPixX, c->dPixN);
-  CK(cudaGetLastError());
+  const bool fused = c->cfg.fuse_primary != 0;
+  if (!fused) {
+    dim3 bs(16, 8), gs((cam->W + 15) / 16, (cam->H + 7) / 8);
+    primaryRaysKernel<<<gs, bs, 0, c->stream>>>(c->s, *cam, dTri, c->dPixX, c->dPixN);
+    CK(cudaGetLastError());
+    if (info) info->launches++;
+  }
   CK(cudaEventRecord(c->ev[1], c->stream));
-  if (info) info->launches++;
-  e = softCore(c, L, o, np, cam, dTri, c->dPixX, c->dPixN, dVis, dE, dEu, info);
+  e = fused ? softCore(c, L, o, np, cam, dTri, c->dPixX, c->dPixN, dVis, dE, dEu, info, dTri, c->dPixX, c->dPixN)
+            : softCore(c, L, o, np, cam, dTri, c->dPixX, c->dPixN, dVis, dE, dEu, info);
   if (e) return e;
   CK(cudaEventRecord(c->ev[2], c->stream));
   CK(cudaStreamSynchronize(c->stream));

@@ -121,6 +121,8 @@ typedef struct {
   int32_t yield_pct;        /* once a round's trace queue is drained and this percentage of the trace
                                warps has exited, the records still in flight go on in the next round
                                instead of holding the round (results are the same); 0 = 50, < 0 = never */
+  int32_t fuse_primary;     /* nonzero: bt_gpu_soft(_device) trace each pixel's eye ray in the admission of
+                               its shadow root instead of a separate primary-ray pass (same results) */
 } bt_gpu_config;
 
 typedef struct {

@@ -252,3 +252,41 @@ def test_eps_band_logging(gpu):
     assert (band, flips) == (b.info["eps_band_corners"], b.info["eps_fp64_flips"])
     assert band > 0 and 0 <= flips <= band
     assert a.info["tri_tests"] == plain.info["tri_tests"]
+
+
+@pytest.mark.parametrize("name,kw,budget", [("plant", {}, 128), ("plant", {}, 4),
+                                            ("building", dict(floors=1, furniture=3), 128)])
+def test_fused_primary_rays_same_as_separate(name, kw, budget, gpu):
+    """fuse_primary: each shadow root's admission traces its pixel's eye ray
+    instead of a separate primary-ray pass.  Bitwise the same tri, vis, E and
+    Eu, exact and not (the non-exact E reads the fused X and N), also when
+    roots over a tiny budget are re-admitted and retried; and through the
+    device-buffer entry point."""
+    import torch
+    from beamtrace2007_b200.renderer import make_camera
+    s, ps = scene(name, **kw)
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 160, 120)
+    L = s.light_array(2.0)
+    with _renderer(ps, budget=budget) as g:
+        sep = [g.soft_shadows(cam, L, exact=e) for e in (True, False)]
+    with _renderer(ps, budget=budget, fuse_primary=True) as g:
+        fus = [g.soft_shadows(cam, L, exact=e) for e in (True, False)]
+        # the device-buffer entry point, fused
+        import ctypes as C
+        from beamtrace2007_b200 import _native as N
+        n = cam.W * cam.H
+        out = [torch.full((n,), 7, dtype=t, device="cuda:0") for t in (torch.int32, torch.float32, torch.float32,
+                                                                         torch.float32)]
+        torch.cuda.synchronize()
+        N.check(N.lib().bt_gpu_soft_device(g._h, C.byref(cam), C.byref(N.AreaLight.from_array(L)),
+                                           C.byref(N.SoftOpts(1, 0.0)), *(o.data_ptr() for o in out), None))
+        dev = [o.cpu().numpy() for o in out]
+    assert (sep[0].tri >= 0).mean() > 0.2
+    for a, b in zip(sep, fus):
+        for f in ("tri", "vis", "E", "Eu"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    for x, f in zip(dev, ("tri", "vis", "E", "Eu")):
+        assert np.array_equal(x, getattr(sep[0], f)), f
+    if budget < 16:
+        assert fus[0].info["retried_roots"] > 0
