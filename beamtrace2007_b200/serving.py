@@ -4,13 +4,15 @@ memory budget, p50/p99 latency (no counterpart in the reference).
 Requests -- primary visibility (per-pixel hit-triangle ids), point shadows
 (per-pixel shadow mask) or exact area-light soft shadows, each for a camera
 and resolution on one resident scene -- arrive at any time through
-`Server.submit`.  Every resident scene keeps its kd-tree and its engine
-context on the GPU for the server's lifetime; each context has its own CUDA
-stream and worker thread, so different scenes' requests run on the device
-at the same time.  A worker takes everything admitted for its scene at once:
-the soft-shadow requests go into one batched engine run (bt_gpu_batch_soft,
-whose roots share the rounds), the others run one after the other.  A
-request that arrives while its scene's worker is busy joins the next run.
+`Server.submit`.  Every resident scene keeps its kd-tree and
+`workers_per_scene` engine contexts on the GPU for the server's lifetime;
+each context has its own CUDA stream and worker thread, so requests of
+different scenes, and of one scene, run on the device at the same time.  A
+free worker takes its scene's oldest admitted request: if that is a soft-
+shadow request, together with every other soft-shadow request waiting for
+the scene, in one batched engine run (bt_gpu_batch_soft, whose roots share
+the rounds); otherwise that request alone.  So a short primary request does
+not wait behind a long soft-shadow batch while another worker is free.
 
 Admission: the resident scenes and their sub-beam queues are charged to the
 budget at start; a request is admitted, in arrival order, when its own
@@ -81,13 +83,27 @@ def primary_tile(r: Request) -> int:
 
 
 class _SceneSlot:
-    def __init__(self, name, scene_data, engine):
+    def __init__(self, name, scene_data, engines):
         self.name = name
         self.data = scene_data
-        self.engine = engine
+        self.engines = engines
         self.pending: collections.deque[Request] = collections.deque()
         self.cv = threading.Condition()
-        self.thread: threading.Thread | None = None
+        self.threads: list[threading.Thread] = []
+
+    @property
+    def engine(self):
+        return self.engines[0]
+
+    def take(self) -> list:
+        """The oldest pending request, with every other pending soft-shadow
+        request when it is one (called with cv held)."""
+        head = self.pending.popleft()
+        if head.kind != "soft":
+            return [head]
+        batch = [head] + [r for r in self.pending if r.kind == "soft"]
+        self.pending = collections.deque(r for r in self.pending if r.kind != "soft")
+        return batch
 
 
 class Server:
@@ -95,7 +111,7 @@ class Server:
     builds a context (GpuRenderer by default; tests may pass a stand-in)."""
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 21,
-                 engine_factory=None, cache=None, kd_on_gpu: bool = True):
+                 engine_factory=None, cache=None, kd_on_gpu: bool = True, workers_per_scene: int = 2):
         from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
         kd_device = device if kd_on_gpu else None
@@ -115,9 +131,10 @@ class Server:
             else:
                 ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris, kd_device=kd_device)
             self.prep_ms[name] = (time.perf_counter() - t0) * 1e3
-            self.resident += 44 * len(ps.kd_split) + 64 * len(ps.kd_tri_indices) + 32 * ps.num_tris
-            self.resident += 3 * 64 * queue_records
-            slot = _SceneSlot(name, sd, engine_factory(ps, queue_records))
+            # each context holds the scene, its tree and its queues
+            per = 44 * len(ps.kd_split) + 64 * len(ps.kd_tri_indices) + 32 * ps.num_tris + 3 * 64 * queue_records
+            self.resident += per * workers_per_scene
+            slot = _SceneSlot(name, sd, [engine_factory(ps, queue_records) for _ in range(workers_per_scene)])
             self.slots[name] = slot
         if self.resident > self.budget:
             raise ValueError(f"resident scenes and queues need {self.resident / 2**30:.2f} GiB, "
@@ -128,8 +145,10 @@ class Server:
         self.waiting: collections.deque[Request] = collections.deque()
         self.running = True
         for slot in self.slots.values():
-            slot.thread = threading.Thread(target=self._worker, args=(slot,), daemon=True)
-            slot.thread.start()
+            for eng in slot.engines:
+                t = threading.Thread(target=self._worker, args=(slot, eng), daemon=True)
+                slot.threads.append(t)
+                t.start()
 
     def tune(self, sizes=(256, 512, 1024), tiles=(8, 16, 32)):
         """Autotunes the primary tile of every resident scene at each square
@@ -178,17 +197,16 @@ class Server:
             self._admit()
 
     # ---- execution ----
-    def _worker(self, slot: _SceneSlot):
+    def _worker(self, slot: _SceneSlot, engine):
         while True:
             with slot.cv:
                 while self.running and not slot.pending:
                     slot.cv.wait(0.05)
                 if not self.running and not slot.pending:
                     return
-                batch = list(slot.pending)
-                slot.pending.clear()
+                batch = slot.take()
             try:
-                self._run(slot, batch)
+                self._run(slot, engine, batch)
             except Exception as e:  # a failed run fails its requests, not the server
                 for r in batch:
                     if r.result is None:
@@ -205,15 +223,15 @@ class Server:
         v = slot.data.views[r.view]
         return make_camera(v.eye, v.target, v.fov, slot.data.up, r.W, r.H)
 
-    def _run(self, slot: _SceneSlot, batch):
+    def _run(self, slot: _SceneSlot, engine, batch):
         soft = [r for r in batch if r.kind == "soft"]
         if soft:
             cams = [self._camera(slot, r) for r in soft]
             lights = [slot.data.light_array(r.light_scale) for r in soft]
-            res = slot.engine.batch_soft(cams, lights, exact=soft[0].exact) if all(
+            res = engine.batch_soft(cams, lights, exact=soft[0].exact) if all(
                 r.exact == soft[0].exact for r in soft) else None
             if res is None:
-                res = [slot.engine.soft_shadows(c, L, exact=r.exact) for c, L, r in zip(cams, lights, soft)]
+                res = [engine.soft_shadows(c, L, exact=r.exact) for c, L, r in zip(cams, lights, soft)]
             now = time.perf_counter()
             for r, x in zip(soft, res):
                 r.result = x
@@ -224,9 +242,9 @@ class Server:
             cam = self._camera(slot, r)
             tile = r.tile = self.tiles.get((r.scene, r.W, r.H)) or primary_tile(r)
             if r.kind == "primary":
-                r.result = slot.engine.primary_ids(cam, tile=tile)
+                r.result = engine.primary_ids(cam, tile=tile)
             else:
-                r.result = slot.engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=tile)[1]
+                r.result = engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=tile)[1]
             r.done = time.perf_counter()
 
     def close(self):
@@ -234,11 +252,12 @@ class Server:
         for slot in self.slots.values():
             with slot.cv:
                 slot.cv.notify_all()
-            if slot.thread:
-                slot.thread.join(timeout=60)
-            close = getattr(slot.engine, "close", None)
-            if close:
-                close()
+            for t in slot.threads:
+                t.join(timeout=60)
+            for eng in slot.engines:
+                close = getattr(eng, "close", None)
+                if close:
+                    close()
 
     def __enter__(self):
         return self

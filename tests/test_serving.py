@@ -84,6 +84,34 @@ def test_admission_and_batching(native_lib):
             assert r.result.vis[0] == np.float32(r.result.vis[0])
 
 
+class SlowSoftEngine(FakeEngine):
+    """A stand-in whose soft-shadow batches take 0.3 s."""
+
+    def batch_soft(self, cams, lights, exact=True):
+        time.sleep(0.3)
+        return super().batch_soft(cams, lights, exact)
+
+
+@pytest.mark.parametrize("workers", [1, 2])
+def test_primary_does_not_wait_behind_a_soft_batch(native_lib, workers):
+    """With two workers per scene, a primary request that arrives while a
+    long soft-shadow batch runs on the same scene is served by the other
+    worker; with one it waits for the batch."""
+    from beamtrace2007_b200.serving import Request, Server
+    s, _ = scene("room")
+    with Server({"a": s}, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=SlowSoftEngine,
+                kd_on_gpu=False, workers_per_scene=workers) as srv:
+        soft = srv.submit(Request("soft", "a", 64, 64))
+        time.sleep(0.05)
+        prim = srv.submit(Request("primary", "a", 64, 64))
+        assert soft.event.wait(30) and prim.event.wait(30)
+    assert soft.error is None and prim.error is None
+    if workers == 2:
+        assert prim.done < soft.done and prim.latency < 0.2
+    else:
+        assert prim.done >= soft.done
+
+
 def test_config_scenes_through_the_cache(native_lib, tmp_path):
     """Scenes given as the reference's configs are ingested and prepared
     once; a second server on the same cache directory admits them from the
