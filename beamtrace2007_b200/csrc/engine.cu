@@ -808,9 +808,11 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // lanes are refilled at once (one atomic per warp, ballot/popc ranks).
 // Records needing a clip are compacted into the clip queue.
 // (At least 3 CTAs per SM: lets the compiler keep the lane's state in up to
-// 170 registers; at 4 CTAs it spills, which costs more than the warps gain.)
+// 170 registers; at 4 CTAs it spills, which costs more than the warps gain.
+// The tail-round variant clips inline with its polygons in registers and
+// takes 2 CTAs per SM: tail rounds hold too few records to need more warps.)
 template <int App, bool Fused, bool EpsLog = false>
-__global__ void __launch_bounds__(kThreads, 3) traceKernel(const __grid_constant__ RoundParams p) {
+__global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
   const int nCur = min(p.ctr->count[p.cur], p.capacity);
