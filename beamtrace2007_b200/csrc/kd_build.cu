@@ -24,7 +24,9 @@
 // The order of a node's references does not enter any decision (counts,
 // sorted events, per-reference clipping), so the partition writes them in
 // any order.  Positions are compared as floats, so -0 and +0 are one event
-// position (the split plane then stores +0).
+// position; the split plane takes the zero sign of its group's first event
+// (+0 sorts before -0 among events of one type), which is the host build's
+// value whenever a position's events have one sign.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -73,6 +75,12 @@ __device__ __forceinline__ uint32_t orderedBits(float f) {
 }
 __device__ __forceinline__ float fromOrdered(uint32_t k) {
   return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+// Sweep event key: position, then type, then 1 for -0.
+__device__ __forceinline__ unsigned long long eventKey(float pos, int type) {
+  const bool negZero = pos == 0.f && (__float_as_uint(pos) >> 31);
+  return (static_cast<unsigned long long>(orderedBits(pos)) << 3) | (unsigned long long)(type << 1) |
+         (negZero ? 1ull : 0ull);
 }
 
 __global__ void initRefs(const float* __restrict__ pos, const uint32_t* __restrict__ tris, int64_t n, Ref* refs) {
@@ -185,12 +193,13 @@ __global__ void __launch_bounds__(kThreads) sweepSelect(const Ref* __restrict__ 
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
       const Ref rf = refs[s0 + i];
       const float a = comp(rf.lo, axis), e = comp(rf.hi, axis);
+      // key: position (ordered bits), type (end 0, planar 1, start 2), -0 marker
       if (a == e) {
-        keys[atomicAdd(&nev, 1)] = (static_cast<unsigned long long>(orderedBits(a)) << 2) | 1ull;
+        keys[atomicAdd(&nev, 1)] = eventKey(a, 1);
       } else {
         const int at = atomicAdd(&nev, 2);
-        keys[at] = (static_cast<unsigned long long>(orderedBits(a)) << 2) | 2ull;
-        keys[at + 1] = static_cast<unsigned long long>(orderedBits(e)) << 2;
+        keys[at] = eventKey(a, 2);
+        keys[at + 1] = eventKey(e, 0);
       }
     }
     __syncthreads();
@@ -203,12 +212,12 @@ __global__ void __launch_bounds__(kThreads) sweepSelect(const Ref* __restrict__ 
     if (threadIdx.x == 0) {
       uint64_t nl = 0, nr = N;
       for (int i = 0; i < n;) {
-        const uint32_t pk = uint32_t(keys[i] >> 2);
-        const float p = fromOrdered(pk);
+        const uint32_t pk = uint32_t(keys[i] >> 3);
+        const float p = (keys[i] & 1) ? -0.f : fromOrdered(pk);
         uint64_t pe = 0, pp = 0, ps = 0;
-        while (i < n && uint32_t(keys[i] >> 2) == pk && (keys[i] & 3) == 0) ++pe, ++i;
-        while (i < n && uint32_t(keys[i] >> 2) == pk && (keys[i] & 3) == 1) ++pp, ++i;
-        while (i < n && uint32_t(keys[i] >> 2) == pk && (keys[i] & 3) == 2) ++ps, ++i;
+        while (i < n && uint32_t(keys[i] >> 3) == pk && ((keys[i] >> 1) & 3) == 0) ++pe, ++i;
+        while (i < n && uint32_t(keys[i] >> 3) == pk && ((keys[i] >> 1) & 3) == 1) ++pp, ++i;
+        while (i < n && uint32_t(keys[i] >> 3) == pk && ((keys[i] >> 1) & 3) == 2) ++ps, ++i;
         nr -= pe + pp;
         if (p > lo && p < hi) {
           const float c = kdr::sahCost(k, b, axis, p, nl + pp, nr + pp);

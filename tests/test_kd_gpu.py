@@ -79,3 +79,34 @@ def test_gpu_tree_full_building(gpu):
     dev = PreparedScene(s.pos, s.tris, kd_device=0)
     _same_tree(dev, host)
     print(f"building kd build: host {host.kd_build_ms:.0f} ms, GPU {dev.kd_build_ms:.0f} ms")
+
+
+def _grid_tris(n, z=0.0, jitter=0.0, seed=0):
+    """n x n quads (2n^2 triangles) on the plane z (x, y in [-1, 1])."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(-1, 1, n + 1)
+    pos = np.array([[x, y, z + jitter * rng.uniform(-1, 1)] for y in xs for x in xs], np.float32)
+    tris = []
+    for j in range(n):
+        for i in range(n):
+            a = j * (n + 1) + i
+            tris += [[a, a + 1, a + n + 2], [a, a + n + 2, a + n + 1]]
+    return pos, np.array(tris, np.uint32)
+
+
+@pytest.mark.gpu
+def test_gpu_tree_edge_cases(gpu):
+    """Degenerate inputs: one triangle, two, a flat grid (planar events and a
+    zero-extent axis), one triangle repeated (identical events), and a grid
+    across zero (positions of both zero signs)."""
+    from beamtrace2007_b200.renderer import PreparedScene
+    one = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.uint32))
+    two = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32), np.array([[0, 1, 2], [0, 1, 3]],
+                                                                                          np.uint32))
+    flat = _grid_tris(40)
+    rep_pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    rep = (rep_pos, np.tile(np.array([[0, 1, 2]], np.uint32), (300, 1)))
+    signed = _grid_tris(30, z=0.0, jitter=0.25, seed=4)
+    signed[0][np.abs(signed[0]) < 1e-9] = -0.0
+    for pos, tris in (one, two, flat, rep, signed):
+        _same_tree(PreparedScene(pos, tris, kd_device=0), PreparedScene(pos, tris))
