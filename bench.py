@@ -458,7 +458,7 @@ def main():
                                                "rounds", "passes", "retried_roots", "max_spill")},
             "ms_primary": float(np.mean([d["ms_primary"] for d in infos])),
             "ms_trace": float(np.mean([d["ms_trace"] for d in infos]))}
-    if not args.no_extras:
+    if not args.no_extras and ws == 1:  # (at N > 1 the other GPUs would wait on rank 0's extras)
         line["batched"] = batched_measure(g, s, N, lib, C, steps=3)
         # the batched-jobs workload at bounded size (the full 64 jobs of up to
         # 200K triangles at up to 512^2 take minutes per batch)
