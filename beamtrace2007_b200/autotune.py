@@ -32,7 +32,7 @@ def _best(timings: dict):
     return min(timings, key=timings.get)
 
 
-def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, -1),
+def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, 30000, -1),
                 capacities=(0,), yield_pcts=(0,), reps: int = 2, device: int = 0):
     """Times `reps` soft-shadow frames (after one warm-up) for every
     combination of the candidate settings; returns (best settings as
