@@ -21,6 +21,13 @@ def test_exports_every_declared_symbol(native_lib):
     assert not missing, missing
 
 
+def test_every_declared_symbol_has_a_ctypes_signature(native_lib):
+    """The Python binding (_native.SIGNATURES) covers the whole header."""
+    from beamtrace2007_b200 import _native as N
+    missing = [n for n in _declared() if n not in N.SIGNATURES]
+    assert not missing, missing
+
+
 def test_no_device_is_an_error_not_an_abort(native_lib):
     """Without a GPU (this container) every device call returns a status."""
     from beamtrace2007_b200 import _native as N
