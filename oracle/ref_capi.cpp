@@ -526,3 +526,36 @@ BTR_API void btr_config_arrays(void* h, double* pos, uint32_t* tris, uint16_t* m
   put(lights + 16, c.background);
   lights[19] = lights[20] = lights[21] = 0;
 }
+
+// The reference's own fuzzy split and clean-up (beam_geom.h:83-150) of one
+// polygon by one line, for the polygon fuzz test; corners as doubles of the
+// build's Real.  Returns 0 if its splitter reported an overflow.
+BTR_API int btr_split_clean(const double* px, const double* py, int n, const double* line, double eps, double* inx,
+                            double* iny, int* nin, double* outx, double* outy, int* nout) {
+  PolyN<kMaxPoly> p, in, out;
+  for (int i = 0; i < n && i < kMaxPoly; ++i) p.push(Real(px[i]), Real(py[i]));
+  Line2 L;
+  L.a = Real(line[0]);
+  L.b = Real(line[1]);
+  L.c = Real(line[2]);
+  if (!splitPoly(p, L, Real(eps), in, out)) return 0;
+  cleanPoly(in, Real(eps));
+  cleanPoly(out, Real(eps));
+  *nin = in.n;
+  *nout = out.n;
+  for (int i = 0; i < in.n; ++i) {
+    inx[i] = double(in.x[i]);
+    iny[i] = double(in.y[i]);
+  }
+  for (int i = 0; i < out.n; ++i) {
+    outx[i] = double(out.x[i]);
+    outy[i] = double(out.y[i]);
+  }
+  return 1;
+}
+
+BTR_API double btr_poly_area(const double* px, const double* py, int n) {
+  PolyN<kMaxPoly> p;
+  for (int i = 0; i < n && i < kMaxPoly; ++i) p.push(Real(px[i]), Real(py[i]));
+  return double(p.area());
+}

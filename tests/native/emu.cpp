@@ -440,3 +440,43 @@ EMU_API int emu_soft_rounds(void* h, const float* light, float offset, int64_t n
   *chain = longest;
   return round;
 }
+
+// One fuzzy split of a polygon (n <= 4 corners) by a line, then the
+// clean-up of both pieces, with this package's polygon code (splitPoly,
+// cleanPoly of beam_math.cuh): the pieces' corners and counts, and 0 if
+// the splitter reported an overflow.  For the polygon fuzz test.
+EMU_API int emu_split_clean(const float* px, const float* py, int n, const float* line, float eps, float* inx,
+                            float* iny, int* nin, float* outx, float* outy, int* nout) {
+  Poly<kPolyMax> p, in, out;
+  p.n = n;
+  for (int i = 0; i < n && i < kPolyMax; ++i) {
+    p.x[i] = px[i];
+    p.y[i] = py[i];
+  }
+  Line L{line[0], line[1], line[2]};
+  if (!splitPoly(p, L, eps, in, out)) return 0;
+  cleanPoly(in, eps);
+  cleanPoly(out, eps);
+  *nin = in.n;
+  *nout = out.n;
+  for (int i = 0; i < in.n; ++i) {
+    inx[i] = in.x[i];
+    iny[i] = in.y[i];
+  }
+  for (int i = 0; i < out.n; ++i) {
+    outx[i] = out.x[i];
+    outy[i] = out.y[i];
+  }
+  return 1;
+}
+
+// Signed area of a polygon with this package's Poly::area.
+EMU_API float emu_poly_area(const float* px, const float* py, int n) {
+  Poly<kPolyMax> p;
+  p.n = n;
+  for (int i = 0; i < n && i < kPolyMax; ++i) {
+    p.x[i] = px[i];
+    p.y[i] = py[i];
+  }
+  return p.area();
+}
