@@ -92,6 +92,11 @@ REF_SCENES = {
                 "area_light 4 2.95 4  1 0 0  0 0 1\n",
     "ref_plant": "mesh procedural plant\nup 0 1 0\nview 2.6 1.7 3.4  0 0.55 0  45\npoint_light 1.0 3.0 0.8\n"
                  "area_light 0.9 2.8 0.7  0.4 0 0  0 0 0.4\n",
+    # a closed sphere over a floor (the reference's crack-test scene) and its tessellation sweep
+    "ref_sphere": "mesh procedural sphere stacks=16\nmesh procedural floorquad y=-1.2 size=8\nup 0 1 0\n"
+                  "view 0.3 0.8 3.2  0 0 0  45\npoint_light 1.5 3.0 1.0\narea_light 1.2 3.0 0.8  0.6 0 0  0 0 0.6\n",
+    "ref_tess_sweep": "mesh procedural tess_sweep stacks=8\nup 0 1 0\nview 0 5 9  0 0 0  55\n"
+                      "point_light 2 6 2\narea_light 1 6 1  1 0 0  0 0 1\n",
 }
 
 
