@@ -480,3 +480,56 @@ EMU_API float emu_poly_area(const float* px, const float* py, int n) {
   }
   return p.area();
 }
+
+// The kd slab decision (decide, beam_math.cuh) for one beam -- apex O, plane
+// through p0 spanned by u and v, corners (qx, qy) -- against a box and a
+// split plane on `axis`: kNear 0, kFar 1, kBoth 2; -1 if the corner rays
+// mix direction signs on an axis (not a pre-split piece), -2 if the split
+// lies behind the apex.  Returns the plane's u, v, d (the ray at (x, y) is
+// O + t (d + x u + y v)) as the decision used them.  For the kd fuzz test.
+EMU_API int emu_decide(const float* O, const float* p0, const float* u, const float* v, const float* qx,
+                       const float* qy, int n, int axis, float split, const float* box6, float* uvd) {
+  Query q;
+  memset(&q, 0, sizeof q);
+  q.P = makePlane(mk(O[0], O[1], O[2]), mk(p0[0], p0[1], p0[2]), mk(u[0], u[1], u[2]), mk(v[0], v[1], v[2]));
+  q.mode = kModeAnyHit;
+  q.exclude = -1;
+  querySetup(q, 1.f);
+  const V3 vv[3] = {q.P.u, q.P.v, q.P.d};
+  for (int k = 0; k < 3; ++k) {
+    uvd[3 * k] = vv[k].x;
+    uvd[3 * k + 1] = vv[k].y;
+    uvd[3 * k + 2] = vv[k].z;
+  }
+  Beam b;
+  memset(&b, 0, sizeof b);
+  for (int i = 0; i < 4; ++i) {
+    const int j = i < n ? i : n - 1;
+    b.qx[i] = qx[j];
+    b.qy[i] = qy[j];
+  }
+  b.n = n;
+  int neg = 0;
+  for (int c = 0; c < 3; ++c) {
+    int pos = 0, negs = 0;
+    for (int i = 0; i < n; ++i) {
+      const float w = qx[i] * comp(q.P.u, c) + qy[i] * comp(q.P.v, c) + comp(q.P.d, c);
+      pos += w > 0;
+      negs += w < 0;
+    }
+    if (pos && negs) return -1;
+    if (negs) neg |= 1 << c;
+  }
+  b.neg = neg;
+  beamAxes(q, b);
+  setStatus(q, b, -1, nullptr, 0);
+  Box box;
+  for (int c = 0; c < 3; ++c) {
+    box.lo[c] = box6[c];
+    box.hi[c] = box6[3 + c];
+  }
+  const bool posA = !((neg >> axis) & 1);
+  const float Ns = (posA ? 1.f : -1.f) * (split - comp(q.P.O, axis));
+  if (!(Ns > 0)) return -2;
+  return decide(q, b, axis, Ns, box);
+}
