@@ -97,6 +97,12 @@ REF_SCENES = {
                   "view 0.3 0.8 3.2  0 0 0  45\npoint_light 1.5 3.0 1.0\narea_light 1.2 3.0 0.8  0.6 0 0  0 0 0.6\n",
     "ref_tess_sweep": "mesh procedural tess_sweep stacks=8\nup 0 1 0\nview 0 5 9  0 0 0  55\n"
                       "point_light 2 6 2\narea_light 1 6 1  1 0 0  0 0 1\n",
+    # its closed-form soft-shadow scene and a one-floor cut of its office building
+    "ref_analytic": "mesh procedural analytic h=1 occ=1\nup 0 1 0\nview 0 5 5  0 0 0  60\n"
+                    "point_light 0.3 3 0.2\narea_light 0 3 0  1 0 0  0 0 1\n",
+    "ref_building": "mesh procedural building floors=1 rooms=2 detail=6\nup 0 1 0\n"
+                    "view 1.0 1.6 2.4  6 1.2 2.6  70\npoint_light 2.5 2.6 2.5\n"
+                    "area_light 2.5 2.75 2.5  0.8 0 0  0 0 0.8\n",
 }
 
 
