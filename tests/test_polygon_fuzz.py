@@ -5,9 +5,10 @@ tests/native/emu.cpp), against the reference's own splitPoly/cleanPoly
 triangles and quads over six orders of magnitude, with lines through
 vertices, inside and just outside the fuzzy band, and anywhere: bitwise the
 same pieces.  And the reference's own invariants of the split
-(tests/test_geometry.cpp:54-110): the pieces' areas add up to the polygon's,
-and splitting by L and by -L gives the same two pieces the other way round,
-bit for bit (neighbouring beams agree on their shared edge)."""
+(tests/test_geometry.cpp:54-110): the pieces stay convex, their areas add
+up to the polygon's, and splitting by L and by -L gives the same two pieces
+the other way round, bit for bit (neighbouring beams agree on their shared
+edge)."""
 import ctypes as C
 
 import numpy as np
@@ -97,6 +98,15 @@ def test_split_invariants():
         assert okn == 1
         # L and -L: the same pieces, exchanged
         assert _same(pin, nout) and _same(pout, nin)
+        # the pieces stay convex: no turn against the polygon's orientation
+        # beyond rounding (cleanPoly has welded near-collinear corners)
+        for x, y in (pin, pout):
+            if len(x) >= 3:
+                xd, yd = np.asarray(x, np.float64), np.asarray(y, np.float64)
+                ex, ey = np.roll(xd, -1) - xd, np.roll(yd, -1) - yd
+                turn = ex * np.roll(ey, -1) - ey * np.roll(ex, -1)
+                scale = float(np.max(np.hypot(ex, ey))) ** 2
+                assert np.all(turn >= -1e-5 * scale), turn
         # the areas add up (the pieces share the crossing points)
         A = float(emu.emu_poly_area(f(px), f(py), len(px)))
         parts = sum(float(emu.emu_poly_area(f(x), f(y), len(x))) for x, y in (pin, pout) if len(x) >= 3)
