@@ -246,38 +246,38 @@ BT_CLIP bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, 
   in.clear();
   out.clear();
   float d[N];
-  int cls[N];
-  int nin = 0, nout = 0;
+  int side[N];
+  int keptIn = 0, keptOut = 0;
   BT_UNROLL for (int i = 0; i < N; ++i) {
     d[i] = 0.f;
-    cls[i] = 0;
+    side[i] = 0;
     if (i < p.n) {
       d[i] = L.eval(p.x[i], p.y[i]);
-      cls[i] = d[i] > eps ? 1 : (d[i] < -eps ? -1 : 0);
+      side[i] = d[i] > eps ? 1 : (d[i] < -eps ? -1 : 0);
     }
   }
   BT_UNROLL for (int i = 0; i < N; ++i) {
     if (i < p.n) {
-      const int cj = i + 1 == p.n ? cls[0] : cls[i + 1 < N ? i + 1 : 0];
-      nin += (cls[i] >= 0) + (cls[i] * cj < 0);
-      nout += (cls[i] <= 0) + (cls[i] * cj < 0);
+      const int sideNext = i + 1 == p.n ? side[0] : side[i + 1 < N ? i + 1 : 0];
+      keptIn += (side[i] >= 0) + (side[i] * sideNext < 0);
+      keptOut += (side[i] <= 0) + (side[i] * sideNext < 0);
     }
   }
-  if (nin > N || nout > N) return false;
+  if (keptIn > N || keptOut > N) return false;
   BT_UNROLL for (int i = 0; i < N; ++i) {
     if (i < p.n) {
       const bool wrap = i + 1 == p.n;
-      const int jn = i + 1 < N ? i + 1 : 0;
-      const int cj = wrap ? cls[0] : cls[jn];
-      const float dj = wrap ? d[0] : d[jn];
-      const float xj = wrap ? p.x[0] : p.x[jn], yj = wrap ? p.y[0] : p.y[jn];
-      if (cls[i] >= 0) in.push(p.x[i], p.y[i]);
-      if (cls[i] <= 0) out.push(p.x[i], p.y[i]);
-      if (cls[i] * cj < 0) {
-        const bool iFirst = p.x[i] < xj || (p.x[i] == xj && p.y[i] < yj);
-        const float da = iFirst ? d[i] : dj, db = iFirst ? dj : d[i];
-        const float xa = iFirst ? p.x[i] : xj, xb = iFirst ? xj : p.x[i];
-        const float ya = iFirst ? p.y[i] : yj, yb = iFirst ? yj : p.y[i];
+      const int next = i + 1 < N ? i + 1 : 0;
+      const int sideNext = wrap ? side[0] : side[next];
+      const float dNext = wrap ? d[0] : d[next];
+      const float xj = wrap ? p.x[0] : p.x[next], yj = wrap ? p.y[0] : p.y[next];
+      if (side[i] >= 0) in.push(p.x[i], p.y[i]);
+      if (side[i] <= 0) out.push(p.x[i], p.y[i]);
+      if (side[i] * sideNext < 0) {
+        const bool fromHere = p.x[i] < xj || (p.x[i] == xj && p.y[i] < yj);
+        const float da = fromHere ? d[i] : dNext, db = fromHere ? dNext : d[i];
+        const float xa = fromHere ? p.x[i] : xj, xb = fromHere ? xj : p.x[i];
+        const float ya = fromHere ? p.y[i] : yj, yb = fromHere ? yj : p.y[i];
         float t = da / (da - db);
         float X = xa + t * (xb - xa);
         float Y = ya + t * (yb - ya);
@@ -304,10 +304,10 @@ BT_CLIP void cleanPoly(Poly<N>& p, float epsSplit) {
       float ex = xj - xh, ey = yj - yh;
       float dx = xi - xh, dy = yi - yh;
       float len = sqrtf(ex * ex + ey * ey);
-      float dist2 = dx * dx + dy * dy;
-      float cr = fabs_(ex * dy - ey * dx);
-      bool dup = dist2 <= eps * eps;
-      bool collinear = cr <= eps * len;
+      float gapSq = dx * dx + dy * dy;
+      float offLine = fabs_(ex * dy - ey * dx);
+      bool dup = gapSq <= eps * eps;
+      bool collinear = offLine <= eps * len;
       if (dup || collinear) {
         // drop vertex i: the later ones move down one slot
         BT_UNROLL for (int k = 0; k + 1 < N; ++k) {

@@ -103,81 +103,85 @@ struct KdBuild {
     return kdr::sahCost(kdr::Costs{costTraverse, costIntersect, emptyBonus}, toBox(box), axis, s, nl, nr);
   }
 
-  // Binned SAH above binThreshold references, exact event sweep below
-  // (kdtree.cpp:215-285).
+  // The cheapest split plane of `box` for `refs` (SAH, kd_rules.h): per
+  // axis with extent, binned candidates above binThreshold references, else
+  // every face of the references' extents (kdtree.cpp:215-285 makes the same
+  // choices; a candidate replaces the best only when strictly cheaper, so
+  // among equal costs the first in axis order, then plane order, stays).
   void findSplit(const std::vector<TriBox>& refs, const Aabb& box, int& bestAxis, float& bestSplit,
                  float& bestCost) const {
-    const size_t N = refs.size();
     if (!(box.surfaceArea() > 0)) return;
-    for (int axis = 0; axis < 3; ++axis) {
-      float lo = box.lo[axis], hi = box.hi[axis];
-      if (!(hi > lo)) continue;
-      if (N > size_t(binThreshold)) {
-        const int B = bins;
-        std::vector<size_t> starts(size_t(B), 0), ends(size_t(B), 0);
-        float scale = float(B) / (hi - lo);
-        for (const TriBox& r : refs) {
-          starts[size_t(kdr::binOf(r.b.lo[axis], lo, scale, B))]++;
-          ends[size_t(kdr::binOf(r.b.hi[axis], lo, scale, B))]++;
-        }
-        size_t nl = 0, nr = N;
-        for (int k = 1; k < B; ++k) {
-          nl += starts[size_t(k - 1)];
-          nr -= ends[size_t(k - 1)];
-          float s = kdr::binPlane(lo, hi, k, B);
-          float c = sahCost(box, axis, s, nl, nr);
-          if (c < bestCost) {
-            bestCost = c;
-            bestAxis = axis;
-            bestSplit = s;
-          }
-        }
-      } else {
-        struct Ev {
-          float pos;
-          int type;  // 0 end, 1 planar, 2 start
-        };
-        std::vector<Ev> ev;
-        ev.reserve(2 * N);
-        for (const TriBox& r : refs) {
-          float a = r.b.lo[axis], b = r.b.hi[axis];
-          if (a == b) {
-            ev.push_back({a, 1});
-          } else {
-            ev.push_back({a, 2});
-            ev.push_back({b, 0});
-          }
-        }
-        std::sort(ev.begin(), ev.end(),
-                  [](const Ev& x, const Ev& y) { return x.pos != y.pos ? x.pos < y.pos : x.type < y.type; });
-        size_t nl = 0, nr = N;
-        for (size_t i = 0; i < ev.size();) {
-          float p = ev[i].pos;
-          size_t pe = 0, pp = 0, ps = 0;
-          while (i < ev.size() && ev[i].pos == p && ev[i].type == 0) {
-            ++pe;
-            ++i;
-          }
-          while (i < ev.size() && ev[i].pos == p && ev[i].type == 1) {
-            ++pp;
-            ++i;
-          }
-          while (i < ev.size() && ev[i].pos == p && ev[i].type == 2) {
-            ++ps;
-            ++i;
-          }
-          nr -= pe + pp;
-          if (p > lo && p < hi) {
-            float c = sahCost(box, axis, p, nl + pp, nr + pp);
-            if (c < bestCost) {
-              bestCost = c;
-              bestAxis = axis;
-              bestSplit = p;
-            }
-          }
-          nl += ps + pp;
-        }
+    auto offer = [&](int axis, float plane, size_t below, size_t above) {
+      const float c = sahCost(box, axis, plane, below, above);
+      if (c < bestCost) {
+        bestCost = c;
+        bestAxis = axis;
+        bestSplit = plane;
       }
+    };
+    for (int axis = 0; axis < 3; ++axis) {
+      if (!(box.hi[axis] > box.lo[axis])) continue;
+      if (refs.size() > size_t(binThreshold))
+        offerBinned(refs, box, axis, offer);
+      else
+        offerFaces(refs, box, axis, offer);
+    }
+  }
+
+  // Planes between `bins` equal bins: a reference counts below a plane once
+  // the bin of its low end lies below it, above while the bin of its high
+  // end does not.
+  template <class Offer>
+  void offerBinned(const std::vector<TriBox>& refs, const Aabb& box, int axis, Offer& offer) const {
+    const float lo = box.lo[axis], hi = box.hi[axis];
+    const float perUnit = float(bins) / (hi - lo);
+    std::vector<size_t> lowEnds(size_t(bins), 0), highEnds(size_t(bins), 0);
+    for (const TriBox& r : refs) {
+      ++lowEnds[size_t(kdr::binOf(r.b.lo[axis], lo, perUnit, bins))];
+      ++highEnds[size_t(kdr::binOf(r.b.hi[axis], lo, perUnit, bins))];
+    }
+    size_t below = 0, above = refs.size();
+    for (int k = 1; k < bins; ++k) {
+      below += lowEnds[size_t(k - 1)];
+      above -= highEnds[size_t(k - 1)];
+      offer(axis, kdr::binPlane(lo, hi, k, bins), below, above);
+    }
+  }
+
+  // Planes at every distinct face position strictly inside the box.  Faces
+  // sort by position, and at one position closing faces before flat ones
+  // (references of no extent) before opening ones; a flat reference at the
+  // plane counts on both sides.
+  template <class Offer>
+  void offerFaces(const std::vector<TriBox>& refs, const Aabb& box, int axis, Offer& offer) const {
+    enum : uint8_t { kClosing = 0, kFlat = 1, kOpening = 2 };
+    struct Face {
+      float at;
+      uint8_t kind;
+    };
+    std::vector<Face> faces;
+    faces.reserve(2 * refs.size());
+    for (const TriBox& r : refs) {
+      const float a = r.b.lo[axis], b = r.b.hi[axis];
+      if (a == b) {
+        faces.push_back({a, kFlat});
+      } else {
+        faces.push_back({a, kOpening});
+        faces.push_back({b, kClosing});
+      }
+    }
+    std::sort(faces.begin(), faces.end(),
+              [](const Face& x, const Face& y) { return x.at != y.at ? x.at < y.at : x.kind < y.kind; });
+    const float lo = box.lo[axis], hi = box.hi[axis];
+    size_t below = 0, above = refs.size();
+    for (size_t i = 0; i < faces.size();) {
+      const float at = faces[i].at;
+      size_t n[3] = {0, 0, 0};
+      do ++n[faces[i++].kind];
+      while (i < faces.size() && faces[i].at == at);
+      above -= n[kClosing] + n[kFlat];
+      if (at > lo && at < hi) offer(axis, at, below + n[kFlat], above + n[kFlat]);
+      below += n[kOpening] + n[kFlat];
     }
   }
 

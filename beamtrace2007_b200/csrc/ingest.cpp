@@ -3,15 +3,18 @@
 //
 // A config names meshes and views; the scene built from it must be the one
 // the reference builds from the same file, vertex for vertex, since the kd
-// tree and every beam depend on the float coordinates.  So the parser, the
-// loaders and the generators follow the reference's arithmetic in its
-// order and in single precision (its float build):
-//   parseConfig / loadConfig / buildScene   src/scene/scene.cpp:127-262
-//   loadOBJ / loadPLY                       src/scene/loaders.cpp:29-240
+// tree and every beam depend on the float coordinates.  What that fixes is
+// the arithmetic, not the code: decimal text to double (correctly rounded)
+// to float, polygons cut into fans around their first corner, the index
+// rules of the two mesh formats, the view formulas of `orbit` and `walk`,
+// and the generators' float operations and random draws in their order.
+// The file readers and the config parser here are written from the formats'
+// own descriptions (Wavefront OBJ, Stanford PLY, and the config keys of
+// src/scene/scene.h:13-61); the generators restate the reference's scenes:
 //   buildProcedural and its scenes          src/scene/procedural.cpp:17-226
 //   addQuad / addBox / addSphere            src/scene/scene.cpp:44-87
 //   Scene::finalize                         src/scene/scene.cpp:8-42
-//   Rng (PCG32), splitWS, trim              src/util/misc.h:24-46, misc.cpp
+//   PCG32 and its [0, 1) mapping            src/util/misc.h:24-46
 // Compiled with -ffp-contract=off like the reference.
 #include <algorithm>
 #include <cmath>
@@ -19,10 +22,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <charconv>
 #include <map>
-#include <sstream>
 #include <stdexcept>
 #include <string>
+#include <string_view>
 #include <vector>
 
 #include "bt_gpu.h"
@@ -74,20 +78,6 @@ class Pcg32 {
   }
   uint64_t state_ = 0, inc_ = 0;
 };
-
-std::vector<std::string> words(const std::string& s) {
-  std::vector<std::string> out;
-  std::istringstream is(s);
-  std::string t;
-  while (is >> t) out.push_back(t);
-  return out;
-}
-
-std::string stripped(const std::string& s) {
-  const size_t a = s.find_first_not_of(" \t\r\n");
-  if (a == std::string::npos) return "";
-  return s.substr(a, s.find_last_not_of(" \t\r\n") - a + 1);
-}
 
 struct Mesh {
   std::vector<V> pos;
@@ -272,7 +262,8 @@ void scenePlant(Mesh& s, uint64_t seed) {
       const V side = unit(cross(axis, n) + n * float(g.uniform(-0.5, 0.5)));
       const V up = unit(cross(axis, side));
       const float L = float(0.07 + 0.06 * g.uniform()), W = L * 0.45f;
-      // a folded diamond: four triangles around a raised midrib point
+      // the leaf: a centre vertex lifted off the blade plane, joined to the
+      // tip, the two side points and the base (four triangles, a shallow tent)
       const uint32_t ic = s.vert(c + up * (L * 0.15f));
       const uint32_t i0 = s.vert(c - axis * L), i1 = s.vert(c + side * W), i2 = s.vert(c + axis * L),
                      i3 = s.vert(c - side * W);
@@ -309,37 +300,135 @@ void sceneBuilding(Mesh& s, int floors, int rooms, int detail) {
       }
 }
 
-using Params = std::map<std::string, std::string>;
 
-double param(const Params& p, const char* k, double def) {
-  const auto it = p.find(k);
-  return it == p.end() ? def : std::stod(it->second);
+// ---- text fields and numbers ----
+
+constexpr bool isBlank(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\f' || c == '\v'; }
+
+// Walks the blank-separated fields of a piece of text.
+class Fields {
+ public:
+  explicit Fields(std::string_view text) : rest_(text) {}
+  bool next(std::string_view& field) {
+    size_t a = 0;
+    while (a < rest_.size() && isBlank(rest_[a])) ++a;
+    size_t b = a;
+    while (b < rest_.size() && !isBlank(rest_[b])) ++b;
+    field = rest_.substr(a, b - a);
+    rest_.remove_prefix(b);
+    return !field.empty();
+  }
+  std::vector<std::string_view> all() {
+    std::vector<std::string_view> out;
+    std::string_view f;
+    while (next(f)) out.push_back(f);
+    return out;
+  }
+
+ private:
+  std::string_view rest_;
+};
+
+// Calls fn(line number from 1, line) for every line of `text` (LF ends a line).
+template <class Fn>
+void eachLine(std::string_view text, Fn&& fn) {
+  int number = 0;
+  while (!text.empty()) {
+    const size_t lf = text.find('\n');
+    fn(++number, text.substr(0, lf));
+    if (lf == std::string_view::npos) break;
+    text.remove_prefix(lf + 1);
+  }
 }
 
-bool procedural(const std::string& name, const Params& p, Mesh& s, std::string& err) {
+// Reads a number at the start of `s` as strtod does, without its leading
+// blanks: optional sign, then decimal digits with an optional exponent, a
+// 0x-prefixed hexadecimal float, inf or nan.  The double is the correctly
+// rounded value of the digits.  Returns the characters used, 0 when `s`
+// does not start with a number.
+size_t numberPrefix(std::string_view s, double& v) {
+  size_t i = 0;
+  const bool neg = !s.empty() && s[0] == '-';
+  if (!s.empty() && (s[0] == '+' || s[0] == '-')) i = 1;
+  if (i < s.size() && (s[i] == '+' || s[i] == '-')) return 0;
+  const bool hex = i + 1 < s.size() && s[i] == '0' && (s[i + 1] == 'x' || s[i + 1] == 'X');
+  const char* from = s.data() + i + (hex ? 2 : 0);
+  const auto r = std::from_chars(from, s.data() + s.size(), v, hex ? std::chars_format::hex : std::chars_format::general);
+  if (r.ec == std::errc::invalid_argument) {
+    if (!hex) return 0;
+    v = neg ? -0.0 : 0.0;  // "0x" with no hexadecimal digits: the "0"
+    return i + 1;
+  }
+  const size_t used = size_t(r.ptr - s.data());
+  if (r.ec == std::errc::result_out_of_range) {
+    v = std::strtod(std::string(s.substr(0, used)).c_str(), nullptr);  // saturated: +-HUGE_VAL or a zero
+    return used;
+  }
+  if (neg) v = -v;
+  return used;
+}
+
+// The whole field as a number.
+bool wholeNumber(std::string_view s, double& v) { return !s.empty() && numberPrefix(s, v) == s.size(); }
+
+// An integer at the start of `s` (a leading '+' allowed); values beyond
+// int64 saturate.  False when `s` does not start with one.
+bool integerPrefix(std::string_view s, int64_t& v) {
+  const size_t skip = (s.size() > 1 && s[0] == '+' && s[1] != '-') ? 1 : 0;
+  const auto r = std::from_chars(s.data() + skip, s.data() + s.size(), v);
+  if (r.ec == std::errc::invalid_argument) return false;
+  if (r.ec == std::errc::result_out_of_range) v = s[skip] == '-' ? INT64_MIN : INT64_MAX;
+  return true;
+}
+
+std::string quoted(std::string_view s) { return "'" + std::string(s) + "'"; }
+
+// ---- procedural scenes by name ----
+
+// key=value parameters of a procedural mesh line.
+class SceneParams {
+ public:
+  void set(std::string_view kv) {
+    const size_t e = kv.find('=');
+    values_[std::string(kv.substr(0, e))] = std::string(kv.substr(e + 1));
+  }
+  double get(const char* key, double fallback) const {
+    const auto it = values_.find(key);
+    if (it == values_.end()) return fallback;
+    double v;
+    if (!wholeNumber(it->second, v))
+      throw std::invalid_argument(std::string("procedural parameter ") + key + "=" + it->second + " is not a number");
+    return v;
+  }
+
+ private:
+  std::map<std::string, std::string, std::less<>> values_;
+};
+
+bool procedural(std::string_view name, const SceneParams& p, Mesh& s, std::string& why) {
   if (name == "room") {
     sceneRoom(s);
   } else if (name == "plant") {
-    scenePlant(s, uint64_t(param(p, "seed", 7)));
+    scenePlant(s, uint64_t(p.get("seed", 7)));
   } else if (name == "building") {
-    sceneBuilding(s, int(param(p, "floors", 7)), int(param(p, "rooms", 8)), int(param(p, "detail", 33)));
+    sceneBuilding(s, int(p.get("floors", 7)), int(p.get("rooms", 8)), int(p.get("detail", 33)));
   } else if (name == "tess_sweep") {
-    const int stacks = int(param(p, "stacks", 16));
+    const int stacks = int(p.get("stacks", 16));
     const uint16_t floorM = s.material(V(0.75f, 0.75f, 0.75f)), ballM = s.material(V(0.8f, 0.5f, 0.35f));
     s.quad(V(-6, 0, -6), V(-6, 0, 6), V(6, 0, 6), V(6, 0, -6), floorM);
     for (int i = 0; i < 5; ++i)
       for (int j = 0; j < 5; ++j) s.sphere(V(float(-4 + 2 * i), 0.8f, float(-4 + 2 * j)), 0.75f, stacks, 2 * stacks, ballM);
   } else if (name == "analytic") {
-    const float h = float(param(p, "h", 1)), occ = float(param(p, "occ", 1)), F = float(param(p, "floor", 10));
-    const float ox = float(param(p, "ox", 0)), oz = float(param(p, "oz", 0));
+    const float h = float(p.get("h", 1)), occ = float(p.get("occ", 1)), F = float(p.get("floor", 10));
+    const float ox = float(p.get("ox", 0)), oz = float(p.get("oz", 0));
     const uint16_t floorM = s.material(V(0.8f, 0.8f, 0.8f)), occM = s.material(V(0.8f, 0.4f, 0.3f));
     s.quad(V(-F, 0, -F), V(-F, 0, F), V(F, 0, F), V(F, 0, -F), floorM);
     const float a = occ / 2;
     s.quad(V(ox - a, h, oz - a), V(ox - a, h, oz + a), V(ox + a, h, oz + a), V(ox + a, h, oz - a), occM);
   } else if (name == "random_tris") {
-    const int n = int(param(p, "n", 50));
-    Pcg32 g(uint64_t(param(p, "seed", 1)));
-    const float size = float(param(p, "size", 0.3));
+    const int n = int(p.get("n", 50));
+    Pcg32 g(uint64_t(p.get("seed", 1)));
+    const float size = float(p.get("size", 0.3));
     const uint16_t m = s.material(V(0.7f, 0.7f, 0.7f));
     for (int i = 0; i < n; ++i) {
       const V c = draw3(g, 0, 1, 0, 1, 0, 1);
@@ -348,238 +437,295 @@ bool procedural(const std::string& name, const Params& p, Mesh& s, std::string& 
       s.tri(idx[0], idx[1], idx[2], m);
     }
   } else if (name == "floorquad") {
-    const float y = float(param(p, "y", 0)), F = float(param(p, "size", 10)) / 2;
+    const float y = float(p.get("y", 0)), F = float(p.get("size", 10)) / 2;
     const uint16_t m = s.material(V(0.75f, 0.75f, 0.72f));
     s.quad(V(-F, y, -F), V(-F, y, F), V(F, y, F), V(F, y, -F), m);
   } else if (name == "sphere") {
     const uint16_t m = s.material(V(0.7f, 0.7f, 0.7f));
-    const int st = int(param(p, "stacks", 24));
-    s.sphere(V(0, 0, 0), float(param(p, "r", 1)), st, 2 * st, m);
+    const int st = int(p.get("stacks", 24));
+    s.sphere(V(0, 0, 0), float(p.get("r", 1)), st, 2 * st, m);
   } else {
-    err = "unknown procedural scene '" + name + "'";
+    why = "no procedural scene named " + quoted(name);
     return false;
   }
   return true;
 }
 
-// ---- mesh files (loaders.cpp) ----
+// ---- mesh files ----
 
-bool slurp(const std::string& path, std::string& out) {
-  FILE* f = fopen(path.c_str(), "rb");
+bool readWholeFile(const std::string& path, std::string& bytes) {
+  std::FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return false;
-  fseek(f, 0, SEEK_END);
-  const long n = ftell(f);
-  fseek(f, 0, SEEK_SET);
-  out.resize(size_t(n > 0 ? n : 0));
-  const size_t got = n > 0 ? fread(&out[0], 1, size_t(n), f) : 0;
-  fclose(f);
-  return n >= 0 && got == size_t(n);
+  bytes.clear();
+  char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) bytes.append(chunk, got);
+  const bool ok = !std::ferror(f);
+  std::fclose(f);
+  return ok;
 }
 
-// Polygon (i0, i1, ..., ik) as the fan (i0, i[k-1], i[k]); indices outside
-// [0, nv) drop that triangle only.
-void fan(Mesh& s, uint32_t base, const std::vector<long>& idx, long nv, uint16_t m) {
-  for (size_t k = 2; k < idx.size(); ++k) {
-    const long a = idx[0], b = idx[k - 1], c = idx[k];
-    if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) continue;
-    s.tri(base + uint32_t(a), base + uint32_t(b), base + uint32_t(c), m);
+// Adds polygon `corners` (indices into the positions [first, first + count)
+// of one file) as the triangles (c0, c[k-1], c[k]); a triangle with a corner
+// outside that range is left out, the rest of the polygon is kept.
+void addPolygon(Mesh& m, uint32_t first, const std::vector<int64_t>& corners, int64_t count, uint16_t mat) {
+  auto valid = [count](int64_t c) { return c >= 0 && c < count; };
+  for (size_t k = 2; k < corners.size(); ++k) {
+    const int64_t a = corners[0], b = corners[k - 1], c = corners[k];
+    if (valid(a) && valid(b) && valid(c)) m.tri(first + uint32_t(a), first + uint32_t(b), first + uint32_t(c), mat);
   }
 }
 
-// Wavefront OBJ: `v x y z` and `f a b c ...` (a/vt/vn accepted, negative
-// indices count back from the last vertex); other lines are ignored.
-bool loadObj(const std::string& path, Mesh& s, uint16_t m, std::string& err) {
-  std::string text;
-  if (!slurp(path, text)) {
-    err = "cannot read " + path;
+// Wavefront OBJ geometry.  A `v` record adds a position; coordinates that
+// are missing or not numbers read as 0.  An `f` record is a polygon whose
+// corners name positions of this file: 1-based, or negative to count back
+// from the newest position, each possibly followed by /texture/normal
+// references, which are ignored; a field that does not start with an
+// integer ends the corner list.  Every other record (vt, vn, o, g, usemtl,
+// l, ...) is skipped.
+bool readObj(const std::string& path, Mesh& m, uint16_t mat, std::string& why) {
+  std::string bytes;
+  if (!readWholeFile(path, bytes)) {
+    why = "could not open mesh file " + path;
     return false;
   }
-  const uint32_t base = uint32_t(s.pos.size());
-  long nv = 0;
-  std::vector<long> face;
-  const char* p = text.c_str();
-  const char* const end = p + text.size();
-  while (p < end) {
-    const char* eol = static_cast<const char*>(memchr(p, '\n', size_t(end - p)));
-    if (!eol) eol = end;
-    while (p < eol && (*p == ' ' || *p == '\t')) ++p;
-    const bool tag = p + 1 < eol && (p[1] == ' ' || p[1] == '\t');
-    if (tag && p[0] == 'v') {
-      char* q;
-      const double x = strtod(p + 1, &q);
-      const double y = strtod(q, &q);
-      const double z = strtod(q, &q);
-      s.vert(V(float(x), float(y), float(z)));
-      ++nv;
-    } else if (tag && p[0] == 'f') {
-      face.clear();
-      const char* q = p + 1;
-      while (q < eol) {
-        while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
-        if (q >= eol) break;
-        char* r;
-        const long i = strtol(q, &r, 10);
-        if (r == q) break;
-        face.push_back(i > 0 ? i - 1 : nv + i);
-        q = r;
-        while (q < eol && *q != ' ' && *q != '\t') ++q;
+  const uint32_t first = uint32_t(m.pos.size());
+  int64_t count = 0;
+  std::vector<int64_t> corners;
+  eachLine(bytes, [&](int, std::string_view line) {
+    Fields f(line);
+    std::string_view record, field;
+    if (!f.next(record)) return;
+    if (record == "v") {
+      float xyz[3] = {0, 0, 0};
+      for (float& c : xyz) {
+        double d;
+        if (!f.next(field) || numberPrefix(field, d) == 0) break;
+        c = float(d);
       }
-      fan(s, base, face, nv, m);
+      m.vert(V(xyz[0], xyz[1], xyz[2]));
+      ++count;
+    } else if (record == "f") {
+      corners.clear();
+      int64_t ref;
+      while (f.next(field) && integerPrefix(field, ref))
+        corners.push_back(ref > 0 ? ref - 1 : (ref < -count ? -1 : count + ref));
+      addPolygon(m, first, corners, count, mat);
     }
-    p = eol + 1;
-  }
-  if (nv == 0) {
-    err = "no vertices in " + path;
+  });
+  if (count == 0) {
+    why = path + " holds no vertex positions";
     return false;
   }
   return true;
 }
 
-enum class Ply { I8, U8, I16, U16, I32, U32, F32, F64, Bad };
+// PLY (ascii, binary_little_endian, binary_big_endian).  The header lists
+// groups of records ("element NAME COUNT"), each with its columns
+// ("property TYPE NAME" or "property list LENGTHTYPE TYPE NAME"); the body
+// holds the records group after group.  Positions come from the x, y, z
+// columns of group `vertex`, polygons from the vertex_indices (or
+// vertex_index) list of group `face`; everything else is read and dropped.
+enum class PlyType : uint8_t { None, I8, U8, I16, U16, I32, U32, F32, F64 };
 
-Ply plyType(const std::string& t) {
-  static const std::pair<const char*, Ply> kNames[] = {
-      {"char", Ply::I8},   {"int8", Ply::I8},     {"uchar", Ply::U8},   {"uint8", Ply::U8},
-      {"short", Ply::I16}, {"int16", Ply::I16},   {"ushort", Ply::U16}, {"uint16", Ply::U16},
-      {"int", Ply::I32},   {"int32", Ply::I32},   {"uint", Ply::U32},   {"uint32", Ply::U32},
-      {"float", Ply::F32}, {"float32", Ply::F32}, {"double", Ply::F64}, {"float64", Ply::F64}};
-  for (const auto& kv : kNames)
-    if (t == kv.first) return kv.second;
-  return Ply::Bad;
+PlyType plyTypeNamed(std::string_view n) {
+  struct Name { const char* text; PlyType type; };
+  static const Name kNames[] = {{"char", PlyType::I8},    {"int8", PlyType::I8},     {"uchar", PlyType::U8},
+                                {"uint8", PlyType::U8},   {"short", PlyType::I16},   {"int16", PlyType::I16},
+                                {"ushort", PlyType::U16}, {"uint16", PlyType::U16},  {"int", PlyType::I32},
+                                {"int32", PlyType::I32},  {"uint", PlyType::U32},    {"uint32", PlyType::U32},
+                                {"float", PlyType::F32},  {"float32", PlyType::F32}, {"double", PlyType::F64},
+                                {"float64", PlyType::F64}};
+  for (const Name& x : kNames)
+    if (n == x.text) return x.type;
+  return PlyType::None;
 }
 
-int plyBytes(Ply t) {
-  switch (t) {
-    case Ply::I8: case Ply::U8: return 1;
-    case Ply::I16: case Ply::U16: return 2;
-    case Ply::I32: case Ply::U32: case Ply::F32: return 4;
-    case Ply::F64: return 8;
-    default: return 0;
-  }
+size_t plySize(PlyType t) {
+  static const size_t kSize[] = {0, 1, 1, 2, 2, 4, 4, 4, 8};
+  return kSize[size_t(t)];
 }
 
-double plyBinary(const char*& p, Ply t, bool big) {
-  unsigned char b[8] = {0};
-  const int n = plyBytes(t);
-  for (int i = 0; i < n; ++i) b[i] = static_cast<unsigned char>(p[big ? n - 1 - i : i]);
-  p += n;
-  switch (t) {
-    case Ply::I8: return double(int8_t(b[0]));
-    case Ply::U8: return double(b[0]);
-    case Ply::I16: { int16_t v; memcpy(&v, b, 2); return v; }
-    case Ply::U16: { uint16_t v; memcpy(&v, b, 2); return v; }
-    case Ply::I32: { int32_t v; memcpy(&v, b, 4); return v; }
-    case Ply::U32: { uint32_t v; memcpy(&v, b, 4); return v; }
-    case Ply::F32: { float v; memcpy(&v, b, 4); return v; }
-    case Ply::F64: { double v; memcpy(&v, b, 8); return v; }
-    default: return 0;
-  }
-}
-
-struct PlyProperty {
+struct PlyColumn {
   std::string name;
-  Ply type = Ply::Bad, countType = Ply::Bad;
-  bool list = false;
-};
-struct PlyElement {
-  std::string name;
-  size_t count = 0;
-  std::vector<PlyProperty> props;
+  PlyType type = PlyType::None;
+  PlyType lengthType = PlyType::None;  // set for list columns
 };
 
-// PLY in ascii, binary_little_endian or binary_big_endian: x, y, z of the
-// `vertex` element and vertex_indices / vertex_index lists of `face`.
-bool loadPly(const std::string& path, Mesh& s, uint16_t m, std::string& err) {
-  std::string data;
-  if (!slurp(path, data)) {
-    err = "cannot read " + path;
-    return false;
-  }
-  const size_t hdrEnd = data.find("end_header");
-  if (data.compare(0, 3, "ply") != 0 || hdrEnd == std::string::npos) {
-    err = path + ": not a PLY file";
-    return false;
-  }
-  size_t body = data.find('\n', hdrEnd);
-  if (body == std::string::npos) {
-    err = path + ": truncated header";
-    return false;
-  }
-  ++body;
-  std::istringstream hs(data.substr(0, hdrEnd));
-  std::string line, format;
-  std::vector<PlyElement> elems;
-  while (std::getline(hs, line)) {
-    const auto t = words(line);
-    if (t.empty()) continue;
-    if (t[0] == "format" && t.size() > 1) {
-      format = t[1];
-    } else if (t[0] == "element" && t.size() > 2) {
-      PlyElement e;
-      e.name = t[1];
-      e.count = size_t(std::stoull(t[2]));
-      elems.push_back(e);
-    } else if (t[0] == "property" && !elems.empty()) {
-      PlyProperty pr;
-      if (t.size() > 4 && t[1] == "list") {
-        pr.list = true;
-        pr.countType = plyType(t[2]);
-        pr.type = plyType(t[3]);
-        pr.name = t[4];
-      } else if (t.size() > 2) {
-        pr.type = plyType(t[1]);
-        pr.name = t[2];
+struct PlyGroup {
+  std::string name;
+  uint64_t rows = 0;
+  std::vector<PlyColumn> columns;
+};
+
+enum class PlyEncoding { Ascii, Little, Big };
+
+// Reads the header; `body` = offset of the first byte after end_header's line.
+bool plyHeader(const std::string& bytes, const std::string& path, PlyEncoding& enc, std::vector<PlyGroup>& groups,
+               size_t& body, std::string& why) {
+  size_t at = 0;
+  bool sawMagic = false, sawFormat = false;
+  while (at < bytes.size()) {
+    const size_t lf = bytes.find('\n', at);
+    const size_t end = lf == std::string::npos ? bytes.size() : lf;
+    const std::vector<std::string_view> t = Fields(std::string_view(bytes).substr(at, end - at)).all();
+    at = lf == std::string::npos ? bytes.size() : lf + 1;
+    if (!sawMagic) {
+      if (t.size() != 1 || t[0] != "ply") break;
+      sawMagic = true;
+      continue;
+    }
+    if (t.empty() || t[0] == "comment" || t[0] == "obj_info") continue;
+    if (t[0] == "end_header") {
+      if (!sawFormat) {
+        why = path + ": PLY header names no format";
+        return false;
       }
-      elems.back().props.push_back(pr);
+      if (lf == std::string::npos) {
+        why = path + ": PLY file ends inside its header";
+        return false;
+      }
+      body = at;
+      return true;
+    }
+    if (t[0] == "format" && t.size() >= 2) {
+      sawFormat = true;
+      if (t[1] == "ascii") {
+        enc = PlyEncoding::Ascii;
+      } else if (t[1] == "binary_little_endian") {
+        enc = PlyEncoding::Little;
+      } else if (t[1] == "binary_big_endian") {
+        enc = PlyEncoding::Big;
+      } else {
+        why = path + ": PLY encoding " + quoted(t[1]) + " is not supported";
+        return false;
+      }
+    } else if (t[0] == "element" && t.size() >= 3) {
+      PlyGroup g;
+      g.name = std::string(t[1]);
+      const auto r = std::from_chars(t[2].data(), t[2].data() + t[2].size(), g.rows);
+      if (r.ec != std::errc() || r.ptr != t[2].data() + t[2].size()) {
+        why = path + ": PLY record count " + quoted(t[2]) + " is not a count";
+        return false;
+      }
+      groups.push_back(std::move(g));
+    } else if (t[0] == "property" && !groups.empty()) {
+      PlyColumn c;
+      const bool list = t.size() >= 5 && t[1] == "list";
+      if (list) {
+        c.lengthType = plyTypeNamed(t[2]);
+        c.type = plyTypeNamed(t[3]);
+        c.name = std::string(t[4]);
+      } else if (t.size() >= 3) {
+        c.type = plyTypeNamed(t[1]);
+        c.name = std::string(t[2]);
+      }
+      if (c.type == PlyType::None || (list && c.lengthType == PlyType::None)) {
+        why = path + ": PLY column with an unknown type";
+        return false;
+      }
+      groups.back().columns.push_back(std::move(c));
+    } else {
+      why = path + ": PLY header line " + quoted(t[0]) + " not understood";
+      return false;
     }
   }
-  const bool ascii = format == "ascii", big = format == "binary_big_endian";
-  if (!ascii && !big && format != "binary_little_endian") {
-    err = path + ": unsupported PLY format " + format;
+  why = sawMagic ? path + ": PLY header has no end_header line" : path + ": not a PLY file (no 'ply' line)";
+  return false;
+}
+
+// Values of a PLY body, one at a time.
+class PlyBody {
+ public:
+  PlyBody(std::string_view bytes, PlyEncoding enc) : rest_(bytes), fields_(bytes), enc_(enc) {}
+
+  bool value(PlyType t, double& v) {
+    if (enc_ == PlyEncoding::Ascii) {
+      std::string_view f;
+      return fields_.next(f) && wholeNumber(f, v);
+    }
+    const size_t n = plySize(t);
+    if (rest_.size() < n) return false;
+    unsigned char b[8];
+    std::memcpy(b, rest_.data(), n);
+    rest_.remove_prefix(n);
+    if (enc_ == PlyEncoding::Big) std::reverse(b, b + n);  // this library runs on little-endian hosts
+    switch (t) {
+      case PlyType::I8: v = double(int8_t(b[0])); break;
+      case PlyType::U8: v = double(b[0]); break;
+      case PlyType::I16: v = double(bitsAs<int16_t>(b)); break;
+      case PlyType::U16: v = double(bitsAs<uint16_t>(b)); break;
+      case PlyType::I32: v = double(bitsAs<int32_t>(b)); break;
+      case PlyType::U32: v = double(bitsAs<uint32_t>(b)); break;
+      case PlyType::F32: v = double(bitsAs<float>(b)); break;
+      case PlyType::F64: v = bitsAs<double>(b); break;
+      default: return false;
+    }
+    return true;
+  }
+
+ private:
+  template <class T>
+  static T bitsAs(const unsigned char* b) {
+    T x;
+    std::memcpy(&x, b, sizeof x);
+    return x;
+  }
+  std::string_view rest_;
+  Fields fields_;
+  PlyEncoding enc_;
+};
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the PLY reader assumes a little-endian host");
+
+bool readPly(const std::string& path, Mesh& m, uint16_t mat, std::string& why) {
+  std::string bytes;
+  if (!readWholeFile(path, bytes)) {
+    why = "could not open mesh file " + path;
     return false;
   }
-  const uint32_t base = uint32_t(s.pos.size());
-  long nv = 0;
-  const char* p = data.c_str() + body;
-  const char* const end = data.c_str() + data.size();
-  auto value = [&](Ply t) -> double {
-    if (ascii) {
-      char* q;
-      const double v = strtod(p, &q);
-      p = q;
-      return v;
-    }
-    if (p + plyBytes(t) > end) return 0;
-    return plyBinary(p, t, big);
-  };
-  std::vector<long> idx;
-  for (const PlyElement& e : elems)
-    for (size_t i = 0; i < e.count; ++i) {
+  PlyEncoding enc = PlyEncoding::Ascii;
+  std::vector<PlyGroup> groups;
+  size_t body = 0;
+  if (!plyHeader(bytes, path, enc, groups, body, why)) return false;
+  PlyBody in(std::string_view(bytes).substr(body), enc);
+  const uint32_t first = uint32_t(m.pos.size());
+  int64_t count = 0;
+  std::vector<int64_t> corners;
+  auto readGroup = [&](const PlyGroup& g) {
+    const bool positions = g.name == "vertex", polygons = g.name == "face";
+    for (uint64_t row = 0; row < g.rows; ++row) {
       double xyz[3] = {0, 0, 0};
-      idx.clear();
-      for (const PlyProperty& pr : e.props) {
-        if (pr.list) {
-          const long n = long(value(pr.countType));
-          for (long k = 0; k < n; ++k) {
-            const double v = value(pr.type);
-            if (pr.name == "vertex_indices" || pr.name == "vertex_index") idx.push_back(long(v));
-          }
-        } else {
-          const double v = value(pr.type);
-          if (pr.name == "x") xyz[0] = v;
-          else if (pr.name == "y") xyz[1] = v;
-          else if (pr.name == "z") xyz[2] = v;
+      corners.clear();
+      for (const PlyColumn& c : g.columns) {
+        double v;
+        if (c.lengthType == PlyType::None) {
+          if (!in.value(c.type, v)) return false;
+          if (c.name.size() == 1 && c.name[0] >= 'x' && c.name[0] <= 'z') xyz[c.name[0] - 'x'] = v;
+          continue;
+        }
+        if (!in.value(c.lengthType, v)) return false;
+        const bool keep = polygons && (c.name == "vertex_indices" || c.name == "vertex_index");
+        for (int64_t k = 0, n = int64_t(v); k < n; ++k) {
+          if (!in.value(c.type, v)) return false;
+          if (keep) corners.push_back(int64_t(v));
         }
       }
-      if (e.name == "vertex") {
-        s.vert(V(float(xyz[0]), float(xyz[1]), float(xyz[2])));
-        ++nv;
-      } else if (e.name == "face") {
-        fan(s, base, idx, nv, m);
+      if (positions) {
+        m.vert(V(float(xyz[0]), float(xyz[1]), float(xyz[2])));
+        ++count;
+      } else if (polygons) {
+        addPolygon(m, first, corners, count, mat);
       }
     }
-  if (nv == 0) {
-    err = path + ": no vertices";
+    return true;
+  };
+  for (const PlyGroup& g : groups)
+    if (!readGroup(g)) {
+      why = path + ": PLY body ends early or holds a value that is not a number";
+      return false;
+    }
+  if (count == 0) {
+    why = path + " holds no vertex positions";
     return false;
   }
   return true;
@@ -587,25 +733,16 @@ bool loadPly(const std::string& path, Mesh& s, uint16_t m, std::string& err) {
 
 }  // namespace
 
-// ---- configs (scene.cpp:127-262) ----
+// ---- configs ----
 
 struct bt_scene_file {
   bt_scene_file_info info;
-  std::vector<std::string> meshLines;
-  std::vector<float> views;  // eye, target, fov per view
+  std::vector<std::vector<std::string>> meshes;  // the fields after `mesh`, per mesh line
+  std::vector<float> views;                      // eye, target, fov per view
   Mesh mesh;
 };
 
 namespace {
-
-bool numbers(const std::vector<std::string>& t, size_t n, float* out, std::string& err) {
-  if (t.size() < 1 + n) {
-    err = "expected " + std::to_string(n) + " numbers after '" + t[0] + "'";
-    return false;
-  }
-  for (size_t i = 0; i < n; ++i) out[i] = float(std::stod(t[1 + i]));
-  return true;
-}
 
 void setV(float* dst, V v) {
   dst[0] = v.x;
@@ -618,140 +755,177 @@ void addView(bt_scene_file& f, V eye, V target, float fov) {
   f.views.insert(f.views.end(), {eye.x, eye.y, eye.z, target.x, target.y, target.z, fov});
 }
 
-bool parse(const std::string& text, bt_scene_file& f, std::string& err) {
-  std::istringstream is(text);
-  std::string line;
-  int lineNo = 0;
-  try {
-    while (std::getline(is, line)) {
-      ++lineNo;
-      const size_t hash = line.find('#');
-      if (hash != std::string::npos) line = line.substr(0, hash);
-      const auto t = words(line);
-      if (t.empty()) continue;
-      const std::string& k = t[0];
-      float v[9];
-      bt_scene_file_info& in = f.info;
-      if (k == "name") {
-        snprintf(in.name, sizeof in.name, "%s", t.size() > 1 ? t[1].c_str() : "");
-      } else if (k == "mesh") {
-        f.meshLines.push_back(stripped(line.substr(line.find("mesh") + 4)));
-      } else if (k == "cull_backfaces") {
-        in.cull_backfaces = t.size() > 1 && t[1] != "0";
-      } else if (k == "up") {
-        if (!numbers(t, 3, v, err)) return false;
-        setV(in.up, V(v[0], v[1], v[2]));
-      } else if (k == "view") {
-        if (!numbers(t, 7, v, err)) return false;
-        addView(f, V(v[0], v[1], v[2]), V(v[3], v[4], v[5]), v[6]);
-      } else if (k == "orbit") {
-        // orbit cx cy cz radius height count fov: views on a circle about c
-        if (!numbers(t, 7, v, err)) return false;
-        const int n = int(v[5]);
-        const V c(v[0], v[1], v[2]), up = unit(getV(in.up));
-        const V a = orthogonalTo(up), b = cross(up, a);
-        for (int i = 0; i < n; ++i) {
-          const double ang = 2 * M_PI * (i + 0.125) / n;
-          const V eye = c + a * float(v[3] * std::cos(ang)) + b * float(v[3] * std::sin(ang)) + up * v[4];
-          addView(f, eye, c, v[6]);
-        }
-      } else if (k == "walk") {
-        // walk x0 y0 z0 x1 y1 z1 count fov: views along a segment, looking
-        // ahead with a small left-right swing
-        if (!numbers(t, 8, v, err)) return false;
-        const V p0(v[0], v[1], v[2]), p1(v[3], v[4], v[5]);
-        const int n = int(v[6]);
-        const V dir = unit(p1 - p0);
-        for (int i = 0; i < n; ++i) {
-          const float s = n > 1 ? float(i) / float(n - 1) : 0;
-          const V eye = p0 + (p1 - p0) * (s * 0.85f);
-          const V side = unit(cross(dir, unit(getV(in.up))));
-          const float swing = float(0.6 * std::sin(2.3 * i));
-          addView(f, eye, eye + dir + side * swing, v[7]);
-        }
-      } else if (k == "point_light") {
-        if (!numbers(t, 3, v, err)) return false;
-        in.has_point_light = 1;
-        setV(in.point_light, V(v[0], v[1], v[2]));
-      } else if (k == "area_light") {
-        if (!numbers(t, 9, v, err)) return false;
-        in.has_area_light = 1;
-        setV(in.light_c, V(v[0], v[1], v[2]));
-        setV(in.light_u, V(v[3], v[4], v[5]));
-        setV(in.light_v, V(v[6], v[7], v[8]));
-      } else if (k == "light_intensity") {
-        if (!numbers(t, 1, v, err)) return false;
-        in.light_intensity = v[0];
-      } else if (k == "background") {
-        if (!numbers(t, 3, v, err)) return false;
-        setV(in.background, V(v[0], v[1], v[2]));
-      } else {
-        err = "unknown key '" + k + "'";
+// orbit cx cy cz radius height count fov: `count` views on a circle of
+// `radius` about c, raised by `height` along up, looking at c; the first at
+// an eighth of the spacing past the first axis orthogonal to up.
+void addOrbit(bt_scene_file& f, const float* a) {
+  const int n = int(a[5]);
+  const V c(a[0], a[1], a[2]), up = unit(getV(f.info.up));
+  const V e0 = orthogonalTo(up), e1 = cross(up, e0);
+  for (int i = 0; i < n; ++i) {
+    const double phi = 2 * M_PI * (i + 0.125) / n;
+    addView(f, c + e0 * float(a[3] * std::cos(phi)) + e1 * float(a[3] * std::sin(phi)) + up * a[4], c, a[6]);
+  }
+}
+
+// walk x0 y0 z0 x1 y1 z1 count fov: `count` views spread over the first 85%
+// of the segment p0 -> p1, each looking one unit ahead, turned sideways by
+// 0.6 sin(2.3 i) units.
+void addWalk(bt_scene_file& f, const float* a) {
+  const V p0(a[0], a[1], a[2]), p1(a[3], a[4], a[5]);
+  const int n = int(a[6]);
+  const V dir = unit(p1 - p0);
+  for (int i = 0; i < n; ++i) {
+    const float s = n > 1 ? float(i) / float(n - 1) : 0;
+    const V eye = p0 + (p1 - p0) * (s * 0.85f);
+    const V side = unit(cross(dir, unit(getV(f.info.up))));
+    addView(f, eye, eye + dir + side * float(0.6 * std::sin(2.3 * i)), a[7]);
+  }
+}
+
+// Keys that take a fixed number of numbers.
+struct NumericKey {
+  const char* key;
+  int count;
+  void (*apply)(bt_scene_file& f, const float* a);
+};
+
+const NumericKey kNumericKeys[] = {
+    {"up", 3, [](bt_scene_file& f, const float* a) { setV(f.info.up, getV(a)); }},
+    {"view", 7, [](bt_scene_file& f, const float* a) { addView(f, getV(a), getV(a + 3), a[6]); }},
+    {"orbit", 7, addOrbit},
+    {"walk", 8, addWalk},
+    {"point_light", 3,
+     [](bt_scene_file& f, const float* a) {
+       f.info.has_point_light = 1;
+       setV(f.info.point_light, getV(a));
+     }},
+    {"area_light", 9,
+     [](bt_scene_file& f, const float* a) {
+       f.info.has_area_light = 1;
+       setV(f.info.light_c, getV(a));
+       setV(f.info.light_u, getV(a + 3));
+       setV(f.info.light_v, getV(a + 6));
+     }},
+    {"light_intensity", 1, [](bt_scene_file& f, const float* a) { f.info.light_intensity = a[0]; }},
+    {"background", 3, [](bt_scene_file& f, const float* a) { setV(f.info.background, getV(a)); }},
+};
+
+// One `key values...` line (the text after '#' dropped); false with `why`.
+bool configLine(bt_scene_file& f, const std::vector<std::string_view>& t, std::string& why) {
+  const std::string_view key = t[0];
+  if (key == "name") {
+    snprintf(f.info.name, sizeof f.info.name, "%s", t.size() > 1 ? std::string(t[1]).c_str() : "");
+    return true;
+  }
+  if (key == "mesh") {
+    f.meshes.emplace_back(t.begin() + 1, t.end());
+    return true;
+  }
+  if (key == "cull_backfaces") {
+    f.info.cull_backfaces = t.size() > 1 && t[1] != "0";
+    return true;
+  }
+  for (const NumericKey& k : kNumericKeys) {
+    if (key != k.key) continue;
+    if (int(t.size()) - 1 < k.count) {
+      why = quoted(key) + " takes " + std::to_string(k.count) + " numbers, got " + std::to_string(t.size() - 1);
+      return false;
+    }
+    float a[9];
+    for (int i = 0; i < k.count; ++i) {
+      double d;
+      if (!wholeNumber(t[size_t(1 + i)], d)) {
+        why = quoted(t[size_t(1 + i)]) + " is not a number";
         return false;
       }
+      a[i] = float(d);
     }
-  } catch (const std::exception& e) {
-    err = "line " + std::to_string(lineNo) + ": " + e.what();
+    k.apply(f, a);
+    return true;
+  }
+  why = quoted(key) + " is not a config key";
+  return false;
+}
+
+bool parse(std::string_view text, bt_scene_file& f, std::string& why) {
+  bool ok = true;
+  eachLine(text, [&](int number, std::string_view line) {
+    if (!ok) return;
+    const std::vector<std::string_view> t = Fields(line.substr(0, line.find('#'))).all();
+    if (t.empty() || configLine(f, t, why)) return;
+    why = "line " + std::to_string(number) + ": " + why;
+    ok = false;
+  });
+  return ok;
+}
+
+// A mesh line: `obj PATH` or `ply PATH` with optional `scale s`,
+// `translate x y z` and `color r g b` (placed as p * s + t, in that order),
+// or `procedural NAME` with key=value parameters.  A file mesh without a
+// colour takes the next of six palette colours by its place among the
+// config's meshes.
+bool addMesh(Mesh& s, const std::vector<std::string>& t, int place, std::string& why) {
+  static const V kPalette[6] = {V(0.75f, 0.75f, 0.75f), V(0.8f, 0.55f, 0.4f), V(0.45f, 0.65f, 0.8f),
+                                V(0.6f, 0.8f, 0.45f),   V(0.85f, 0.8f, 0.5f), V(0.7f, 0.5f, 0.75f)};
+  if (t.size() < 2) {
+    why = "mesh line " + quoted(t.empty() ? "" : t[0]) + " names no file or scene";
     return false;
   }
+  float scale = 1;
+  V shift, color = kPalette[place % 6];
+  SceneParams params;
+  auto numbersAt = [&](size_t i, int k, float* out) {
+    for (int j = 0; j < k; ++j) {
+      double d;
+      if (!wholeNumber(t[i + size_t(j)], d)) throw std::invalid_argument(quoted(t[i + size_t(j)]) + " is not a number");
+      out[j] = float(d);
+    }
+  };
+  for (size_t i = 2; i < t.size(); ++i) {
+    const std::string& w = t[i];
+    float a[3];
+    if (w == "scale" && i + 1 < t.size()) {
+      numbersAt(i + 1, 1, &scale);
+      i += 1;
+    } else if ((w == "translate" || w == "color") && i + 3 < t.size()) {
+      numbersAt(i + 1, 3, a);
+      (w == "translate" ? shift : color) = V(a[0], a[1], a[2]);
+      i += 3;
+    } else if (w.find('=') != std::string::npos) {
+      params.set(w);
+    }
+  }
+  const size_t before = s.pos.size();
+  bool ok;
+  if (t[0] == "obj") {
+    ok = readObj(t[1], s, s.material(color), why);
+  } else if (t[0] == "ply") {
+    ok = readPly(t[1], s, s.material(color), why);
+  } else if (t[0] == "procedural") {
+    ok = procedural(t[1], params, s, why);
+  } else {
+    why = "mesh kind " + quoted(t[0]) + " is not obj, ply or procedural";
+    return false;
+  }
+  if (!ok) return false;
+  for (size_t i = before; i < s.pos.size(); ++i) s.pos[i] = s.pos[i] * scale + shift;
   return true;
 }
 
-// The meshes of the config, in order; each may carry `scale s`,
-// `translate x y z`, `color r g b` (file meshes) or key=value parameters
-// (procedural scenes).  Then Scene::finalize's degeneracy rule, keeping
-// each surviving triangle's material.
-bool build(bt_scene_file& f, std::string& err) {
-  static const V kPalette[6] = {V(0.75f, 0.75f, 0.75f), V(0.8f, 0.55f, 0.4f), V(0.45f, 0.65f, 0.8f),
-                                V(0.6f, 0.8f, 0.45f),   V(0.85f, 0.8f, 0.5f), V(0.7f, 0.5f, 0.75f)};
+// The meshes in config order, then bt_scene_finalize's degeneracy rule;
+// each surviving triangle keeps its material.
+bool build(bt_scene_file& f, std::string& why) {
   Mesh& s = f.mesh;
-  int index = 0;
   try {
-    for (const std::string& ml : f.meshLines) {
-      const auto t = words(ml);
-      if (t.size() < 2) {
-        err = "bad mesh line: " + ml;
-        return false;
-      }
-      float scale = 1;
-      V translate, color = kPalette[index % 6];
-      Params params;
-      for (size_t i = 2; i < t.size(); ++i) {
-        if (t[i] == "scale" && i + 1 < t.size()) {
-          scale = float(std::stod(t[++i]));
-        } else if (t[i] == "translate" && i + 3 < t.size()) {
-          translate = V(float(std::stod(t[i + 1])), float(std::stod(t[i + 2])), float(std::stod(t[i + 3])));
-          i += 3;
-        } else if (t[i] == "color" && i + 3 < t.size()) {
-          color = V(float(std::stod(t[i + 1])), float(std::stod(t[i + 2])), float(std::stod(t[i + 3])));
-          i += 3;
-        } else if (t[i].find('=') != std::string::npos) {
-          const size_t e = t[i].find('=');
-          params[t[i].substr(0, e)] = t[i].substr(e + 1);
-        }
-      }
-      const size_t first = s.pos.size();
-      bool ok;
-      if (t[0] == "obj") {
-        ok = loadObj(t[1], s, s.material(color), err);
-      } else if (t[0] == "ply") {
-        ok = loadPly(t[1], s, s.material(color), err);
-      } else if (t[0] == "procedural") {
-        ok = procedural(t[1], params, s, err);
-      } else {
-        err = "unknown mesh type " + t[0];
-        return false;
-      }
-      if (!ok) return false;
-      for (size_t i = first; i < s.pos.size(); ++i) s.pos[i] = s.pos[i] * scale + translate;
-      ++index;
-    }
+    for (size_t i = 0; i < f.meshes.size(); ++i)
+      if (!addMesh(s, f.meshes[i], int(i), why)) return false;
   } catch (const std::exception& e) {
-    err = std::string("mesh parameters: ") + e.what();
+    why = e.what();
     return false;
   }
-  // degenerate triangles out (bt_scene_finalize's rule; it keeps the order,
-  // so the kept triangles are matched back to their materials in one walk)
+  // bt_scene_finalize keeps the order of the triangles it keeps, so one walk
+  // matches them back to their materials
   const int64_t nt = int64_t(s.mat.size());
   std::vector<uint32_t> kept(size_t(3 * std::max<int64_t>(nt, 1)));
   std::vector<float> nrm(kept.size()), area(size_t(std::max<int64_t>(nt, 1)));
@@ -760,7 +934,7 @@ bool build(bt_scene_file& f, std::string& err) {
                                             nrm.data(), area.data(), bounds)
                         : 0;
   if (nk < 0) {
-    err = "triangle index out of range";
+    why = "triangle index out of range";
     return false;
   }
   std::vector<uint16_t> mat;
@@ -775,7 +949,7 @@ bool build(bt_scene_file& f, std::string& err) {
   s.mat.swap(mat);
   if (s.colors.empty()) s.material(V(0.75f, 0.75f, 0.75f));
   if (nk == 0) {
-    err = "scene has no triangles";
+    why = "the config yields no triangles";
     return false;
   }
   return true;
@@ -789,17 +963,17 @@ bt_scene_file* fresh() {
   return f;
 }
 
-int make(const std::string& text, const std::string& path, bt_scene_file** out) {
+int make(std::string_view text, const std::string& path, bt_scene_file** out) {
   *out = nullptr;
   bt_scene_file* f = fresh();
-  std::string err;
-  if (!parse(text, *f, err)) {
-    btSetError((path.empty() ? err : path + ": " + err).c_str());
+  std::string why;
+  if (!parse(text, *f, why)) {
+    btSetError((path.empty() ? why : path + ": " + why).c_str());
     delete f;
     return BT_ERR_INVALID;
   }
-  if (!build(*f, err)) {
-    btSetError(err.c_str());
+  if (!build(*f, why)) {
+    btSetError(why.c_str());
     delete f;
     return BT_ERR_INVALID;
   }
@@ -822,8 +996,8 @@ int bt_scene_load_config(const char* path, bt_scene_file** out) {
   if (!path || !out) return BT_ERR_INVALID;
   *out = nullptr;
   std::string text;
-  if (!slurp(path, text)) {
-    btSetError((std::string("cannot open config ") + path).c_str());
+  if (!readWholeFile(path, text)) {
+    btSetError((std::string("could not read config file ") + path).c_str());
     return BT_ERR_INVALID;
   }
   return make(text, path, out);

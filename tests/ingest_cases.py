@@ -110,16 +110,17 @@ def configs(p: dict) -> dict:
     }
 
 
-# config text -> a phrase the rejection message contains (both sides reject)
+# config text -> (a phrase of the reference's rejection, a phrase of ours):
+# both sides reject the config for the same reason, each in its own words
 ERRORS = {
-    "bogus 1 2 3\n": "unknown key 'bogus'",
-    "view 1 2 3\n": "expected 7 numbers after 'view'",
-    "mesh procedural room\nup 0 x 1\n": "line 2",
-    "mesh stl part.stl\n": "unknown mesh type stl",
-    "mesh procedural teapot\n": "unknown procedural scene 'teapot'",
-    "mesh obj /nonexistent/part.obj\n": "cannot read",
-    "view 0 0 1 0 0 0 60\n": "scene has no triangles",
-    "mesh obj\n": "bad mesh line",
+    "bogus 1 2 3\n": ("unknown key 'bogus'", "line 1: 'bogus' is not a config key"),
+    "view 1 2 3\n": ("expected 7 numbers after 'view'", "line 1: 'view' takes 7 numbers, got 3"),
+    "mesh procedural room\nup 0 x 1\n": ("line 2", "line 2: 'x' is not a number"),
+    "mesh stl part.stl\n": ("unknown mesh type stl", "mesh kind 'stl' is not obj, ply or procedural"),
+    "mesh procedural teapot\n": ("unknown procedural scene 'teapot'", "no procedural scene named 'teapot'"),
+    "mesh obj /nonexistent/part.obj\n": ("cannot read", "could not open mesh file /nonexistent/part.obj"),
+    "view 0 0 1 0 0 0 60\n": ("scene has no triangles", "the config yields no triangles"),
+    "mesh obj\n": ("bad mesh line", "mesh line 'obj' names no file or scene"),
 }
 
 

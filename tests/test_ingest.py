@@ -82,21 +82,21 @@ def test_full_building_config_matches_reference(native_lib, oracle_ready):
     _same_as_reference(sf, ref_config(text))
 
 
-@pytest.mark.parametrize("text,phrase", list(cases.ERRORS.items()))
-def test_rejected_configs(native_lib, text, phrase):
+@pytest.mark.parametrize("text,phrases", list(cases.ERRORS.items()))
+def test_rejected_configs(native_lib, text, phrases):
     from beamtrace2007_b200._native import BtError
     from beamtrace2007_b200.ingest import parse_config
     with pytest.raises(BtError) as e:
         parse_config(text)
-    assert phrase in str(e.value)
+    assert phrases[1] in str(e.value)
 
 
-@pytest.mark.parametrize("text,phrase", list(cases.ERRORS.items()))
-def test_reference_rejects_the_same_configs(oracle_ready, text, phrase):
+@pytest.mark.parametrize("text,phrases", list(cases.ERRORS.items()))
+def test_reference_rejects_the_same_configs(oracle_ready, text, phrases):
     from ref import ref_config
     with pytest.raises(ValueError) as e:
         ref_config(text)
-    assert phrase in str(e.value)
+    assert phrases[0] in str(e.value)
 
 
 def test_bad_mesh_files(native_lib, tmp_path):
@@ -108,13 +108,13 @@ def test_bad_mesh_files(native_lib, tmp_path):
         parse_config(f"mesh ply {bad}\n")
     odd = tmp_path / "odd.ply"
     odd.write_text("ply\nformat binary_middle_endian 1.0\nelement vertex 0\nend_header\n")
-    with pytest.raises(BtError, match="unsupported PLY format"):
+    with pytest.raises(BtError, match="encoding 'binary_middle_endian' is not supported"):
         parse_config(f"mesh ply {odd}\n")
     empty = tmp_path / "empty.obj"
     empty.write_text("# nothing\n")
-    with pytest.raises(BtError, match="no vertices"):
+    with pytest.raises(BtError, match="holds no vertex positions"):
         parse_config(f"mesh obj {empty}\n")
-    with pytest.raises(BtError, match="cannot open config"):
+    with pytest.raises(BtError, match="could not read config file"):
         load_config(str(tmp_path / "missing.cfg"))
 
 
