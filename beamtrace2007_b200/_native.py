@@ -81,7 +81,7 @@ class GpuConfig(C.Structure):
                 ("capacity", C.c_int64), ("blocks_per_sm", C.c_int32), ("kernel_timing", C.c_int32),
                 ("max_retries", C.c_int32), ("tail_records", C.c_int64),
                 ("eps_stats", C.c_int32), ("yield_pct", C.c_int32),
-                ("fuse_primary", C.c_int32)]
+                ("fuse_primary", C.c_int32), ("eps_fp64", C.c_int32)]
 
 
 class SoftOpts(C.Structure):
@@ -102,7 +102,8 @@ class RunInfo(C.Structure):
                 ("ms_round", C.c_double), ("launches", C.c_int32), ("round_launches", C.c_int32),
                 ("passes", C.c_int32), ("retried_roots", C.c_int32), ("max_spill", C.c_int32),
                 ("roots", C.c_int64), ("rounds", C.c_int32), ("tail_rounds", C.c_int32), ("ms_kernel_admit", C.c_double),
-                ("ms_kernel_trace", C.c_double), ("ms_kernel_clip", C.c_double), ("yields", C.c_int64)]
+                ("ms_kernel_trace", C.c_double), ("ms_kernel_clip", C.c_double), ("yields", C.c_int64),
+                ("overflow_roots", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -111,6 +112,36 @@ class RunInfo(C.Structure):
 class Polys(C.Structure):
     _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("n", C.c_void_p), ("tri", C.c_void_p), ("area", C.c_void_p),
                 ("root", C.c_void_p), ("cap", C.c_int64)]
+
+
+BT_REQ_SOFT, BT_REQ_PRIMARY_IDS, BT_REQ_POINT_MASK = 0, 1, 2
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("scene", C.c_int32), ("cam", Camera), ("light", AreaLight), ("opts", SoftOpts),
+                ("point_light", C.c_float * 3), ("cull", C.c_int32), ("tile", C.c_int32), ("tri", C.c_void_p),
+                ("vis", C.c_void_p), ("E", C.c_void_p), ("Eu", C.c_void_p), ("mask", C.c_void_p),
+                ("user", C.c_uint64)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("user", C.c_uint64), ("kind", C.c_int32), ("status", C.c_int32),
+                ("ms_queued", C.c_double), ("ms_total", C.c_double), ("error", C.c_char * 160)]
+
+
+class ServeConfig(C.Structure):
+    _fields_ = [("vis_lanes", C.c_int32), ("soft_jobs", C.c_int32), ("soft_pixels", C.c_int64),
+                ("capacity", C.c_int64), ("fold_ms", C.c_double), ("memory_budget", C.c_int64)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("refused", C.c_int64), ("queued", C.c_int64),
+                ("running", C.c_int64), ("soft_runs", C.c_int64), ("soft_folded", C.c_int64),
+                ("scene_bytes", C.c_int64), ("lane_bytes", C.c_int64), ("queue_high_water", C.c_int64),
+                ("admitted_bytes", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _P = C.c_void_p
@@ -162,6 +193,10 @@ SIGNATURES = {
     "bt_gpu_point_mask_device": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, _P, _P,
                                       C.POINTER(RunInfo)]),
     "bt_gpu_raster": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, C.POINTER(Polys), _I64, _P, _P]),
+    "bt_gpu_serve_start": (_I, [_P, C.POINTER(ServeConfig)]),
+    "bt_gpu_submit": (_I, [_P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "bt_gpu_poll": (_I, [_P, C.POINTER(Completion), C.c_int32, C.POINTER(C.c_int32), C.c_int32]),
+    "bt_gpu_serve_stats": (_I, [_P, C.POINTER(ServeStats)]),
 }
 
 _lib = None

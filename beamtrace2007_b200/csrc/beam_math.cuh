@@ -239,10 +239,43 @@ BT_HD Line makeLine(float a, float b, float c, float ext) {
   return L;
 }
 
+// An edge line in FP64 (the opt-in band re-decision, eps_fp64): the same
+// line as the float one -- from the same float vertices and apex, in the
+// same canonical orientation -- with every operation in double, normalised
+// to unit (a, b).  ok = 0 where the float line is not a plain edge (a
+// constant line) or the FP64 one is degenerate: no re-decision then.
+struct Line64 {
+  double a, b, c;
+  int ok;
+  BT_HD double eval(float x, float y) const { return double(x) * a + double(y) * b + c; }
+};
+
+// Side of a point at float distance d from line L: +1 / -1 outside the
+// fuzzy band, 0 inside it; with l64 (F64), a point inside the float band
+// takes the side of its FP64 distance when that lies outside the band, and
+// *dq carries that distance (as float) for crossing interpolation.
+template <bool F64>
+BT_HD int bandSide(float d, float x, float y, float eps, const Line64* l64, float* dq) {
+  const int s = d > eps ? 1 : (d < -eps ? -1 : 0);
+  if (!F64 || s != 0 || !l64 || !l64->ok) return s;
+  const double d64 = l64->eval(x, y);
+  if (d64 > double(eps)) {
+    *dq = float(d64);
+    return 1;
+  }
+  if (d64 < -double(eps)) {
+    *dq = float(d64);
+    return -1;
+  }
+  return 0;
+}
+
 // Fuzzy split of convex p by L; crossings computed from the
-// lexicographically smaller endpoint (beam_geom.h:83-114).
-template <int N>
-BT_CLIP bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out) {
+// lexicographically smaller endpoint (beam_geom.h:83-114).  F64: band
+// vertices re-decided by l64 (bandSide).
+template <int N, bool F64 = false>
+BT_CLIP bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, Poly<N>& out,
+                       const Line64* l64 = nullptr) {
   in.clear();
   out.clear();
   float d[N];
@@ -253,7 +286,7 @@ BT_CLIP bool splitPoly(const Poly<N>& p, const Line& L, float eps, Poly<N>& in, 
     side[i] = 0;
     if (i < p.n) {
       d[i] = L.eval(p.x[i], p.y[i]);
-      side[i] = d[i] > eps ? 1 : (d[i] < -eps ? -1 : 0);
+      side[i] = bandSide<F64>(d[i], p.x[i], p.y[i], eps, l64, &d[i]);
     }
   }
   BT_UNROLL for (int i = 0; i < N; ++i) {
@@ -327,15 +360,16 @@ BT_CLIP void cleanPoly(Poly<N>& p, float epsSplit) {
 
 // Bit 0: some vertex strictly inside; bit 1: some vertex strictly outside
 // (beam_core.h:69-78).
-template <int N>
-BT_HD int classifyPoly(const Poly<N>& p, const Line& L, float eps) {
+template <int N, bool F64 = false>
+BT_HD int classifyPoly(const Poly<N>& p, const Line& L, float eps, const Line64* l64 = nullptr) {
   int c = 0;
   BT_UNROLL for (int i = 0; i < N; ++i) {
     if (i < p.n) {
       float d = L.eval(p.x[i], p.y[i]);
-      if (d > eps)
+      const int s = bandSide<F64>(d, p.x[i], p.y[i], eps, l64, &d);
+      if (s > 0)
         c |= 1;
-      else if (d < -eps)
+      else if (s < 0)
         c |= 2;
     }
   }
@@ -598,6 +632,42 @@ BT_HD void triSetup(const Query& q, V3 v0, V3 v1, V3 v2, V3 nT, const uint32_t* 
   ti.ok = 1;
 }
 
+// An edge line of a triangle in FP64 (Line64), oriented as triSetup orients
+// the float one: the plane through the apex and the edge's vertices vi, vj
+// taken in canonical vertex order (fwd: vi's index is the smaller), times
+// the sign sg of the orientation test.  fl: the float line (a constant one
+// gets no FP64 twin).
+BT_HD Line64 edgeLine64(const Query& q, V3 vi, V3 vj, bool fwd, float sg, const Line& fl) {
+  double ri[3], rj[3];
+  for (int a = 0; a < 3; ++a) {
+    ri[a] = double(comp(vi, a)) - double(comp(q.P.O, a));
+    rj[a] = double(comp(vj, a)) - double(comp(q.P.O, a));
+  }
+  const double* p0 = fwd ? ri : rj;
+  const double* p1 = fwd ? rj : ri;
+  const double m[3] = {p0[1] * p1[2] - p0[2] * p1[1], p0[2] * p1[0] - p0[0] * p1[2], p0[0] * p1[1] - p0[1] * p1[0]};
+  const double f = fwd ? double(sg) : -double(sg);
+  const double a = f * (m[0] * double(q.P.u.x) + m[1] * double(q.P.u.y) + m[2] * double(q.P.u.z));
+  const double b = f * (m[0] * double(q.P.v.x) + m[1] * double(q.P.v.y) + m[2] * double(q.P.v.z));
+  const double c = f * (m[0] * double(q.P.d.x) + m[1] * double(q.P.d.y) + m[2] * double(q.P.d.z));
+  const double nrm = sqrt(a * a + b * b);
+  Line64 e;
+  e.ok = (fl.a != 0.f || fl.b != 0.f) && nrm > 0;
+  e.a = e.ok ? a / nrm : 0;
+  e.b = e.ok ? b / nrm : 0;
+  e.c = e.ok ? c / nrm : 0;
+  return e;
+}
+
+// The three edge lines of a triangle (vertices v0..v2 with indices T) in
+// FP64, edge k from vertex k to k + 1; fl: the float edge lines.
+BT_HD void edgeLines64(const Query& q, V3 v0, V3 v1, V3 v2, const uint32_t* T, float sg, const Line* fl,
+                       Line64* e) {
+  e[0] = edgeLine64(q, v0, v1, T[0] < T[1], sg, fl[0]);
+  e[1] = edgeLine64(q, v1, v2, T[1] < T[2], sg, fl[1]);
+  e[2] = edgeLine64(q, v2, v0, T[2] < T[0], sg, fl[2]);
+}
+
 // Hit plane of triangle t (BeamCtx::hitPlane, beam_core.h:290-297).
 BT_HD void hitPlane(const Query& q, V3 nT, V3 v0, float* A, float& C) {
   A[0] = dot(nT, q.P.u);
@@ -655,13 +725,17 @@ BT_HD bool separated(const Query& q, const Beam& b, const TriInfo& ti) {
   return outAll != 0;
 }
 
-// Fuzzy 4-corner vote (BeamCtx::testLine, beam_core.h:356-362).
-BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, int& nl, bool& allIn) {
+// Fuzzy 4-corner vote (BeamCtx::testLine, beam_core.h:356-362); F64: band
+// corners re-decided by l64.
+template <bool F64 = false>
+BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, int& nl, bool& allIn,
+                    const Line64* l64 = nullptr) {
   bool anyIn = false, anyOut = false;
   for (int k = 0; k < 4; ++k) {
     float dv = B.qx[k] * line.a + B.qy[k] * line.b + line.c;
-    anyIn |= dv > q.eps;
-    anyOut |= dv < -q.eps;
+    const int sd = bandSide<F64>(dv, B.qx[k], B.qy[k], q.eps, l64, &dv);
+    anyIn |= sd > 0;
+    anyOut |= sd < 0;
   }
   if (!anyIn) return false;
   if (anyOut) allIn = false;
@@ -671,12 +745,15 @@ BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, in
 
 // The cheap beam-triangle tests: trivial cases, depth line, far plane
 // (BeamCtx::classifyTri, beam_core.h:374-409).  The current hit's plane
-// comes from the beam (hitA, hitC, hitN).
-BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl) {
+// comes from the beam (hitA, hitC, hitN).  F64: the edge votes re-decide
+// band corners with the FP64 edge lines e64.
+template <bool F64 = false>
+BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl,
+                        const Line64* e64 = nullptr) {
   nl = 0;
   bool allIn = true;
   for (int k = 0; k < 3; ++k)
-    if (!testLine(q, B, ti.edge[k], L, nl, allIn)) return kTriKeep;
+    if (!testLine<F64>(q, B, ti.edge[k], L, nl, allIn, F64 ? &e64[k] : nullptr)) return kTriKeep;
   if (q.mode == kModeNearest && B.hit >= 0) {
     if (!testLine(q, B, closerLine(q, ti, B.hitA, B.hitC, B.hitN, B.hit), L, nl, allIn)) return kTriKeep;
   }
@@ -703,10 +780,17 @@ BT_HD Line lineAt(const Line* L, int li) {
   return r;
 }
 
-template <int N, class Sink>
-BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sink& sink, uint32_t& fiveSplits) {
+template <int N, class Sink, bool F64 = false>
+BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sink& sink, uint32_t& fiveSplits,
+                     const Line64* e64in = nullptr) {
   Line L[5];
   BT_UNROLL for (int k = 0; k < 5; ++k) L[k] = Lin[k];
+  Line64 E[3];  // F64: the edge lines' FP64 twins, kept in the order of L[0..2]
+  if (F64) {
+    E[0] = e64in[0];
+    E[1] = e64in[1];
+    E[2] = e64in[2];
+  }
   {
     float score[3];
     BT_UNROLL for (int k = 0; k < 3; ++k) {
@@ -725,6 +809,11 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
       Line tl = L[0];
       L[0] = L[1];
       L[1] = tl;
+      if (F64) {
+        const Line64 te = E[0];
+        E[0] = E[1];
+        E[1] = te;
+      }
     }
     if (score[2] < score[1]) {
       float ts = score[1];
@@ -733,6 +822,11 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
       Line tl = L[1];
       L[1] = L[2];
       L[2] = tl;
+      if (F64) {
+        const Line64 te = E[1];
+        E[1] = E[2];
+        E[2] = te;
+      }
       if (score[1] < score[0]) {
         ts = score[0];
         score[0] = score[1];
@@ -740,6 +834,11 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
         tl = L[0];
         L[0] = L[1];
         L[1] = tl;
+        if (F64) {
+          const Line64 te = E[0];
+          E[0] = E[1];
+          E[1] = te;
+        }
       }
     }
   }
@@ -759,7 +858,11 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
     bool inside = true;
     for (; li < nl; ++li) {
       const Line Lk = lineAt(L, li);
-      int c = classifyPoly(p, Lk, q.eps);
+      // F64: the edge lines (the first three) re-decide band vertices
+      Line64 Ek;
+      Ek.ok = 0;
+      if (F64 && li < 3) Ek = li == 0 ? E[0] : (li == 1 ? E[1] : E[2]);
+      int c = classifyPoly<N, F64>(p, Lk, q.eps, &Ek);
       if (!(c & 2)) continue;
       if (!(c & 1)) {
         if (!sink.push(0, p)) ok = false;
@@ -767,7 +870,7 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
         break;
       }
       Poly<N> in, out;
-      if (!splitPoly(p, Lk, q.eps, in, out)) return false;
+      if (!splitPoly<N, F64>(p, Lk, q.eps, in, out, &Ek)) return false;
       cleanPoly(out, q.eps);
       if (out.n >= 3 && !sink.push(0, out)) ok = false;
       cleanPoly(in, q.eps);

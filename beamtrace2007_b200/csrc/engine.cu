@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -30,11 +31,13 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
 #include "bt_gpu.h"
 #include "engine_core.cuh"
+#include "serve_engine.h"
 
 using namespace btg;
 
@@ -701,7 +704,8 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
 // Returns true if nothing
 // measurable changed and the record (updated in place) continues at the next
 // triangle.  Works on its own query and beam: the caller's stay in registers.
-template <int App>
+// F64: band corners of the edge lines re-decided in FP64 (eps_fp64).
+template <int App, bool F64 = false>
 __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Stats* cs, SubBeam* keep = nullptr,
                                         bool* kept = nullptr) {
   Stats& st = *cs;
@@ -721,7 +725,8 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   int nl = 0;
   bool commit = false;
   PieceLog log;
-  const int slots = splitPass1<SplitEnv<App>>(p.s, q, rec, b, st, ti, L, nl, commit, &log);
+  Line64 e64[3];
+  const int slots = splitPass1<SplitEnv<App>, F64>(p.s, q, rec, b, st, ti, L, nl, commit, &log, e64);
   if (slots < 0) {
     killRoot(p, root);
     liveSub(p, root, 1);
@@ -749,10 +754,11 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   // `slots` pieces at most: one may stay with the lane (tail rounds), the
   // rest take reserved queue slots
   env.reserve(keep ? slots - 1 : slots);
-  splitPass2(q, rec, b, ti, L, nl, env, st, &log);
+  splitPass2<SplitEnv<App>, F64>(q, rec, b, ti, L, nl, env, st, &log, e64);
   // slivers dropped by beamGeom were counted in `slots` but never queued
-  // (nor kept)
-  const int unused = env.finish() + (keep && !env.kept ? 1 : 0);
+  // (nor kept); with no piece at all (slots = 0) there was no kept slot to
+  // give back: the record itself was already taken off by the add above
+  const int unused = env.finish() + (keep && slots > 0 && !env.kept ? 1 : 0);
   if (kept) *kept = env.kept;
   if (unused > 0) liveSub(p, root, unused);
   return false;
@@ -811,7 +817,7 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // 170 registers; at 4 CTAs it spills, which costs more than the warps gain.
 // The tail-round variant clips inline with its polygons in registers and
 // takes 2 CTAs per SM: tail rounds hold too few records to need more warps.)
-template <int App, bool Fused, bool EpsLog = false>
+template <int App, bool Fused, int Mode = kVoteFloat>
 __global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
@@ -898,7 +904,7 @@ __global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __g
       int occ = -1;
       if (res == kStepContinue) {
         for (;;) {
-          res = testOne<EpsLog>(p.s, q, r, b, st, occ);
+          res = testOne<Mode>(p.s, q, r, b, st, occ);
           if (res != kStepContinue || !moreInLeaf(p.s, q, r)) break;
         }
       }
@@ -921,7 +927,7 @@ __global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __g
         bool hasKept = false;
         Stats cs;
         cs.clear();
-        if (clipRecord<App>(p, &r, &cs, &kept, &hasKept)) {
+        if (clipRecord<App, Mode == kVoteFp64>(p, &r, &cs, &kept, &hasKept)) {
           w.phase = kPhTest;  // nothing changed measurably: the next triangle
         } else if (hasKept) {
           r = kept;
@@ -978,7 +984,7 @@ __global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __g
 // Clip: one lane per record of the clip queue; pieces go to the next
 // round's trace queue.  A record whose clip changes nothing measurable
 // continues at its next triangle in the next round.
-template <int App>
+template <int App, bool F64 = false>
 // (At least 4 CTAs per SM, i.e. at most 128 registers: with its polygons
 // in registers the clip step would take 255 and run 2 CTAs per SM; 4 keeps
 // enough warps for its latency and spills little -- measured 3 and 6 too.)
@@ -1004,7 +1010,7 @@ __global__ void __launch_bounds__(kThreads, 4) clipKernel(const __grid_constant_
       SubBeam rec = p.cq[i];
       Stats cs;
       cs.clear();
-      if (clipRecord<App>(p, &rec, &cs)) {
+      if (clipRecord<App, F64>(p, &rec, &cs)) {
         const int at = queueAppend(p, p.cur ^ 1, 1);
         if (at >= 0) p.tq[p.cur ^ 1][at] = rec;
       }
@@ -1273,6 +1279,16 @@ struct bt_gpu_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t rev[2] = {nullptr, nullptr};
   cudaEvent_t kev[32] = {};  // kernel_timing: 2 per round of a batch, around the trace kernel
+  // serving (serve.cpp): a lane views its parent's scene pool and owns only
+  // its engine buffers; the parent's scene lock is held shared while a lane
+  // works and exclusively while bt_gpu_add_scene replaces the arrays
+  bt_gpu_ctx* parent = nullptr;
+  bool ownsScene = true;
+  std::shared_mutex sceneLock;
+  void* serving = nullptr;       // the serving state of bt_gpu_submit / bt_gpu_poll
+  int32_t* dRanges = nullptr;    // streaming runs: root ranges of the jobs checked for completion
+  int* dJobCounts = nullptr;     // and their live / abandoned root counts
+  std::atomic<int64_t> queueHighWater{0};  // largest trace queue a lane has needed (records)
 };
 
 // For the host-side modules of the library (ingest.cpp): sets the message
@@ -1295,6 +1311,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->eps_stats = 0;
   c->yield_pct = 0;
   c->fuse_primary = 0;
+  c->eps_fp64 = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1418,53 +1435,78 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
 // 16x budget.
 constexpr int kRoundsPerCheck = 8;
 
+// The FP64 band re-decision is compiled for soft shadows only; the other
+// applications map it to the float votes (their kernels are not built twice).
 template <int App>
-int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info) {
-  int e = ensureRoots(c, size_t(R));
-  if (e) return e;
-  CK(cudaMemsetAsync(c->dAttempt, 0, sizeof(int32_t) * size_t(R), c->stream));
-  CK(cudaMemsetAsync(c->dStats, 0, sizeof(unsigned long long) * kNumStats, c->stream));
-  CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
-  app.missFx = c->dMiss;
-  app.gFx = c->dG;
-  app.shade = c->dShade;
+constexpr int kVoteFp64F = App == kAppSoft ? kVoteFp64 : kVoteFloat;
+
+template <int App>
+struct RoundRunner {
+  bt_gpu_ctx* c;
+  bt_run_info* info;
   RoundParams p;
-  p.s = c->s;
-  p.tq[0] = c->dQ[0];
-  p.tq[1] = c->dQ[1];
-  p.cq = c->dQ[2];
-  p.capacity = c->capacity;
-  p.roots = c->dRoots;
-  p.rootCap = R;
-  p.live = c->dLive;
-  p.state = c->dState;
-  p.attempt = c->dAttempt;
-  p.ctr = c->dCtr;
-  p.stats = c->dStats;
-  p.app = app;
-  // eps_stats: the trace kernels that also log the fuzzy-band votes
-  const bool epsLog = c->cfg.eps_stats != 0;
-  const int gA = gridFor(c, admitKernel<App>),
-            gT = epsLog ? gridFor(c, traceKernel<App, false, true>) : gridFor(c, traceKernel<App, false>),
-            gC = gridFor(c, clipKernel<App>),
-            gF = epsLog ? gridFor(c, traceKernel<App, true, true>) : gridFor(c, traceKernel<App, true>);
-  // tail rounds: every root admitted and fewer queued records than this
-  // (default: a sixth of the trace grid's lanes, about two warps' worth per SM -- the fused kernel clips
-  // inside the divergent walk, which only pays once the queue no longer fills the GPU)
-  const int64_t tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads / 6;
-  const int yieldPct = c->cfg.yield_pct == 0 ? 50 : std::min(c->cfg.yield_pct, 100);
-  const int yieldAt = yieldPct < 0 ? INT_MAX : std::max(1, int(int64_t(gT) * kWarps * yieldPct / 100));
-  static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
-  const bool ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
-  // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics).
-  FILE* roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
-  int launches = 0, passes = 0, retried = 0, roundsRun = 0, tailRounds = 0;
+  int mode = kVoteFloat;
+  bool ktime = false;
+  int gA = 0, gT = 0, gC = 0, gF = 0, yieldAt = INT_MAX;
+  int64_t tailRecords = 0;
+  FILE* roundLog = nullptr;  // BT_ROUND_LOG=1: one line per batch of rounds on stderr (diagnostics)
+  int launches = 0, passes = 0, retried = 0, roundsRun = 0, tailRounds = 0, pass = -1, round = 0;
   int64_t yieldsRun = 0;
-  const int32_t* list = nullptr;
-  int n = R;
   Counters hc;
-  memset(&hc, 0, sizeof hc);
-  for (int pass = 0;; ++pass) {
+
+  RoundRunner(bt_gpu_ctx* ctx, bt_run_info* inf) : c(ctx), info(inf) { memset(&hc, 0, sizeof hc); }
+
+  // Clears the per-run state of R roots and sets the launch parameters.
+  int begin(const AppParams& app0, int R) {
+    int e = ensureRoots(c, size_t(R));
+    if (e) return e;
+    CK(cudaMemsetAsync(c->dAttempt, 0, sizeof(int32_t) * size_t(R), c->stream));
+    CK(cudaMemsetAsync(c->dStats, 0, sizeof(unsigned long long) * kNumStats, c->stream));
+    CK(cudaMemsetAsync(c->dCtr, 0, sizeof(Counters), c->stream));
+    AppParams app = app0;
+    app.missFx = c->dMiss;
+    app.gFx = c->dG;
+    app.shade = c->dShade;
+    p.s = c->s;
+    p.tq[0] = c->dQ[0];
+    p.tq[1] = c->dQ[1];
+    p.cq = c->dQ[2];
+    p.capacity = c->capacity;
+    p.roots = c->dRoots;
+    p.rootCap = R;
+    p.live = c->dLive;
+    p.state = c->dState;
+    p.attempt = c->dAttempt;
+    p.ctr = c->dCtr;
+    p.stats = c->dStats;
+    p.app = app;
+    // the edge votes: eps_fp64 (soft shadows) re-decides fuzzy-band corners
+    // in FP64, eps_stats logs them, else the reference's float votes
+    mode = (App == kAppSoft && c->cfg.eps_fp64) ? kVoteFp64 : (c->cfg.eps_stats ? kVoteLog : kVoteFloat);
+    gA = gridFor(c, admitKernel<App>);
+    gT = mode == kVoteFp64 ? gridFor(c, traceKernel<App, false, kVoteFp64F<App>>)
+         : mode == kVoteLog ? gridFor(c, traceKernel<App, false, kVoteLog>)
+                            : gridFor(c, traceKernel<App, false>);
+    gC = mode == kVoteFp64 ? gridFor(c, clipKernel<App, App == kAppSoft>) : gridFor(c, clipKernel<App>);
+    gF = mode == kVoteFp64 ? gridFor(c, traceKernel<App, true, kVoteFp64F<App>>)
+         : mode == kVoteLog ? gridFor(c, traceKernel<App, true, kVoteLog>)
+                            : gridFor(c, traceKernel<App, true>);
+    // tail rounds: every root admitted and fewer queued records than this
+    // (default: a sixth of the trace grid's lanes, about two warps' worth per SM -- the fused kernel clips
+    // inside the divergent walk, which only pays once the queue no longer fills the GPU)
+    tailRecords = c->cfg.tail_records > 0 ? c->cfg.tail_records : int64_t(gT) * kThreads / 6;
+    const int yieldPct = c->cfg.yield_pct == 0 ? 50 : std::min(c->cfg.yield_pct, 100);
+    yieldAt = yieldPct < 0 ? INT_MAX : std::max(1, int(int64_t(gT) * kWarps * yieldPct / 100));
+    static_assert(2 * kRoundsPerCheck <= 32, "kernel_timing events");
+    ktime = c->cfg.kernel_timing && c->kev[0] != nullptr;
+    roundLog = getenv("BT_ROUND_LOG") ? stderr : nullptr;
+    return BT_OK;
+  }
+
+  // Starts the next pass over `n` roots (the first `n`, or `list`) with a
+  // live sub-beam budget of `budget` per root.
+  int startPass(int n, const int32_t* list, int budget) {
+    ++pass;
     p.budget = budget;
     p.reserve = std::max(budget, 32);
     if (int64_t(p.reserve) > c->capacity) {
@@ -1481,88 +1523,117 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
       z.outCount = hc.outCount;
       z.maxQueue = hc.maxQueue;
       CK(cudaMemcpyAsync(c->dCtr, &z, sizeof z, cudaMemcpyHostToDevice, c->stream));
+      hc = z;
     }
     ++passes;
-    for (int round = 0;;) {
-      CK(cudaEventRecord(c->rev[0], c->stream));
-      // the mode of this batch of rounds, from the counters of the last one
-      const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
-                        c->cfg.tail_records >= 0;
-      for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
-        p.cur = round & 1;
-        if (tail) {
-          if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
-          if (epsLog)
-            traceKernel<App, true, true><<<gF, kThreads, 0, c->stream>>>(p);
-          else
-            traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
-          if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
-          launches += 2;
-          tailRounds++;
-        } else {
-          admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
-          if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
-          if (epsLog)
-            traceKernel<App, false, true><<<gT, kThreads, 0, c->stream>>>(p);
-          else
-            traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
-          if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+    round = 0;
+    return BT_OK;
+  }
+
+  // More roots for the running pass (numRoots grew): a pass that had
+  // finished goes on.
+  int reopen() {
+    if (!hc.done) return BT_OK;
+    const int zero = 0;
+    CK(cudaMemcpyAsync(&c->dCtr->done, &zero, sizeof zero, cudaMemcpyHostToDevice, c->stream));
+    hc.done = 0;
+    return BT_OK;
+  }
+
+  // One batch of kRoundsPerCheck rounds, then the counters.
+  int batch() {
+    const int n = p.numRoots;
+    CK(cudaEventRecord(c->rev[0], c->stream));
+    // the mode of this batch of rounds, from the counters of the last one
+    const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
+                      c->cfg.tail_records >= 0;
+    for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
+      p.cur = round & 1;
+      if (tail) {
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+        if (mode == kVoteFp64)
+          traceKernel<App, true, kVoteFp64F<App>><<<gF, kThreads, 0, c->stream>>>(p);
+        else if (mode == kVoteLog)
+          traceKernel<App, true, kVoteLog><<<gF, kThreads, 0, c->stream>>>(p);
+        else
+          traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+        launches += 2;
+        tailRounds++;
+      } else {
+        admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+        if (mode == kVoteFp64)
+          traceKernel<App, false, kVoteFp64F<App>><<<gT, kThreads, 0, c->stream>>>(p);
+        else if (mode == kVoteLog)
+          traceKernel<App, false, kVoteLog><<<gT, kThreads, 0, c->stream>>>(p);
+        else
+          traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
+        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+        if (mode == kVoteFp64)
+          clipKernel<App, App == kAppSoft><<<gC, kThreads, 0, c->stream>>>(p);
+        else
           clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
-          launches += 4;
-        }
-        roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
+        launches += 4;
       }
-      CK(cudaEventRecord(c->rev[1], c->stream));
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-      float ms = 0;
-      cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
-      if (info) {
-        info->ms_round += ms;
-        info->round_launches += 3 * kRoundsPerCheck;
-        if (ktime)
-          for (int k = 0; k < kRoundsPerCheck; ++k) {
-            float t = 0;
-            CK(cudaEventElapsedTime(&t, c->kev[2 * k], c->kev[2 * k + 1]));
-            info->ms_kernel_trace += t;
-          }
-      }
-      if (roundLog)
-        fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d yields %d ms %.3f\n", pass,
-                hc.rounds, hc.inflight, hc.rootNext, n, hc.count[round & 1], hc.yields, ms);
-      if (hc.error) {
-        setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam queue overflow (capacity %d)", c->capacity);
-        return BT_ERR_CAPACITY;
-      }
-      if (hc.done) break;
-      if (launches > kMaxLaunches) {
-        setErr("launch limit reached with %d roots in flight", hc.inflight);
-        return BT_ERR_TIMEOUT;
-      }
+      roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
     }
+    CK(cudaEventRecord(c->rev[1], c->stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&hc, c->dCtr, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
+    if (info) {
+      info->ms_round += ms;
+      info->round_launches += 3 * kRoundsPerCheck;
+      if (ktime)
+        for (int k = 0; k < kRoundsPerCheck; ++k) {
+          float t = 0;
+          CK(cudaEventElapsedTime(&t, c->kev[2 * k], c->kev[2 * k + 1]));
+          info->ms_kernel_trace += t;
+        }
+    }
+    if (roundLog)
+      fprintf(roundLog, "pass %d rounds %d inflight %d rootNext %d/%d queue %d yields %d ms %.3f\n", pass, hc.rounds,
+              hc.inflight, hc.rootNext, n, hc.count[round & 1], hc.yields, ms);
+    if (hc.error) {
+      setErr(hc.error == 2 ? "malformed sub-beam record" : "sub-beam queue overflow (capacity %d)", c->capacity);
+      return BT_ERR_CAPACITY;
+    }
+    if (!hc.done && launches > kMaxLaunches) {
+      setErr("launch limit reached with %d roots in flight", hc.inflight);
+      return BT_ERR_TIMEOUT;
+    }
+    return BT_OK;
+  }
+
+  // After a pass: its roots abandoned over budget, compacted into a retry
+  // list (*list, *nk; nk = 0: none).
+  int endPass(int n, const int32_t** list, int* nk) {
     if (info) info->max_spill = std::max(info->max_spill, hc.maxQueue);
     roundsRun += hc.rounds;
     yieldsRun += hc.yields;
-    if (hc.killed == 0) break;
+    *nk = 0;
+    if (hc.killed == 0) return BT_OK;
     if (pass >= c->cfg.max_retries) {
-      setErr("%d roots still over budget %d after %d retries", hc.killed, budget, pass);
+      setErr("%d roots still over budget %d after %d retries", hc.killed, p.budget, pass);
       return BT_ERR_CAPACITY;
     }
-    // retry the abandoned roots with a larger budget
     int32_t* dst = c->dList[pass & 1];
     CK(cudaMemsetAsync(c->dKillCount, 0, sizeof(int), c->stream));
-    collectKilledKernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->dState, list, n, dst, c->dKillCount);
+    collectKilledKernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->dState, *list, n, dst, c->dKillCount);
     launches++;
-    int nk = 0;
-    CK(cudaMemcpyAsync(&nk, c->dKillCount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(nk, c->dKillCount, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    retried += nk;
-    list = dst;
-    n = nk;
-    budget *= 16;
+    retried += *nk;
+    if (pass == 0 && info) info->overflow_roots += *nk;
+    *list = dst;
+    return BT_OK;
   }
-  if (info) {
+
+  void finish(int64_t R) {
+    if (!info) return;
     info->rounds += roundsRun;
     info->tail_rounds += tailRounds;
     info->yields += yieldsRun;
@@ -1572,6 +1643,28 @@ int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info)
     info->roots += R;
     fillInfo(c, hc, info);
   }
+};
+
+template <int App>
+int runRoots(bt_gpu_ctx* c, AppParams app, int R, int budget, bt_run_info* info) {
+  RoundRunner<App> rr(c, info);
+  int e = rr.begin(app, R);
+  if (e) return e;
+  const int32_t* list = nullptr;
+  int n = R;
+  for (;;) {
+    if ((e = rr.startPass(n, list, budget))) return e;
+    do {
+      if ((e = rr.batch())) return e;
+    } while (!rr.hc.done);
+    int nk = 0;
+    if ((e = rr.endPass(n, &list, &nk))) return e;
+    if (nk == 0) break;
+    // retry the abandoned roots with a larger budget
+    n = nk;
+    budget *= 16;
+  }
+  rr.finish(R);
   return BT_OK;
 }
 
@@ -1836,13 +1929,21 @@ int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu
 
 int bt_gpu_destroy(bt_gpu_ctx* c) {
   if (!c) return BT_OK;
+  if (c->serving) btserve::stop(c);  // the serving threads and their lanes first
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (!c->ownsScene) {  // a serving lane: the scene arrays are its parent's
+    c->dNode = nullptr;
+    c->dBox = nullptr;
+    c->dParent = nullptr;
+    c->dRef = nullptr;
+    c->dTriNV = nullptr;
+  }
   void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
                   c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
                   c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart, c->dHx, c->dHy, c->dHn,
-                  c->dHt, c->dHitCount, c->dFlag};
+                  c->dHt, c->dHitCount, c->dFlag, c->dRanges, c->dJobCounts};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& ev : c->ev)
@@ -1861,6 +1962,12 @@ int bt_gpu_add_scene(bt_gpu_ctx* c, const bt_scene_desc* scene, const bt_kd_desc
     setErr("bt_gpu_add_scene: empty scene or tree");
     return BT_ERR_INVALID;
   }
+  if (!c->ownsScene) {
+    setErr("bt_gpu_add_scene: add scenes to the context itself, not to a serving lane");
+    return BT_ERR_INVALID;
+  }
+  // serving lanes read the arrays being replaced: wait until none works
+  std::unique_lock<std::shared_mutex> lk(c->sceneLock);
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));  // nothing in flight reads the arrays being replaced
   const int e = uploadScene(c, scene, kd);
@@ -2225,6 +2332,8 @@ void addInfo(bt_run_info* a, const bt_run_info& b) {
   a->round_launches += b.round_launches;
   a->passes += b.passes;
   a->retried_roots += b.retried_roots;
+  a->overflow_roots += b.overflow_roots;
+  a->yields += b.yields;
   a->max_spill = std::max(a->max_spill, b.max_spill);
   a->roots += b.roots;
   a->rounds += b.rounds;
@@ -2532,6 +2641,358 @@ int bt_gpu_point_mask(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving lanes: the engine side of bt_gpu_submit / bt_gpu_poll (serve.cpp).
+//
+// A lane is a bt_gpu_ctx that views its parent's scene pool (it owns no
+// scene array) and owns a stream, sub-beam queues, root arrays and a pixel
+// arena, so that lanes run side by side on the device.  A soft lane runs
+// streaming engine runs: the soft-shadow jobs of a run share the rounds as
+// in bt_gpu_batch_soft, jobs that arrive while the run goes on are folded
+// in between batches of rounds (their roots appended to the root list,
+// their parameters to the job table), and a job whose roots are all done is
+// finalised and handed back at once while the run goes on.  Jobs with a
+// root abandoned over budget wait for the retry passes at the run's end.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// For the jobs named in `ranges` (root ranges [a, b), one pair per
+// blockIdx.y): counts[2j] = roots still live, counts[2j + 1] = roots
+// abandoned over budget.
+__global__ void jobStatusKernel(const int32_t* live, const int32_t* state, const int32_t* ranges, int* counts) {
+  const int j = blockIdx.y;
+  const int a = ranges[2 * j], b = ranges[2 * j + 1];
+  int busy = 0, killed = 0;
+  for (int k = a + int(blockIdx.x * blockDim.x + threadIdx.x); k < b; k += int(gridDim.x * blockDim.x)) {
+    busy += live[k] != 0;
+    killed += state[k] == kRootKilled;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    busy += __shfl_down_sync(kFull, busy, o);
+    killed += __shfl_down_sync(kFull, killed, o);
+  }
+  if (laneId() == 0) {
+    if (busy) atomicAdd(&counts[2 * j], busy);
+    if (killed) atomicAdd(&counts[2 * j + 1], killed);
+  }
+}
+
+// Soft-shadow roots of a W x H job (8 x 4 pixel tiles of 32 roots).
+int64_t softRoots(const bt_camera& cam) { return int64_t((cam.W + 7) / 8) * ((cam.H + 3) / 4) * 32; }
+
+}  // namespace
+
+namespace btserve {
+
+int deviceOf(const bt_gpu_ctx* c) { return c->device; }
+void useDevice(const bt_gpu_ctx* c) { cudaSetDevice(c->device); }
+std::shared_mutex& sceneLock(bt_gpu_ctx* c) { return c->sceneLock; }
+void*& servingState(bt_gpu_ctx* c) { return c->serving; }
+const char* lastError() { return g_err; }
+int sceneCount(bt_gpu_ctx* c) { return int(c->pool.size()); }
+
+int64_t sceneTris(bt_gpu_ctx* c, int32_t scene) {
+  return scene >= 0 && size_t(scene) < c->pool.size() ? c->pool[size_t(scene)].numTris : 0;
+}
+
+int64_t sceneBytes(const bt_gpu_ctx* c) {
+  return int64_t(c->s.numNodes) * (8 + 32 + 4) + c->numRefs * 64 + c->numTris * 32;
+}
+
+int64_t laneBytes(const bt_gpu_ctx* c) {
+  return 3 * int64_t(c->capacity) * int64_t(sizeof(SubBeam)) + int64_t(c->rootCap) * 68 + c->pixCap * 40 +
+         c->outCap * 52 + c->hitCap * 40 + c->flagCap;
+}
+
+int64_t laneHighWater(const bt_gpu_ctx* c) { return 3 * c->queueHighWater * int64_t(sizeof(SubBeam)); }
+
+void laneView(bt_gpu_ctx* lane) {
+  const bt_gpu_ctx* p = lane->parent;
+  lane->dNode = p->dNode;
+  lane->dBox = p->dBox;
+  lane->dParent = p->dParent;
+  lane->dRef = p->dRef;
+  lane->dTriNV = p->dTriNV;
+  lane->s = p->s;
+  lane->offset = p->offset;
+  lane->numTris = p->numTris;
+  lane->numRefs = p->numRefs;
+  lane->pool = p->pool;
+}
+
+int laneCreate(bt_gpu_ctx* parent, int64_t capacity, int64_t pixels, int jobs, bt_gpu_ctx** out) {
+  *out = nullptr;
+  bt_gpu_ctx* c = new bt_gpu_ctx();
+  c->cfg = parent->cfg;
+  c->device = parent->device;
+  c->sms = parent->sms;
+  c->parent = parent;
+  c->ownsScene = false;
+  auto fail = [&](int code) {
+    bt_gpu_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(BT_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(BT_ERR_CUDA);
+  for (auto& ev : c->ev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
+  for (auto& ev : c->rev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
+  {
+    std::shared_lock<std::shared_mutex> lk(parent->sceneLock);
+    laneView(c);
+  }
+  const int64_t cap = std::max<int64_t>(1024, std::min<int64_t>(capacity > 0 ? capacity : parent->capacity, 1 << 30));
+  c->capacity = int(cap);
+  int e;
+  if ((e = devAlloc(&c->dQ[0], size_t(cap))) || (e = devAlloc(&c->dQ[1], size_t(cap))) ||
+      (e = devAlloc(&c->dQ[2], size_t(cap))) || (e = devAlloc(&c->dCtr, 1)) || (e = devAlloc(&c->dStats, kNumStats)) ||
+      (e = devAlloc(&c->dKillCount, 1)))
+    return fail(e);
+  if (pixels > 0) {
+    // a soft lane: the pixel arena, roots for it (tiles round each job up),
+    // the job table and the completion-check buffers
+    jobs = std::max(jobs, 1);
+    const int64_t roots = pixels + int64_t(jobs) * 4096;
+    if (roots > 0x7fffffff) return fail(BT_ERR_TOO_LARGE);
+    if ((e = ensurePix(c, pixels)) || (e = ensureRoots(c, size_t(roots))) || (e = devAlloc(&c->dJobs, size_t(jobs))) ||
+        (e = devAlloc(&c->dJobStart, size_t(jobs) + 1)) || (e = devAlloc(&c->dRanges, 2 * size_t(jobs))) ||
+        (e = devAlloc(&c->dJobCounts, 2 * size_t(jobs))))
+      return fail(e);
+    c->jobCap = jobs;
+  }
+  *out = c;
+  return BT_OK;
+}
+
+void laneDestroy(bt_gpu_ctx* lane) { bt_gpu_destroy(lane); }
+
+int laneVisibility(bt_gpu_ctx* c, int kind, int32_t scene, const bt_camera& cam, int32_t cull, int32_t tile,
+                   const float* light, int32_t* tri, uint8_t* mask, bt_run_info* info) {
+  if (scene < 0 || size_t(scene) >= c->pool.size() || !camOk(&cam)) {
+    setErr("serving: bad scene %d or camera", scene);
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  // render scene `scene` of the pool: its kd root, box and apex offset
+  const PoolScene& ps = c->pool[size_t(scene)];
+  c->s.bounds = ps.box;
+  c->s.rootNode = ps.rootNode;
+  c->offset = ps.offset;
+  const int64_t npix = int64_t(cam.W) * cam.H;
+  int e;
+  if ((e = ensurePix(c, npix)) || (e = ensureFlag(c, npix))) return e;
+  if (tile <= 0) tile = 16;
+  if (kind == BT_REQ_PRIMARY_IDS)
+    e = bt_gpu_primary_ids_device(c, &cam, cull, tile, c->dPixTri, info);
+  else
+    e = bt_gpu_point_mask_device(c, &cam, cull, tile, light, tri ? c->dPixTri : nullptr, c->dFlag, info);
+  if (e) return e;
+  if (tri && ps.triBase != 0)
+    rebaseKernel<<<int((npix + 255) / 256), 256, 0, c->stream>>>(c->dPixTri, npix, ps.triBase);
+  if (tri) CK(cudaMemcpyAsync(tri, c->dPixTri, sizeof(int32_t) * size_t(npix), cudaMemcpyDeviceToHost, c->stream));
+  if (mask && kind != BT_REQ_PRIMARY_IDS)
+    CK(cudaMemcpyAsync(mask, c->dFlag, size_t(npix), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (info && info->max_spill > c->queueHighWater) c->queueHighWater = info->max_spill;
+  return BT_OK;
+}
+
+int laneSoftRun(bt_gpu_ctx* c, SoftFeed& feed, double foldMs, bt_run_info* info) {
+  struct Job {
+    uint64_t tag;
+    StreamJob j;
+    int64_t off;        // first pixel in the arena
+    int32_t a, b;       // its roots
+    int state;          // 0 running, 1 waiting for the retry passes, 2 handed back
+  };
+  std::vector<Job> jobs;
+  std::vector<AppParams> hj;
+  std::vector<int32_t> start(1, 0);
+  int64_t off = 0, R = 0;
+  int anyExact = 0;
+  CK(cudaSetDevice(c->device));
+  const auto t0 = std::chrono::steady_clock::now();
+  auto ageMs = [&] { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+
+  // Folds in the jobs the feed has for this run; returns how many, or a
+  // negative error code.
+  auto fold = [&]() -> int {
+    const size_t n0 = jobs.size();
+    StreamJob j;
+    uint64_t tag = 0;
+    while (int(jobs.size()) < c->jobCap && feed.next(j, tag, c->pixCap - off, int64_t(c->rootCap) - R)) {
+      const PoolScene& ps = c->pool[size_t(j.scene)];
+      const int64_t np = int64_t(j.cam.W) * j.cam.H, Rj = softRoots(j.cam);
+      SceneDev sj = c->s;
+      sj.bounds = ps.box;
+      sj.rootNode = ps.rootNode;
+      dim3 bs(16, 8), gs((j.cam.W + 15) / 16, (j.cam.H + 7) / 8);
+      primaryRaysKernel<<<gs, bs, 0, c->stream>>>(sj, j.cam, c->dPixTri + off, c->dPixX + 3 * off,
+                                                 c->dPixN + 3 * off);
+      AppParams a = baseApp(c, &j.cam);
+      a.rootBox = ps.box;
+      a.rootNode = ps.rootNode;
+      a.triBase = ps.triBase;
+      a.Lc = mk(j.light.c[0], j.light.c[1], j.light.c[2]);
+      a.LU = mk(j.light.U[0], j.light.U[1], j.light.U[2]);
+      a.LV = mk(j.light.V[0], j.light.V[1], j.light.V[2]);
+      a.offset = j.opts.offset > 0 ? j.opts.offset : ps.offset;
+      a.exact = j.opts.exact;
+      a.pixTri = c->dPixTri + off;
+      a.pixX = c->dPixX + 3 * off;
+      a.pixN = c->dPixN + 3 * off;
+      a.vis = c->dVis + off;
+      a.E = c->dE + off;
+      a.Eu = c->dEu + off;
+      a.tiled = 1;
+      a.tilesX = (j.cam.W + 7) / 8;
+      a.shade = c->dShade;
+      hj.push_back(a);
+      start.push_back(int32_t(R + Rj));
+      jobs.push_back(Job{tag, j, off, int32_t(R), int32_t(R + Rj), 0});
+      anyExact |= j.opts.exact;
+      off += np;
+      R += Rj;
+    }
+    const size_t added = jobs.size() - n0;
+    if (added) {
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(c->dJobs + n0, &hj[n0], sizeof(AppParams) * added, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->dJobStart + n0, &start[n0], sizeof(int32_t) * (added + 1), cudaMemcpyHostToDevice,
+                         c->stream));
+    }
+    return int(added);
+  };
+
+  // Finalises job i into its host buffers and hands it back.
+  auto handBack = [&](Job& J) -> int {
+    AppParams a = hj[size_t(&J - jobs.data())];
+    a.missFx = c->dMiss + J.a;
+    a.gFx = c->dG + J.a;
+    const int Rj = J.b - J.a;
+    softFinalizeKernel<<<(Rj + 255) / 256, 256, 0, c->stream>>>(a, c->dState + J.a, Rj);
+    const int64_t np = int64_t(J.j.cam.W) * J.j.cam.H;
+    if (a.triBase != 0 && J.j.tri)
+      rebaseKernel<<<int((np + 255) / 256), 256, 0, c->stream>>>(c->dPixTri + J.off, np, a.triBase);
+    CK(cudaGetLastError());
+    const size_t f4 = sizeof(float) * size_t(np);
+    if (J.j.tri) CK(cudaMemcpyAsync(J.j.tri, c->dPixTri + J.off, f4, cudaMemcpyDeviceToHost, c->stream));
+    if (J.j.vis) CK(cudaMemcpyAsync(J.j.vis, c->dVis + J.off, f4, cudaMemcpyDeviceToHost, c->stream));
+    if (J.j.E) CK(cudaMemcpyAsync(J.j.E, c->dE + J.off, f4, cudaMemcpyDeviceToHost, c->stream));
+    if (J.j.Eu) CK(cudaMemcpyAsync(J.j.Eu, c->dEu + J.off, f4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    J.state = 2;
+    feed.finished(J.tag, BT_OK, "");
+    return BT_OK;
+  };
+
+  // The running jobs whose roots are all admitted: those with every root
+  // done are handed back; those with an abandoned root wait for the retries.
+  std::vector<int32_t> ranges;
+  std::vector<int> counts;
+  std::vector<size_t> cand;
+  auto settle = [&](int rootNext) -> int {
+    cand.clear();
+    ranges.clear();
+    int32_t longest = 0;
+    for (size_t i = 0; i < jobs.size(); ++i)
+      if (jobs[i].state == 0 && jobs[i].b <= rootNext) {
+        cand.push_back(i);
+        ranges.push_back(jobs[i].a);
+        ranges.push_back(jobs[i].b);
+        longest = std::max(longest, jobs[i].b - jobs[i].a);
+      }
+    if (cand.empty()) return BT_OK;
+    const size_t nc = cand.size();
+    counts.assign(2 * nc, 0);
+    CK(cudaMemcpyAsync(c->dRanges, ranges.data(), sizeof(int32_t) * 2 * nc, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->dJobCounts, 0, sizeof(int) * 2 * nc, c->stream));
+    dim3 g(unsigned(std::min<int64_t>((longest + 255) / 256, 64)), unsigned(nc));
+    jobStatusKernel<<<g, 256, 0, c->stream>>>(c->dLive, c->dState, c->dRanges, c->dJobCounts);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(counts.data(), c->dJobCounts, sizeof(int) * 2 * nc, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < nc; ++k) {
+      if (counts[2 * k] != 0) continue;
+      Job& J = jobs[cand[k]];
+      if (counts[2 * k + 1] != 0) {
+        J.state = 1;
+        continue;
+      }
+      const int e = handBack(J);
+      if (e) return e;
+    }
+    return BT_OK;
+  };
+
+  auto failAll = [&](int e) {
+    const std::string why = g_err;
+    for (Job& J : jobs)
+      if (J.state != 2) {
+        J.state = 2;
+        feed.finished(J.tag, e, why.c_str());
+      }
+    return e;
+  };
+
+  const int first = fold();
+  if (first < 0) return failAll(first);
+  if (first == 0) return BT_OK;
+  RoundRunner<kAppSoft> rr(c, info);
+  AppParams batch = baseApp(c, nullptr);
+  batch.exact = anyExact;
+  batch.jobs = c->dJobs;
+  batch.jobStart = c->dJobStart;
+  batch.numJobs = int(jobs.size());
+  int e = rr.begin(batch, int(c->rootCap));
+  if (!e) e = rr.startPass(int(R), nullptr, c->cfg.budget);
+  if (e) return failAll(e);
+  // pass 0, folding arrivals in while the run is young
+  for (;;) {
+    if ((e = rr.batch()) || (e = settle(rr.hc.rootNext))) return failAll(e);
+    const int added = ageMs() < foldMs ? fold() : 0;
+    if (added < 0) return failAll(added);
+    if (added > 0) {
+      // roots [old numRoots, R) join the pass; admission overshoots the
+      // end of the root list by up to a warp's claim per warp, so its
+      // cursor comes back to the old end first
+      if (rr.hc.rootNext > rr.p.numRoots) {
+        CK(cudaMemcpyAsync(&c->dCtr->rootNext, &rr.p.numRoots, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        rr.hc.rootNext = rr.p.numRoots;
+      }
+      rr.p.numRoots = int(R);
+      rr.p.app.numJobs = int(jobs.size());
+      rr.p.app.exact = anyExact;
+      if ((e = rr.reopen())) return failAll(e);
+      continue;
+    }
+    if (rr.hc.done) break;
+  }
+  if (rr.hc.maxQueue > c->queueHighWater) c->queueHighWater = rr.hc.maxQueue;
+  // retry passes for the roots abandoned over budget
+  const int32_t* list = nullptr;
+  int n = int(R), budget = c->cfg.budget;
+  for (;;) {
+    int nk = 0;
+    if ((e = rr.endPass(n, &list, &nk))) return failAll(e);
+    if (nk == 0) break;
+    n = nk;
+    budget *= 16;
+    if ((e = rr.startPass(n, list, budget))) return failAll(e);
+    do {
+      if ((e = rr.batch())) return failAll(e);
+    } while (!rr.hc.done);
+  }
+  for (Job& J : jobs)
+    if (J.state != 2 && (e = handBack(J))) return failAll(e);
+  rr.finish(R);
+  return BT_OK;
+}
+
+}  // namespace btserve
 
 // ---------------------------------------------------------------------------
 // Allocation-free soft shadows (bt_gpu_soft_points_noalloc).
@@ -2867,6 +3328,11 @@ int bt_gpu_soft_points_noalloc(const bt_scene_desc* sc, const bt_kd_desc* kd, co
   // of every pass and writes each root's state when it admits the root, so
   // nothing a previous call left in the array is read.
   int e = softCore(&c, L, o, n, nullptr, dTri, dX, dN, dVis, dE, dEu, info);
+  if (e == BT_ERR_CAPACITY) {
+    const std::string why = g_err;
+    setErr("%s (the allocation-free call's queues hold %lld sub-beams each, out of its fixed scratch array)",
+           why.c_str(), (long long)lay.cap);
+  }
   if (e) return e;
   CK(cudaStreamSynchronize(0));
   if (info)

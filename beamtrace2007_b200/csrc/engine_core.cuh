@@ -316,10 +316,30 @@ BT_HD int advance(const SceneDev& s, const Query& q, const Beam& B, SubBeam& r, 
 }
 
 
+BT_HD V3 edgePlane(const V3* r, const uint32_t* T, int i, int j) {
+  return T[i] < T[j] ? cross(r[i], r[j]) : neg(cross(r[j], r[i]));
+}
+
 BT_COLD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
   TriRec t = loadRef(s, k);
   triSetup(q, t.v0, t.v1, t.v2, t.n, t.vi, t.tri, ti);
 }
+
+// setupRef and the FP64 twins of the edge lines (the eps_fp64 clip).
+BT_COLD void setupRef64(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti, Line64* e64) {
+  TriRec t = loadRef(s, k);
+  triSetup(q, t.v0, t.v1, t.v2, t.n, t.vi, t.tri, ti);
+  e64[0].ok = e64[1].ok = e64[2].ok = 0;
+  if (!ti.ok) return;
+  const V3 m0 = edgePlane(ti.r, t.vi, 0, 1);
+  const float sg = dot(ti.r[2], m0) > 0 ? 1.f : -1.f;  // triSetup's orientation sign
+  edgeLines64(q, t.v0, t.v1, t.v2, t.vi, sg, ti.edge, e64);
+}
+
+// How an edge vote treats beam corners inside the fuzzy band: as the
+// reference does (float); the same, counting the band corners and their
+// FP64 re-evaluation (eps_stats); re-deciding them in FP64 (eps_fp64).
+enum VoteMode { kVoteFloat = 0, kVoteLog = 1, kVoteFp64 = 2 };
 
 // Tests the pending triangle (wfTestOne, wavefront_core.h:236-268).
 // kStepFinished: AnyHit beam fully occluded by `occluder` (caller outputs
@@ -348,10 +368,6 @@ BT_HD int classifyAfterEdges(const Query& q, const Beam& B, const TriInfo& ti, b
   if (allIn) return kTriAllIn;
   if (separated(q, B, ti)) return kTriKeep;
   return kTriClip;
-}
-
-BT_HD V3 edgePlane(const V3* r, const uint32_t* T, int i, int j) {
-  return T[i] < T[j] ? cross(r[i], r[j]) : neg(cross(r[j], r[i]));
 }
 
 // Disagreement logging for one edge vote: corners whose float distance to
@@ -394,8 +410,45 @@ BT_HD void logBand(const Query& q, const Beam& B, const Line& L, const TriRec& t
   }
 }
 
-template <bool EpsLog = false>
+// voteLine with the corners inside the float band re-decided by the FP64
+// edge line from vertex i to j of t (computed only when a corner is in the
+// band); counts the band corners and those the FP64 line re-decides.
+BT_HD bool voteLine64(const Query& q, const Beam& B, const Line& L, const TriRec& t, int i, int j, float sg,
+                      bool& allIn, Stats& st) {
+  bool anyIn = false, anyOut = false;
+  bool in[4];
+  int band = 0;
+  for (int k = 0; k < 4; ++k) {
+    const float dv = B.qx[k] * L.a + B.qy[k] * L.b + L.c;
+    in[k] = !(dv > q.eps) && !(dv < -q.eps);
+    anyIn |= dv > q.eps;
+    anyOut |= dv < -q.eps;
+    band += in[k];
+  }
+  if (band) {
+    const V3 vf[3] = {t.v0, t.v1, t.v2};
+    const Line64 e = edgeLine64(q, vf[i], vf[j], t.vi[i] < t.vi[j], sg, L);
+    st.epsBand += uint32_t(band);
+    if (e.ok)
+      for (int k = 0; k < 4; ++k) {
+        if (!in[k]) continue;
+        const double d = e.eval(B.qx[k], B.qy[k]);
+        if (d > double(q.eps)) {
+          anyIn = true;
+          st.epsFlip++;
+        } else if (d < -double(q.eps)) {
+          anyOut = true;
+          st.epsFlip++;
+        }
+      }
+  }
+  if (anyOut) allIn = false;
+  return anyIn;
+}
+
+template <int Mode = kVoteFloat>
 BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats& st, int& occluder) {
+  constexpr bool EpsLog = Mode == kVoteLog, F64 = Mode == kVoteFp64;
   const uint2 leaf = s.node[r.node];
   const uint32_t i = uint32_t(r.cursor);
   r.cursor = int32_t(i + 1);
@@ -419,15 +472,18 @@ BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats&
   bool allIn = true;
   ti.edge[0] = makeLine(sg * dot(m0, q.P.u), sg * dot(m0, q.P.v), sg * dot(m0, q.P.d), q.ext);
   if (EpsLog) logBand(q, B, ti.edge[0], t, 0, 1, sg, st);
-  if (!voteLine(q, B, ti.edge[0], allIn)) return kStepContinue;
+  if (F64 ? !voteLine64(q, B, ti.edge[0], t, 0, 1, sg, allIn, st) : !voteLine(q, B, ti.edge[0], allIn))
+    return kStepContinue;
   const V3 m1 = edgePlane(ti.r, t.vi, 1, 2);
   ti.edge[1] = makeLine(sg * dot(m1, q.P.u), sg * dot(m1, q.P.v), sg * dot(m1, q.P.d), q.ext);
   if (EpsLog) logBand(q, B, ti.edge[1], t, 1, 2, sg, st);
-  if (!voteLine(q, B, ti.edge[1], allIn)) return kStepContinue;
+  if (F64 ? !voteLine64(q, B, ti.edge[1], t, 1, 2, sg, allIn, st) : !voteLine(q, B, ti.edge[1], allIn))
+    return kStepContinue;
   const V3 m2 = edgePlane(ti.r, t.vi, 2, 0);
   ti.edge[2] = makeLine(sg * dot(m2, q.P.u), sg * dot(m2, q.P.v), sg * dot(m2, q.P.d), q.ext);
   if (EpsLog) logBand(q, B, ti.edge[2], t, 2, 0, sg, st);
-  if (!voteLine(q, B, ti.edge[2], allIn)) return kStepContinue;
+  if (F64 ? !voteLine64(q, B, ti.edge[2], t, 2, 0, sg, allIn, st) : !voteLine(q, B, ti.edge[2], allIn))
+    return kStepContinue;
   ti.n = t.n;
   ti.A[0] = dot(t.n, q.P.u);
   ti.A[1] = dot(t.n, q.P.v);
@@ -563,28 +619,31 @@ struct ClipSink {
 // streams the pieces to env.  Returns -1 if the clip overflowed its fixed
 // lists (the root must be abandoned), else the slots pass 2 will use
 // (0 if nothing changes: the record continues unchanged at cursor + 1).
-template <class Env>
+template <class Env, bool F64 = false>
 BT_CLIP int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, const Beam& B, Stats& st, TriInfo& ti,
-                       Line* L, int& nl, bool& commit, PieceLog* log = nullptr) {
+                       Line* L, int& nl, bool& commit, PieceLog* log = nullptr, Line64* e64 = nullptr) {
   const uint2 leaf = s.node[r.node];
-  setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
-  classifyTri(q, B, ti, L, nl);
+  if (F64)
+    setupRef64(s, q, leaf.x + uint32_t(r.cursor), ti, e64);
+  else
+    setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
+  classifyTri<F64>(q, B, ti, L, nl, e64);
   ClipSink<Env> sink;
   sink.emitting = 0;
   sink.area = AreaSink{0.f, 0, 0};
   sink.log = log;
   if (log) log->count = 0;
   uint32_t five = 0;
-  if (!clipTri<kPolyMax>(q, B, L, nl, sink, five)) return -1;
+  if (!clipTri<kPolyMax, ClipSink<Env>, F64>(q, B, L, nl, sink, five, e64)) return -1;
   st.fiveSplits += five;
   commit = sink.area.newArea >= q.minArea;
   if (!commit) return 0;
   return sink.area.slots0 + (q.mode == kModeAnyHit ? 0 : sink.area.slots1);
 }
 
-template <class Env>
+template <class Env, bool F64 = false>
 BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
-                        Stats& st, const PieceLog* log = nullptr) {
+                        Stats& st, const PieceLog* log = nullptr, const Line64* e64 = nullptr) {
   st.splits++;
   SubBeam base = r;
   base.cursor = r.cursor + 1;
@@ -607,7 +666,7 @@ BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const T
   sink.emit = emit;
   sink.log = nullptr;
   uint32_t five = 0;  // counted in pass 1
-  clipTri<kPolyMax>(q, B, L, nl, sink, five);
+  clipTri<kPolyMax, ClipSink<Env>, F64>(q, B, L, nl, sink, five, e64);
 }
 
 // Root admission: pre-split pieces become records at the kd root; pieces

@@ -212,7 +212,8 @@ class GpuRenderer:
 
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
                  capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
-                 tail_records: int = 0, eps_stats: bool = False, yield_pct: int = 0, fuse_primary: bool = False):
+                 tail_records: int = 0, eps_stats: bool = False, yield_pct: int = 0, fuse_primary: bool = False,
+                 eps_fp64: bool = False):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -226,6 +227,7 @@ class GpuRenderer:
         cfg.eps_stats = int(eps_stats)
         cfg.yield_pct = int(yield_pct)
         cfg.fuse_primary = int(fuse_primary)
+        cfg.eps_fp64 = int(eps_fp64)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()

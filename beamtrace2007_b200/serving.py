@@ -1,26 +1,26 @@
-"""Serving loop: resident scenes, continuous batching, admission by a device
-memory budget, p50/p99 latency (no counterpart in the reference).
+"""Serving: resident scenes, continuous batching, admission by a device
+memory budget, p50/p99 latency -- a thin Python front over the library's
+own request loop (bt_gpu_serve_start / bt_gpu_submit / bt_gpu_poll in
+include/bt_gpu.h; no counterpart in the reference).
 
 Requests -- primary visibility (per-pixel hit-triangle ids), point shadows
 (per-pixel shadow mask) or exact area-light soft shadows, each for a camera
 and resolution on one resident scene -- arrive at any time through
-`Server.submit`.  Every resident scene keeps its kd-tree and
-`workers_per_scene` engine contexts on the GPU for the server's lifetime;
-each context has its own CUDA stream and worker thread, so requests of
-different scenes, and of one scene, run on the device at the same time.  A
-free worker takes its scene's oldest admitted request: if that is a soft-
-shadow request, together with every other soft-shadow request waiting for
-the scene, in one batched engine run (bt_gpu_batch_soft, whose roots share
-the rounds); otherwise that request alone.  So a short primary request does
-not wait behind a long soft-shadow batch while another worker is free.
+`Server.submit`.  All scenes live in one context's scene pool with their
+kd-trees for the server's lifetime.  Inside the library:
 
-Admission: the resident scenes and their sub-beam queues are charged to the
-budget at start; a request is admitted, in arrival order, when its own
-device memory (outputs, per-pixel scratch, roots) fits in what is left, and
-released when it completes.
+* soft-shadow requests share a streaming engine run on the soft lane:
+  those that arrive while the run is young are folded into the rounds in
+  flight, and each is handed back as soon as its own roots are done;
+* primary and point requests run on `vis_lanes` lanes (engine buffers and a
+  CUDA stream each), overlapping each other and the soft run on the GPU;
+* admission refuses a request (BT_ERR_BUSY) while the resident scenes, the
+  lanes' sub-beam queue high-water mark and the admitted requests would
+  exceed the memory budget; refused requests wait here, in arrival order,
+  and are submitted again as completions free memory.
 
 Results do not depend on what else is in flight: the engine accumulates in
-fixed point and the batch path is bitwise the single-job path.
+fixed point and a job gives bitwise the same result alone or in a run.
 
 Scenes are given as generated scenes, prepared scenes, or paths of the
 reference's scene configs; configs go through a SceneCache
@@ -31,13 +31,18 @@ from the cache directory.
 from __future__ import annotations
 
 import collections
+import ctypes as C
 import threading
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _native as N
+
 KINDS = ("primary", "point", "soft")
+_KIND_CODE = {"primary": N.BT_REQ_PRIMARY_IDS, "point": N.BT_REQ_POINT_MASK, "soft": N.BT_REQ_SOFT}
+BT_ERR_BUSY = -7
 
 
 @dataclass
@@ -52,6 +57,7 @@ class Request:
     tile: int = 0             # primary / point: the tile it ran with (set by the server)
     arrival: float = 0.0      # perf_counter seconds, set by submit
     done: float = 0.0
+    ms_queued: float = 0.0    # in the library: submit to start (soft: to joining a run)
     result: object = None
     error: str | None = None
     event: threading.Event = field(default_factory=threading.Event)
@@ -65,53 +71,27 @@ class Request:
         return self.done - self.arrival
 
 
-def request_bytes(r: Request) -> int:
-    """Device memory a request holds while it runs: outputs and per-pixel
-    scratch (tri, X, N, vis, E, Eu) and, per root, the engine's root state
-    (soft: one root per pixel; primary and point: polygon lists)."""
-    px = r.W * r.H
-    if r.kind == "soft":
-        return px * (4 + 12 + 12 + 12 + 164)
-    return px * (2 * 44 + 16) + (px // 256 + 1) * 164
-
-
 def primary_tile(r: Request) -> int:
-    """Pixels per side of a primary root: 16 (the reference's tile) from 512
-    pixels up; 8 below, where 16 leaves too few roots to fill the GPU
-    (measured on the served scenes: 69 vs 142 ms at 256^2)."""
+    """Pixels per side of a primary root when the scene and size were not
+    tuned: 16 (the reference's tile) from 512 pixels up; 8 below, where 16
+    leaves too few roots to fill the GPU."""
     return 16 if min(r.W, r.H) >= 512 else 8
 
 
-class _SceneSlot:
-    def __init__(self, name, scene_data, engines):
+class _Scene:
+    def __init__(self, name, data, prepared, sid):
         self.name = name
-        self.data = scene_data
-        self.engines = engines
-        self.pending: collections.deque[Request] = collections.deque()
-        self.cv = threading.Condition()
-        self.threads: list[threading.Thread] = []
-
-    @property
-    def engine(self):
-        return self.engines[0]
-
-    def take(self) -> list:
-        """The oldest pending request, with every other pending soft-shadow
-        request when it is one (called with cv held)."""
-        head = self.pending.popleft()
-        if head.kind != "soft":
-            return [head]
-        batch = [head] + [r for r in self.pending if r.kind == "soft"]
-        self.pending = collections.deque(r for r in self.pending if r.kind != "soft")
-        return batch
+        self.data = data
+        self.prepared = prepared
+        self.id = sid
 
 
 class Server:
-    """Resident scenes on one GPU.  `engine_factory(prepared_scene, capacity)`
-    builds a context (GpuRenderer by default; tests may pass a stand-in)."""
+    """Resident scenes on one GPU behind the library's request loop."""
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 21,
-                 engine_factory=None, cache=None, kd_on_gpu: bool = True, workers_per_scene: int = 2):
+                 cache=None, kd_on_gpu: bool = True, vis_lanes: int = 2, fold_ms: float = 100.0,
+                 soft_pixels: int = 8 << 20):
         from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
         kd_device = device if kd_on_gpu else None
@@ -119,145 +99,157 @@ class Server:
         self.prep_ms: dict = {}   # scene -> ms to admit it (ingest, finalise, kd-tree)
         self.budget = int(memory_budget_gb * (1 << 30))
         self.device = device
-        if engine_factory is None:
-            def engine_factory(ps, capacity):
-                return GpuRenderer(ps, device=device, capacity=capacity)
-        self.slots: dict[str, _SceneSlot] = {}
-        self.resident = 0
+        self.scenes: dict[str, _Scene] = {}
+        self.engine = None
         for name, sd in scenes.items():
             t0 = time.perf_counter()
             if isinstance(sd, str):  # a scene config: ingested and prepared through the cache
                 sd, ps = self.cache.get(sd)
             else:
                 ps = sd if isinstance(sd, PreparedScene) else PreparedScene(sd.pos, sd.tris, kd_device=kd_device)
+            if self.engine is None:
+                self.engine = GpuRenderer(ps, device=device, capacity=queue_records)
+                sid = 0
+            else:
+                sid = self.engine.add_scene(ps)
             self.prep_ms[name] = (time.perf_counter() - t0) * 1e3
-            # each context holds the scene, its tree and its queues
-            per = 44 * len(ps.kd_split) + 64 * len(ps.kd_tri_indices) + 32 * ps.num_tris + 3 * 64 * queue_records
-            self.resident += per * workers_per_scene
-            slot = _SceneSlot(name, sd, [engine_factory(ps, queue_records) for _ in range(workers_per_scene)])
-            self.slots[name] = slot
-        if self.resident > self.budget:
-            raise ValueError(f"resident scenes and queues need {self.resident / 2**30:.2f} GiB, "
-                             f"over the {memory_budget_gb} GiB budget")
+            self.scenes[name] = _Scene(name, sd, ps, sid)
+        cfg = N.ServeConfig(vis_lanes=vis_lanes, soft_jobs=256, soft_pixels=soft_pixels, capacity=queue_records,
+                            fold_ms=fold_ms, memory_budget=self.budget)
+        N.check(N.lib().bt_gpu_serve_start(self.engine._h, C.byref(cfg)))
         self.tiles: dict = {}   # (scene, W, H) -> primary tile chosen by `tune`
-        self.in_use = 0
         self.lock = threading.Lock()
-        self.waiting: collections.deque[Request] = collections.deque()
+        self.inflight: dict[int, tuple] = {}   # ticket -> (request, its C struct and output arrays)
+        self.waiting: collections.deque[Request] = collections.deque()  # refused for memory, in arrival order
+        self.refusals = 0
         self.running = True
-        for slot in self.slots.values():
-            for eng in slot.engines:
-                t = threading.Thread(target=self._worker, args=(slot, eng), daemon=True)
-                slot.threads.append(t)
-                t.start()
+        self.poller = threading.Thread(target=self._poll, daemon=True)
+        self.poller.start()
 
-    def tune(self, sizes=(256, 512, 1024), tiles=(8, 16, 32)):
+    @property
+    def slots(self):
+        return self.scenes
+
+    def tune(self, sizes=(256, 512, 1024), tiles=(8, 16, 32), reps: int = 2):
         """Autotunes the primary tile of every resident scene at each square
-        size (autotune.tune_tile); call before the stream starts (it uses the
-        scenes' contexts).  Untuned sizes use `primary_tile`."""
-        from .autotune import tune_tile
+        size: each candidate's primary request is timed through the serving
+        lanes (the fastest of `reps` after a warm-up).  Call before the
+        stream starts.  Untuned sizes use `primary_tile`."""
         out = {}
-        for name, slot in self.slots.items():
+        for name in self.scenes:
             for W in sizes:
-                r = Request("primary", name, W, W)
-                best, t = tune_tile(slot.engine, self._camera(slot, r), tiles)
+                ms = {}
+                for tile in tiles:
+                    t = []
+                    for _ in range(reps + 1):
+                        r = self.submit(Request("primary", name, W, W, tile=tile))
+                        r.event.wait()
+                        t.append(r.latency * 1e3)
+                    ms[tile] = float(np.min(t[1:]))
+                best = min(ms, key=ms.get)
                 self.tiles[(name, W, W)] = best
-                out[f"{name}/{W}"] = {"tile": best, "ms": {k: round(v * 1e3, 2) for k, v in t.items()}}
+                out[f"{name}/{W}"] = {"tile": best, "ms": {k: round(v, 2) for k, v in ms.items()}}
         return out
 
-    # ---- admission ----
+    def camera(self, r: Request):
+        from .renderer import make_camera
+        sc = self.scenes[r.scene]
+        v = sc.data.views[r.view]
+        return make_camera(v.eye, v.target, v.fov, sc.data.up, r.W, r.H)
+
+    _camera = camera
+
+    # ---- requests ----
     def submit(self, r: Request) -> Request:
-        if r.kind not in KINDS or r.scene not in self.slots:
+        if r.kind not in KINDS or r.scene not in self.scenes:
             raise ValueError(f"bad request {r.kind} / {r.scene}")
-        if request_bytes(r) > self.budget - self.resident:
-            raise ValueError("request larger than the memory budget")
         r.arrival = time.perf_counter()
+        if r.kind != "soft" and not r.tile:
+            r.tile = self.tiles.get((r.scene, r.W, r.H)) or primary_tile(r)
         with self.lock:
-            self.waiting.append(r)
-            self._admit()
+            if self.waiting or not self._submit(r):
+                self.waiting.append(r)
         return r
 
-    def _admit(self):
-        # in arrival order, while the head fits (called with self.lock held)
-        while self.waiting:
-            r = self.waiting[0]
-            need = request_bytes(r)
-            if self.resident + self.in_use + need > self.budget:
-                break
-            self.waiting.popleft()
-            self.in_use += need
-            slot = self.slots[r.scene]
-            with slot.cv:
-                slot.pending.append(r)
-                slot.cv.notify()
-
-    def _release(self, reqs):
-        with self.lock:
-            for r in reqs:
-                self.in_use -= request_bytes(r)
-            self._admit()
-
-    # ---- execution ----
-    def _worker(self, slot: _SceneSlot, engine):
-        while True:
-            with slot.cv:
-                while self.running and not slot.pending:
-                    slot.cv.wait(0.05)
-                if not self.running and not slot.pending:
-                    return
-                batch = slot.take()
-            try:
-                self._run(slot, engine, batch)
-            except Exception as e:  # a failed run fails its requests, not the server
-                for r in batch:
-                    if r.result is None:
-                        r.error = f"{type(e).__name__}: {e}"
-            now = time.perf_counter()
-            for r in batch:
-                r.done = now if r.done == 0.0 else r.done
-            self._release(batch)
-            for r in batch:
-                r.event.set()
-
-    def _camera(self, slot, r):
-        from .renderer import make_camera
-        v = slot.data.views[r.view]
-        return make_camera(v.eye, v.target, v.fov, slot.data.up, r.W, r.H)
-
-    def _run(self, slot: _SceneSlot, engine, batch):
-        soft = [r for r in batch if r.kind == "soft"]
-        if soft:
-            cams = [self._camera(slot, r) for r in soft]
-            lights = [slot.data.light_array(r.light_scale) for r in soft]
-            res = engine.batch_soft(cams, lights, exact=soft[0].exact) if all(
-                r.exact == soft[0].exact for r in soft) else None
-            if res is None:
-                res = [engine.soft_shadows(c, L, exact=r.exact) for c, L, r in zip(cams, lights, soft)]
-            now = time.perf_counter()
-            for r, x in zip(soft, res):
-                r.result = x
-                r.done = now
-        for r in batch:
-            if r.kind == "soft":
-                continue
-            cam = self._camera(slot, r)
-            tile = r.tile = self.tiles.get((r.scene, r.W, r.H)) or primary_tile(r)
-            if r.kind == "primary":
-                r.result = engine.primary_ids(cam, tile=tile)
-            else:
-                r.result = engine.point_mask(cam, np.asarray(slot.data.point_light, np.float32), tile=tile)[1]
+    def _submit(self, r: Request) -> bool:
+        """Hands a request to the library (called with self.lock held);
+        False when it is refused for memory now."""
+        sc = self.scenes[r.scene]
+        q = N.Request()
+        q.kind = _KIND_CODE[r.kind]
+        q.scene = sc.id
+        q.cam = self.camera(r)
+        n = r.W * r.H
+        keep = []
+        if r.kind == "soft":
+            L = N.AreaLight.from_array(sc.data.light_array(r.light_scale))
+            q.light = L
+            q.opts = N.SoftOpts(int(r.exact), 0.0)
+            keep = [np.zeros(n, np.int32)] + [np.zeros(n, np.float32) for _ in range(3)]
+            q.tri, q.vis, q.E, q.Eu = (N.ptr(a) for a in keep)
+        else:
+            q.cull = 0
+            q.tile = r.tile
+            q.point_light[:] = [float(x) for x in sc.data.point_light] if r.kind == "point" else [0.0, 0.0, 0.0]
+            keep = [np.zeros(n, np.int32), np.zeros(n, np.uint8)]
+            q.tri = N.ptr(keep[0])
+            q.mask = N.ptr(keep[1]) if r.kind == "point" else None
+        ticket = C.c_uint64()
+        rc = N.lib().bt_gpu_submit(self.engine._h, C.byref(q), C.byref(ticket))
+        if rc == BT_ERR_BUSY:
+            self.refusals += 1
+            return False
+        if rc != N.BT_OK:
+            r.error = N.lib().bt_gpu_last_error().decode(errors="replace")
             r.done = time.perf_counter()
+            r.event.set()
+            return True
+        self.inflight[ticket.value] = (r, q, keep)
+        return True
+
+    def _poll(self):
+        comps = (N.Completion * 64)()
+        count = C.c_int32()
+        while self.running:
+            N.lib().bt_gpu_poll(self.engine._h, comps, 64, C.byref(count), 50)
+            now = time.perf_counter()
+            with self.lock:
+                for k in range(count.value):
+                    c = comps[k]
+                    r, q, keep = self.inflight.pop(c.ticket)
+                    r.ms_queued = c.ms_queued
+                    if c.status != N.BT_OK:
+                        r.error = c.error.decode(errors="replace")
+                    elif r.kind == "soft":
+                        from .renderer import SoftResult
+                        r.result = SoftResult(*keep)
+                    elif r.kind == "primary":
+                        r.result = keep[0].reshape(r.H, r.W)
+                    else:
+                        r.result = keep[1].reshape(r.H, r.W)
+                    r.done = now
+                    r.event.set()
+                # refused requests again, in arrival order, while they are admitted
+                while self.waiting and self._submit(self.waiting[0]):
+                    self.waiting.popleft()
+
+    def stats(self) -> dict:
+        st = N.ServeStats()
+        N.check(N.lib().bt_gpu_serve_stats(self.engine._h, C.byref(st)))
+        d = st.as_dict()
+        d["waiting_here"] = len(self.waiting)
+        d["refusals"] = self.refusals
+        return d
 
     def close(self):
+        if not self.running:
+            return
+        deadline = time.perf_counter() + 600
+        while (self.inflight or self.waiting) and time.perf_counter() < deadline:
+            time.sleep(0.01)
         self.running = False
-        for slot in self.slots.values():
-            with slot.cv:
-                slot.cv.notify_all()
-            for t in slot.threads:
-                t.join(timeout=60)
-            for eng in slot.engines:
-                close = getattr(eng, "close", None)
-                if close:
-                    close()
+        self.poller.join(timeout=60)
+        self.engine.close()
 
     def __enter__(self):
         return self
@@ -271,9 +263,10 @@ def poisson_stream(server: Server, rate: float, n: int, mix=(0.60, 0.25, 0.15), 
     """Submits n requests with exponential inter-arrival times (rate per
     second), kinds drawn from `mix` (primary, point, soft), square
     resolutions from `sizes`, scenes uniformly; waits for all and returns
-    (requests, summary)."""
+    (requests, summary).  `offered_s` is the submission window; a rate is
+    sustained when the requests finish within about that window."""
     rng = np.random.default_rng(seed)
-    names = list(scenes or server.slots.keys())
+    names = list(scenes or server.scenes.keys())
     reqs = []
     t0 = time.perf_counter()
     t_next = t0
@@ -287,13 +280,17 @@ def poisson_stream(server: Server, rate: float, n: int, mix=(0.60, 0.25, 0.15), 
         if delay > 0:
             time.sleep(delay)
         reqs.append(server.submit(r))
+    t_sub = time.perf_counter()
     for r in reqs:
         r.event.wait()
     t_end = max(r.done for r in reqs)
     lat = np.array([r.latency for r in reqs])
     px = sum(r.pixels for r in reqs)
     summary = {"requests": n, "rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
-               "p99_ms": float(np.percentile(lat, 99) * 1e3), "px_per_s": px / (t_end - t0),
-               "errors": sum(r.error is not None for r in reqs),
-               "by_kind": {k: int(sum(r.kind == k for r in reqs)) for k in KINDS}}
+               "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3),
+               "px_per_s": px / (t_end - t0), "req_per_s": n / (t_end - t0), "offered_s": t_sub - t0,
+               "span_s": t_end - t0, "errors": sum(r.error is not None for r in reqs),
+               "by_kind": {k: int(sum(r.kind == k for r in reqs)) for k in KINDS},
+               "p50_ms_by_kind": {k: float(np.percentile([r.latency for r in reqs if r.kind == k], 50) * 1e3)
+                                  for k in KINDS if any(r.kind == k for r in reqs)}}
     return reqs, summary

@@ -9,8 +9,9 @@
 //
 // Differences of contract, all on the side of the caller:
 //   * Roots over budget are retried on the GPU with a 16x budget instead of
-//     being recomputed on the CPU, so lastOverflowPixels and
-//     lastFallbackSeconds stay 0.
+//     being recomputed on the CPU: lastOverflowPixels counts them (roots over
+//     budget in their first pass, as the reference counts the pixels it
+//     hands to the CPU) and lastFallbackSeconds stays 0.
 //   * A failing call throws std::runtime_error with bt_gpu_last_error()
 //     (the reference aborts the process on CUDA errors, gpu_common.cuh:15-22).
 //   * useMailbox and useWavefront are accepted and ignored: the engine has
@@ -230,7 +231,7 @@ void GpuRenderer::softShadows(const Camera& cam, const AreaLight& light, const S
   res.stats.traceSeconds = info.ms_trace * 1e-3;
   lastRounds = info.rounds;
   lastMaxQueue = info.max_spill;
-  lastOverflowPixels = 0;
+  lastOverflowPixels = int(info.overflow_roots);
   lastFallbackSeconds = 0;
   lastKernelSeconds = info.ms_round * 1e-3;
 }
@@ -255,7 +256,7 @@ void GpuRenderer::primary(const Camera& cam, bool cull, std::vector<OutBeam>& hi
   rs.traceSeconds += info.ms_total * 1e-3;
   lastRounds = info.rounds;
   lastMaxQueue = info.max_spill;
-  lastOverflowPixels = 0;
+  lastOverflowPixels = int(info.overflow_roots);
   lastFallbackSeconds = 0;
   lastKernelSeconds = info.ms_round * 1e-3;
 }
@@ -295,7 +296,7 @@ void GpuRenderer::pointShadows(const Camera& cam, const std::vector<OutBeam>& pr
   rs.traceSeconds += info.ms_total * 1e-3;
   lastRounds = info.rounds;
   lastMaxQueue = info.max_spill;
-  lastOverflowPixels = 0;
+  lastOverflowPixels = int(info.overflow_roots);
   lastFallbackSeconds = 0;
   lastKernelSeconds = info.ms_round * 1e-3;
 }

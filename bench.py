@@ -18,6 +18,10 @@ kernels on the engine's stream inside the timed frames (kernel_timing);
 `e2e`: the same frames through bt_gpu_soft with host output buffers (the
 GpuRenderer::softShadows contract), wall-clocked per call, device-to-host
 copies of tri/vis/E/Eu inside.
+`accuracy`: the last timed frame's visibility against the reference's FP64
+build on its own shading points (max, mean, histogram of the error), and
+the reference's 256-ray sampled visibility's error beside it, computed
+after the timed region.
 `cpu_baseline` / `--impl reference`: the reference's own CPU tracer
 (compiled from its sources, oracle/_ref) on the host's cores; the
 reference arm also times the reference's own GPU engine built for sm_100a
@@ -171,6 +175,45 @@ def cpu_reference(scene, steps: int, warmup: int, min_seconds: float = 10.0, max
             "ms_per_frame": per * 1e3}
 
 
+def accuracy(scene, ps, cam, light, vis, ray_sample: int = 16384):
+    """The timed frame's per-result error, outside the timed region: its
+    visibility against the reference's FP64 build (bt_render_d --exact) on
+    the frame's own shading points, every covered pixel (max, mean and a
+    histogram of |vis - fp64|); and, beside it, the error of the reference's
+    256-ray sampled visibility (--method ray --samples 256) on an even
+    sample of the covered pixels.  The FP64 run is timed on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref import RefTracer, ref_available
+    if not (ref_available("f") and ref_available("d")):
+        return None
+    threads = os.cpu_count() or 1
+    rf = RefTracer(scene.pos, scene.tris, "f")
+    rd = RefTracer(scene.pos, scene.tris, "d")
+    tri, X, N, _ = rf.primary_rays(cam.as_array(), cam.W, cam.H, threads=threads)
+    t0 = time.perf_counter()
+    vd, _, _, _ = rd.soft_points(light, ps.offset, tri, X, N, exact=True, threads=threads)
+    fp64_s = time.perf_counter() - t0
+    cov = np.nonzero(tri >= 0)[0]
+    err = np.abs(vis[cov].astype(np.float64) - vd[cov])
+    edges = [0.0, 1e-7, 1e-6, 1e-5, 1e-4, 1e-3, np.inf]
+    hist, _ = np.histogram(err, bins=edges)
+    pick = cov[np.linspace(0, len(cov) - 1, min(ray_sample, len(cov))).astype(np.int64)]
+    t0 = time.perf_counter()
+    vr = rf.soft_points_ray(light, ps.offset, tri[pick], X[pick], N[pick], pick % cam.W, pick // cam.W, samples=256,
+                            threads=threads)
+    ray_s = time.perf_counter() - t0
+    er = np.abs(vr - vd[pick])
+    return {"pixels": int(len(cov)), "max_abs_err_vs_fp64": float(err.max()), "mean_abs_err_vs_fp64": float(err.mean()),
+            "pixels_over_1e-4": int((err > 1e-4).sum()),
+            "histogram": {"edges": ["0", "1e-7", "1e-6", "1e-5", "1e-4", "1e-3", "inf"],
+                          "counts": [int(x) for x in hist]},
+            "ray256": {"pixels": int(len(pick)), "max_abs_err_vs_fp64": float(er.max()),
+                       "mean_abs_err_vs_fp64": float(er.mean()), "seconds": ray_s, "cores": threads},
+            "fp64_oracle": {"seconds": fp64_s, "px_per_s": len(cov) / fp64_s, "cores": threads,
+                            "what": "reference double build, exact, the frame's shading points"},
+            "oracle": "oracle/_ref (the reference compiled from its sources)"}
+
+
 def reference_gpu(scene, steps: int, warmup: int):
     """The reference's own GPU engine (cuda/ built for sm_100a from its
     sources, oracle/_ref/libbtref_gpu.so) on the same frame, if built."""
@@ -200,6 +243,90 @@ def reference_gpu(scene, steps: int, warmup: int):
                      "as its cuda/CMakeLists.txt sets (wall-clocked GpuRenderer::softShadows)"}
 
 
+# Primary visibility and point shadows (the other two paths of the engine):
+# (scene, square size) at the reference's 16 x 16 tile, the hit polygons of
+# the primary pass as the point-shadow roots.
+VIS_WORKLOADS = (("building", 1024), ("sphere", 256), ("sphere", 1024), ("meeting", 256), ("meeting", 1024))
+
+
+def _vis_scenes():
+    from beamtrace2007_b200 import scenes
+    return {"building": scenes.building(), "sphere": scenes.displaced_sphere(), "meeting": scenes.meeting_room()}
+
+
+def visibility_measure(reps: int = 3):
+    """This engine on VIS_WORKLOADS through bt_gpu_primary / bt_gpu_point
+    (polygon lists to the host, the GpuRenderer::primary / pointShadows
+    contract) and through bt_gpu_primary_ids / bt_gpu_point_mask (ids and
+    mask rasterised on the GPU); wall-clocked per call, median of `reps`
+    after a warm-up."""
+    from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
+    out = {}
+    sc = _vis_scenes()
+    for name in sorted({n for n, _ in VIS_WORKLOADS}):
+        s = sc[name]
+        ps = PreparedScene(s.pos, s.tris, kd_device=0)
+        light = np.asarray(s.point_light, np.float32)
+        with GpuRenderer(ps) as g:
+            for n_, W in VIS_WORKLOADS:
+                if n_ != name:
+                    continue
+                v = s.views[0]
+                cam = make_camera(v.eye, v.target, v.fov, s.up, W, W)
+                tp, tq, tids, tmask = [], [], [], []
+                for rep in range(reps + 1):
+                    t0 = time.perf_counter()
+                    prim = g.primary(cam, tile=16)
+                    t1 = time.perf_counter()
+                    sh = g.point_shadows(cam, prim, light)
+                    t2 = time.perf_counter()
+                    g.primary_ids(cam, tile=16)
+                    t3 = time.perf_counter()
+                    g.point_mask(cam, light, tile=16)
+                    t4 = time.perf_counter()
+                    if rep:
+                        tp.append(t1 - t0)
+                        tq.append(t2 - t1)
+                        tids.append(t3 - t2)
+                        tmask.append(t4 - t3)
+                out[f"{name}/{W}"] = {"primary_ms": float(np.median(tp) * 1e3), "point_ms": float(np.median(tq) * 1e3),
+                                      "hits": len(prim), "shadow_polys": len(sh),
+                                      "primary_ids_ms": float(np.median(tids) * 1e3),
+                                      "point_mask_ms": float(np.median(tmask) * 1e3)}
+    return out
+
+
+def reference_gpu_visibility(reps: int = 3):
+    """The reference's own GPU engine (oracle/_ref/libbtref_gpu.so) on
+    VIS_WORKLOADS: GpuRenderer::primary then pointShadows on its hit
+    polygons, wall-clocked per call, median of `reps` after a warm-up."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from ref import RefGpu, RefTracer, ref_gpu_available
+    if not ref_gpu_available():
+        return None
+    out = {}
+    sc = _vis_scenes()
+    for name in sorted({n for n, _ in VIS_WORKLOADS}):
+        s = sc[name]
+        g = RefGpu(s.pos, s.tris)
+        rf = RefTracer(np.eye(3, dtype=np.float32), np.array([[0, 1, 2]], np.uint32), "f")  # Camera::make only
+        for n_, W in VIS_WORKLOADS:
+            if n_ != name:
+                continue
+            v = s.views[0]
+            cam = rf.camera_make(v.eye, v.target, v.fov, s.up, W, W)
+            rs = [g.primary_point(cam, W, W, np.asarray(s.point_light, np.float64), tile=16) for _ in range(reps + 1)]
+            rs = rs[1:]
+            out[f"{name}/{W}"] = {"primary_ms": float(np.median([r["primary_s"] for r in rs]) * 1e3),
+                                  "point_ms": float(np.median([r["point_s"] for r in rs]) * 1e3),
+                                  "hits": rs[-1]["hits"], "shadow_polys": rs[-1]["shadow_polys"],
+                                  "cpu_fallback_ms": float(np.median([r["primary_fallback_s"] + r["point_fallback_s"]
+                                                                      for r in rs]) * 1e3),
+                                  "overflow_roots": rs[-1]["primary_overflow"] + rs[-1]["point_overflow"]}
+        g.close()
+    return out
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
@@ -223,6 +350,10 @@ def run_reference_arm(args):
             g = reference_gpu(s, max(args.steps, 5), args.warmup)
             if g is not None:
                 line["reference_gpu"] = g
+            if not args.no_extras:
+                vis = reference_gpu_visibility()
+                if vis is not None:
+                    line["reference_gpu_visibility"] = vis
     except Exception as e:  # the CPU arm stands on its own
         line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line))
@@ -314,12 +445,14 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
             "ms_batch": pb, "ms_one_by_one": pp, "host_prep_s": prep_s}
 
 
-def serving_measure():
-    """The served stream: three resident scenes (displaced sphere 327,680
-    triangles, meeting room 178,176, office building 2.1M; their kd-trees
-    built on the GPU when the server admits them), Poisson arrivals, 60%
-    primary / 25% point / 15% soft, 256-1024 px square; p50/p99 latency at a
-    sustainable rate and px/s at saturation."""
+def serving_measure(n: int = 300):
+    """The served stream through the library's request loop (bt_gpu_submit /
+    bt_gpu_poll): three resident scenes (displaced sphere 327,680 triangles,
+    meeting room 178,176, office building 2.1M; their kd-trees built on the
+    GPU when the server admits them) in one context's pool, an 8 GB memory
+    budget, Poisson arrivals, 60% primary / 25% point / 15% soft, 256-1024 px
+    square; p50/p99 latency over `n` requests at the configured 50 req/s and
+    px/s at a saturating 500 req/s."""
     from beamtrace2007_b200 import scenes
     from beamtrace2007_b200.serving import Server, poisson_stream
     sc = {"sphere": scenes.displaced_sphere(), "meeting": scenes.meeting_room(), "building": scenes.building()}
@@ -327,11 +460,12 @@ def serving_measure():
     with Server(sc, memory_budget_gb=8.0) as srv:
         # admitting a scene: finalise + kd-tree built on the GPU (bt_kd_build_gpu)
         out["scene_prep_ms"] = {k: round(v, 1) for k, v in srv.prep_ms.items()}
-        out["tuned_tiles"] = srv.tune(sizes=(256, 512, 1024))  # the autotuner, before the stream
-        poisson_stream(srv, rate=50.0, n=6, sizes=(256,), seed=11)  # warm-up
-        for label, rate, n in (("steady", 10.0, 60), ("saturated", 200.0, 80)):
+        out["tuned_tiles"] = srv.tune(sizes=(256, 512, 1024), tiles=(8, 16, 32))  # the autotuner, before the stream
+        poisson_stream(srv, rate=50.0, n=12, sizes=(256,), seed=11)  # warm-up
+        for label, rate in (("configured_50", 50.0), ("saturated_500", 500.0)):
             _, summ = poisson_stream(srv, rate=rate, n=n, sizes=(256, 512, 1024), seed=7)
             out[label] = summ
+        out["stats"] = srv.stats()
     return out
 
 
@@ -463,11 +597,16 @@ def main():
         # the batched-jobs workload at bounded size (the full 64 jobs of up to
         # 200K triangles at up to 512^2 take minutes per batch)
         line["batched_jobs"] = batched_jobs_measure(n_jobs=32, max_tris=20_000, sizes=(64, 128))
+        line["visibility"] = visibility_measure()
         line["serving"] = serving_measure()
     if not args.no_cpu_baseline and ws == 1:
         c = cpu_reference(s, 3, 1)
         if c:
             line["cpu_baseline"] = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # the last timed frame's results against the FP64 oracle
+        acc = accuracy(s, ps, cam, s.light_array(), dvis.cpu().numpy())
+        if acc:
+            line["accuracy"] = acc
     print(json.dumps(line))
     g.close()
     return 0

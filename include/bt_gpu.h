@@ -22,7 +22,9 @@
  * and scene ingest (configs, OBJ/PLY meshes, procedural scenes):
  *   bt_scene_load_config    loadConfig + buildScene src/scene/scene.h:58-61
  *   bt_scene_parse_config   parseConfig + buildScene src/scene/scene.h:60-61
- * Batching (no counterpart in the reference): bt_gpu_batch_soft.
+ * Batching and serving (no counterpart in the reference): bt_gpu_batch_soft,
+ * bt_gpu_add_scene, bt_gpu_serve_start, bt_gpu_submit, bt_gpu_poll,
+ * bt_gpu_serve_stats.
  */
 #ifndef BT_GPU_H
 #define BT_GPU_H
@@ -123,6 +125,11 @@ typedef struct {
                                instead of holding the round (results are the same); 0 = 50, < 0 = never */
   int32_t fuse_primary;     /* nonzero: bt_gpu_soft(_device) trace each pixel's eye ray in the admission of
                                its shadow root instead of a separate primary-ray pass (same results) */
+  int32_t eps_fp64;         /* nonzero (soft shadows): beam corners whose float distance to a triangle edge
+                               line falls inside the fuzzy band are re-decided with the edge line in FP64
+                               (from the same float vertices) in the votes and the clip, before a split;
+                               results then differ from the reference's float build (eps_band_corners and
+                               eps_fp64_flips count the band corners and the re-decided ones) */
 } bt_gpu_config;
 
 typedef struct {
@@ -147,6 +154,8 @@ typedef struct {
   /* summed device time of the trace launches (kernel_timing only, else 0); admit and clip reserved (0) */
   double ms_kernel_admit, ms_kernel_trace, ms_kernel_clip;
   int64_t yields;             /* records handed on unfinished to the next round (yield_pct) */
+  int64_t overflow_roots;     /* roots over budget in their first pass: the reference recomputes these on
+                                 the CPU (lastOverflowPixels), here they are retried on the GPU */
 } bt_run_info;
 
 /* Beam cross-sections on a query plane (OutBeam, beam_types.h:68-73):
@@ -282,10 +291,24 @@ BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light
  * of at least 8192 64-byte records must fit in BT_NOALLOC_SCRATCH_BYTES
  * (each section rounded up to 256 bytes); larger calls return
  * BT_ERR_TOO_LARGE before any GPU work.  A kd-tree whose indices are out of
- * range or out of order returns BT_ERR_INVALID.
+ * range or out of order returns BT_ERR_INVALID, as do triangle references
+ * or vertex indices out of range.
+ *
+ * BT_ERR_CAPACITY can come back here where bt_gpu_soft_points_device
+ * succeeds: the queues get what the fixed array leaves over (at most about
+ * 349,000 records each, against 2^23 on a context), and a root
+ * that outgrows its live sub-beam budget is retried with 16 times the
+ * budget only while that budget (128, 2048, 32768, ...) fits one queue --
+ * two retries here, four on a context.  The message then names the queue
+ * size.
  *
  * Runs on the current device's legacy default stream and returns when the
- * results are complete.  The first call on a device sets up (looks up the
+ * results are complete.  That stream waits for all work already queued on
+ * the device's blocking streams and holds back their later work until this
+ * call's kernels finish: a caller that keeps its own streams running
+ * alongside should create them with cudaStreamNonBlocking, and must itself
+ * finish the work that writes the inputs before the call (synchronise the
+ * stream that wrote them).  The first call on a device sets up (looks up the
  * scratch array's device address, creates two timing events): make it
  * before any stream capture.  All calls on a device share the scratch array,
  * which keeps the last call's contents; each call clears what must start at
@@ -368,6 +391,86 @@ BT_API int bt_gpu_point_mask_device(bt_gpu_ctx* ctx, const bt_camera* cam, int32
  * set flag = 1.  tri and flag are host buffers of W*H. */
 BT_API int bt_gpu_raster(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_polys* prim, int64_t num_prim,
                          const bt_polys* shadow, int64_t num_shadow, int32_t* tri, uint8_t* flag);
+
+/* ---- serving: continuous batching behind submit / poll ----
+ *
+ * The batched and served variants of the entry points above (no counterpart
+ * in the reference, whose GpuRenderer calls are synchronous, one image at a
+ * time: cuda/gpu_render.h:26-46).  Requests name a scene of the context's
+ * pool and carry host output buffers; bt_gpu_submit queues one and returns
+ * at once, bt_gpu_poll hands back finished ones.  Behind them, serving
+ * threads keep the scenes resident and run requests on lanes -- engine
+ * buffers and a stream of their own on the context's device, so that
+ * requests overlap on the GPU:
+ *  - soft-shadow requests go to the soft lane, whose engine run folds in
+ *    requests that arrive while it goes on: their roots join the rounds
+ *    already in flight (for fold_ms after the run started), and each request
+ *    is handed back as soon as its own roots are done;
+ *  - primary-id and point-shadow-mask requests go to `vis_lanes` lanes, one
+ *    request per lane at a time.
+ * Each result equals what bt_gpu_soft / bt_gpu_primary_ids / bt_gpu_point_mask
+ * give for the request alone.  Admission: a request is refused with
+ * BT_ERR_BUSY while the resident scenes, the lanes' sub-beam queue high-water
+ * mark and the requests already admitted would exceed memory_budget. */
+enum { BT_REQ_SOFT = 0, BT_REQ_PRIMARY_IDS = 1, BT_REQ_POINT_MASK = 2 };
+
+typedef struct {
+  int32_t kind;              /* BT_REQ_* */
+  int32_t scene;             /* scene id of the context's pool (0: the context's own) */
+  bt_camera cam;
+  bt_area_light light;       /* BT_REQ_SOFT */
+  bt_soft_opts opts;         /* BT_REQ_SOFT */
+  float point_light[3];      /* BT_REQ_POINT_MASK */
+  int32_t cull, tile;        /* BT_REQ_PRIMARY_IDS / BT_REQ_POINT_MASK (tile 0: 16) */
+  /* host outputs, W*H each, any may be NULL: ids (the scene's own, -1
+   * background), visibility, E, Eu (soft), mask (point) */
+  int32_t* tri;
+  float* vis;
+  float* E;
+  float* Eu;
+  uint8_t* mask;
+  uint64_t user;             /* handed back with the completion */
+} bt_request;
+
+typedef struct {
+  uint64_t ticket, user;
+  int32_t kind, status;      /* status: BT_OK or the request's error code */
+  double ms_queued;          /* submit to start (soft: to joining a run) */
+  double ms_total;           /* submit to hand-back */
+  char error[160];
+} bt_completion;
+
+typedef struct {
+  int32_t vis_lanes;         /* lanes for primary ids and point masks (0: 2) */
+  int32_t soft_jobs;         /* requests one soft run holds at most (0: 256) */
+  int64_t soft_pixels;       /* pixels one soft run holds at most (0: 8M) */
+  int64_t capacity;          /* sub-beam records per queue of each lane (0: the context's) */
+  double fold_ms;            /* soft requests join a running soft run this long after it starts (0: 100) */
+  int64_t memory_budget;     /* bytes (0: no limit) */
+} bt_serve_config;
+
+typedef struct {
+  int64_t submitted, completed, refused, queued, running;
+  int64_t soft_runs;         /* streaming soft runs so far */
+  int64_t soft_folded;       /* soft requests that joined a run after it had started */
+  int64_t scene_bytes;       /* the resident scene pool */
+  int64_t lane_bytes;        /* the lanes' engine buffers as allocated */
+  int64_t queue_high_water;  /* bytes of sub-beam records the lanes have needed at most */
+  int64_t admitted_bytes;    /* the requests in flight, as admission charges them */
+} bt_serve_stats;
+
+/* Starts serving with `cfg` (NULL: defaults); bt_gpu_submit starts it with
+ * defaults if this was not called.  BT_ERR_INVALID if already started. */
+BT_API int bt_gpu_serve_start(bt_gpu_ctx* ctx, const bt_serve_config* cfg);
+/* Queues a request; *ticket names it in its completion.  BT_ERR_BUSY: over
+ * the memory budget now (submit again later); BT_ERR_INVALID: bad request.
+ * The output buffers must stay valid until the request is handed back. */
+BT_API int bt_gpu_submit(bt_gpu_ctx* ctx, const bt_request* req, uint64_t* ticket);
+/* Hands back up to `cap` finished requests (in the order they finished),
+ * waiting up to wait_ms for the first (0: no wait, < 0: until one
+ * finishes or nothing is in flight). */
+BT_API int bt_gpu_poll(bt_gpu_ctx* ctx, bt_completion* out, int32_t cap, int32_t* count, int32_t wait_ms);
+BT_API int bt_gpu_serve_stats(bt_gpu_ctx* ctx, bt_serve_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -277,6 +277,8 @@ class RefGpu:
                                   C.c_void_p, C.c_void_p, C.c_void_p]
         lib.btrg_destroy.restype = None
         lib.btrg_destroy.argtypes = [C.c_void_p]
+        lib.btrg_primary_point.restype = None
+        lib.btrg_primary_point.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         self.lib = lib
         pos = np.ascontiguousarray(pos, np.float32)
         tris = np.ascontiguousarray(tris, np.uint32)
@@ -295,6 +297,18 @@ class RefGpu:
                            vis.ctypes.data, E.ctypes.data, tm.ctypes.data)
         return dict(tri=tri, vis=vis, E=E, primary_s=tm[0], trace_s=tm[1], kernel_s=tm[2], fallback_s=tm[3],
                     overflow_px=int(tm[4]))
+
+    def primary_point(self, cam, W, H, light, tile=16) -> dict:
+        """GpuRenderer::primary (tile roots) then pointShadows on its hit
+        polygons, each wall-clocked around the synchronous call."""
+        out = np.zeros(10)
+        cam = np.ascontiguousarray(cam, np.float64)
+        light = np.ascontiguousarray(light, np.float64)
+        self.lib.btrg_primary_point(self.h, cam.ctypes.data, int(W), int(H), int(tile), light.ctypes.data,
+                                    out.ctypes.data)
+        return dict(primary_s=out[0], point_s=out[1], hits=int(out[2]), shadow_polys=int(out[3]),
+                    primary_kernel_s=out[4], point_kernel_s=out[5], primary_overflow=int(out[6]),
+                    point_overflow=int(out[7]), primary_fallback_s=out[8], point_fallback_s=out[9])
 
     def close(self):
         if self.h:

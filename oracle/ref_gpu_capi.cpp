@@ -3,8 +3,10 @@
 // compiled for sm_100a from its sources by oracle/Makefile into
 // oracle/_ref/libbtref_gpu.so).  It measures the reference's wavefront
 // engine on the same scenes; nothing in the product links it.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "cuda/gpu_render.h"
 #include "render/render.h"
@@ -76,4 +78,43 @@ BTRG_API void btrg_soft(void* h, const double* cv, int W, int H, const double* l
   timing[2] = c->gpu->lastKernelSeconds;
   timing[3] = c->gpu->lastFallbackSeconds;
   timing[4] = double(c->gpu->lastOverflowPixels);
+}
+
+// GpuRenderer::primary (tile roots) and GpuRenderer::pointShadows on its
+// hit polygons, each wall-clocked around the synchronous call; out:
+// [primary s, point s, hit polygons, shadow polygons, primary kernel s,
+// point kernel s, primary overflow, point overflow, primary CPU-fallback s,
+// point CPU-fallback s].
+BTRG_API void btrg_primary_point(void* h, const double* cv, int W, int H, int tile, const double* light, double* out) {
+  Ctx* c = static_cast<Ctx*>(h);
+  Camera cam;
+  cam.eye = Vec3(Real(cv[0]), Real(cv[1]), Real(cv[2]));
+  cam.fwd = Vec3(Real(cv[3]), Real(cv[4]), Real(cv[5]));
+  cam.right = Vec3(Real(cv[6]), Real(cv[7]), Real(cv[8]));
+  cam.down = Vec3(Real(cv[9]), Real(cv[10]), Real(cv[11]));
+  cam.halfW = Real(cv[12]);
+  cam.halfH = Real(cv[13]);
+  cam.W = W;
+  cam.H = H;
+  std::vector<OutBeam> hits, shadow;
+  RenderStats rs;
+  auto t0 = std::chrono::steady_clock::now();
+  c->gpu->primary(cam, false, hits, rs, tile);
+  auto t1 = std::chrono::steady_clock::now();
+  out[4] = c->gpu->lastKernelSeconds;
+  out[6] = double(c->gpu->lastOverflowPixels);
+  out[8] = c->gpu->lastFallbackSeconds;
+  std::vector<OutBeam> visible;
+  for (const OutBeam& b : hits)
+    if (b.tri >= 0) visible.push_back(b);
+  auto t2 = std::chrono::steady_clock::now();
+  c->gpu->pointShadows(cam, visible, Vec3(Real(light[0]), Real(light[1]), Real(light[2])), shadow, rs);
+  auto t3 = std::chrono::steady_clock::now();
+  out[0] = std::chrono::duration<double>(t1 - t0).count();
+  out[1] = std::chrono::duration<double>(t3 - t2).count();
+  out[2] = double(visible.size());
+  out[3] = double(shadow.size());
+  out[5] = c->gpu->lastKernelSeconds;
+  out[7] = double(c->gpu->lastOverflowPixels);
+  out[9] = c->gpu->lastFallbackSeconds;
 }

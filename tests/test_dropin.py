@@ -71,3 +71,22 @@ def test_bt_render_cuda_soft_shadows(gpu, oracle_ready, tmp_path):
     assert np.all(vis[~m] == -1)
     err = np.abs(vis.astype(np.float64) - vd)[m]
     assert err.max() <= VIS_TOL, f"max |vis - fp64| {err.max():.3g}"
+
+
+def test_reference_gpu_test_program_through_the_shim(gpu):
+    """The reference's own GPU test program (cuda/test_cuda.cpp with its
+    test runner, built unchanged by `make -C oracle shim_tests` as
+    bt_tests_cuda) against the shim: soft shadows against its CPU tracer on
+    its analytic, plant and room scenes; primary and point-shadow polygons
+    rasterised at 384^2 with no interior pixel differing; two runs equal and
+    a budget of 4 with 4096-record queues still exact, its over-budget
+    pixels counted in lastOverflowPixels (retried on the GPU here, not on
+    the CPU)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "bt_tests_cuda")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/bt_tests_cuda not built")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    print(r.stdout + r.stderr)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "5/5 tests passed" in r.stdout + r.stderr
+    assert "no CUDA device" not in r.stderr

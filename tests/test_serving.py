@@ -1,121 +1,141 @@
-"""The serving loop (beamtrace2007_b200/serving.py): admission by memory
-budget and continuous batching (CPU, with a stand-in engine), and on the
-GPU a mixed Poisson stream over three resident scenes whose every result is
-bitwise the result of the same request run alone."""
-import threading
+"""Serving (bt_gpu_serve_start / bt_gpu_submit / bt_gpu_poll and the Python
+front, beamtrace2007_b200/serving.py): continuous batching with soft
+requests folded into a running engine run, lanes that overlap, admission by
+a memory budget, and every result bitwise the result of the same request
+run alone.  The argument checks run without a GPU; the rest on the GPU,
+including a C host (tests/native/serve_c_test.c) that submits and polls
+three mixed requests."""
+import ctypes as C
+import os
+import subprocess
 import time
 
 import numpy as np
 import pytest
 
-from conftest import scene
+from conftest import ROOT, scene
 
 
-class FakeEngine:
-    """Stands in for a GpuRenderer: records what ran together."""
-    log = []
-    lock = threading.Lock()
-
-    def __init__(self, ps, capacity):
-        self.ps = ps
-
-    def _note(self, what):
-        with FakeEngine.lock:
-            FakeEngine.log.append(what)
-        time.sleep(0.02)
-
-    def batch_soft(self, cams, lights, exact=True):
-        self._note(("batch", len(cams)))
-        from beamtrace2007_b200.renderer import SoftResult
-        return [SoftResult(np.zeros(c.W * c.H, np.int32), np.full(c.W * c.H, float(L[0]), np.float32),
-                           np.zeros(c.W * c.H, np.float32), np.zeros(c.W * c.H, np.float32)) for c, L in
-                zip(cams, lights)]
-
-    def soft_shadows(self, cam, L, exact=True):
-        return self.batch_soft([cam], [L], exact)[0]
-
-    def primary(self, cam, tile=16):
-        self._note(("primary", cam.W))
-        return None
-
-    def primary_ids(self, cam, tile=16):
-        self._note(("primary", cam.W))
-        return np.full((cam.H, cam.W), cam.W, np.int32)
-
-    def point_mask(self, cam, light, tile=16):
-        self._note(("point", cam.W))
-        return np.full((cam.H, cam.W), cam.W, np.int32), np.zeros((cam.H, cam.W), np.uint8)
-
-    def point_shadows(self, cam, prim, light):
-        return None
-
-    def raster(self, cam, prim, sh):
-        return np.full(cam.W * cam.H, cam.W, np.int32), np.zeros(cam.W * cam.H, np.uint8)
-
-    def close(self):
-        pass
+def test_serving_arguments_without_a_gpu(native_lib):
+    """Bad calls return status codes (no context here: nothing to serve)."""
+    from beamtrace2007_b200 import _native as N
+    q = N.Request()
+    t = C.c_uint64()
+    assert native_lib.bt_gpu_submit(None, C.byref(q), C.byref(t)) == -1
+    assert native_lib.bt_gpu_serve_start(None, None) == -1
+    cnt = C.c_int32(5)
+    assert native_lib.bt_gpu_poll(None, None, 0, C.byref(cnt), 0) == -1 and cnt.value == 0
+    assert native_lib.bt_gpu_serve_stats(None, None) == -1
 
 
-def test_admission_and_batching(native_lib):
-    from beamtrace2007_b200.serving import Request, Server, request_bytes
-    s, ps = scene("room")
-    scenes = {"a": s, "b": s}
-    FakeEngine.log = []
-    # a budget that holds the resident part and about eight 128^2 soft requests
-    probe = Request("soft", "a", 128, 128)
-    with Server(scenes, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine,
-                kd_on_gpu=False) as srv:
-        srv.budget = srv.resident + 8 * request_bytes(probe)
-        peak = [0]
-        reqs = []
-        for i in range(24):
-            r = Request("soft" if i % 3 else "primary", "ab"[i % 2], 128, 128, light_scale=1.0 + i)
-            reqs.append(srv.submit(r))
-            peak[0] = max(peak[0], srv.in_use)
+def _alone(srv, r):
+    """The request alone: soft shadows as a one-job batch on the server's
+    own context (bitwise the single-job path), primary ids and point masks
+    on a fresh context whose only scene is the request's."""
+    from beamtrace2007_b200.renderer import GpuRenderer
+    sc = srv.scenes[r.scene]
+    cam = srv.camera(r)
+    if r.kind == "soft":
+        [res] = [x for x in srv.engine.batch_soft([cam], [sc.data.light_array(r.light_scale)], exact=r.exact,
+                                                  scenes=[sc.id])]
+        return res
+    with GpuRenderer(sc.prepared, capacity=1 << 20) as g:
+        if r.kind == "primary":
+            return g.primary_ids(cam, tile=r.tile)
+        return g.point_mask(cam, np.asarray(sc.data.point_light, np.float32), tile=r.tile)[1]
+
+
+def _same(r, alone):
+    if r.kind == "soft":
+        return all(np.array_equal(getattr(r.result, k), getattr(alone, k)) for k in ("tri", "vis", "E", "Eu"))
+    return np.array_equal(r.result, alone)
+
+
+@pytest.mark.gpu
+def test_mixed_stream_same_as_alone(gpu):
+    from beamtrace2007_b200.serving import Server, poisson_stream
+    scenes = {"room": scene("room")[0], "plant": scene("plant")[0],
+              "building": scene("building", floors=1, furniture=2)[0]}
+    with Server(scenes, memory_budget_gb=8.0) as srv:
+        tuned = srv.tune(sizes=(64, 128), tiles=(8, 16), reps=1)
+        assert set(tuned) == {f"{s}/{w}" for s in scenes for w in (64, 128)}
+        reqs, summary = poisson_stream(srv, rate=200.0, n=40, sizes=(64, 96, 128), seed=3)
+        assert summary["errors"] == 0, [r.error for r in reqs if r.error]
+        assert summary["p99_ms"] >= summary["p50_ms"] > 0
         for r in reqs:
-            assert r.event.wait(30)
-        assert srv.in_use == 0
-    assert peak[0] <= 8 * request_bytes(probe)
-    assert all(r.error is None and r.done >= r.arrival for r in reqs)
-    # soft requests that waited together ran as one batch at least once
-    assert any(k == "batch" and n > 1 for k, n in FakeEngine.log)
-    for r in reqs:
-        if r.kind == "soft":
-            assert r.result.vis[0] == np.float32(r.result.vis[0])
+            assert _same(r, _alone(srv, r)), (r.kind, r.scene, r.W)
 
 
-class SlowSoftEngine(FakeEngine):
-    """A stand-in whose soft-shadow batches take 0.3 s."""
-
-    def batch_soft(self, cams, lights, exact=True):
-        time.sleep(0.3)
-        return super().batch_soft(cams, lights, exact)
-
-
-@pytest.mark.parametrize("workers", [1, 2])
-def test_primary_does_not_wait_behind_a_soft_batch(native_lib, workers):
-    """With two workers per scene, a primary request that arrives while a
-    long soft-shadow batch runs on the same scene is served by the other
-    worker; with one it waits for the batch."""
+@pytest.mark.gpu
+def test_soft_requests_fold_into_a_running_run(gpu):
+    """Soft requests submitted while a long soft run is going join it (the
+    library counts them as folded) and are handed back before it ends; each
+    equals the request alone."""
     from beamtrace2007_b200.serving import Request, Server
-    s, _ = scene("room")
-    with Server({"a": s}, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=SlowSoftEngine,
-                kd_on_gpu=False, workers_per_scene=workers) as srv:
-        soft = srv.submit(Request("soft", "a", 64, 64))
-        time.sleep(0.05)
-        prim = srv.submit(Request("primary", "a", 64, 64))
-        assert soft.event.wait(30) and prim.event.wait(30)
-    assert soft.error is None and prim.error is None
-    if workers == 2:
-        assert prim.done < soft.done and prim.latency < 0.2
-    else:
-        assert prim.done >= soft.done
+    with Server({"plant": scene("plant")[0]}, memory_budget_gb=8.0, fold_ms=10_000.0) as srv:
+        big = srv.submit(Request("soft", "plant", 512, 512, light_scale=4.0))
+        time.sleep(0.004)
+        small = [srv.submit(Request("soft", "plant", 48, 48, view=0, light_scale=0.5 + 0.25 * i)) for i in range(6)]
+        for r in [big] + small:
+            assert r.event.wait(120) and r.error is None, r.error
+        st = srv.stats()
+        assert st["soft_folded"] >= 1, st
+        assert st["soft_runs"] < 1 + len(small), st
+        # the small requests that joined the big run came back before it
+        assert min(r.done for r in small) < big.done
+        for r in [big] + small:
+            assert _same(r, _alone(srv, r))
 
 
-def test_config_scenes_through_the_cache(native_lib, tmp_path):
+@pytest.mark.gpu
+def test_primary_does_not_wait_behind_a_soft_run(gpu):
+    """A primary request that arrives while a long soft run is going runs on
+    a visibility lane at the same time and comes back first."""
+    from beamtrace2007_b200.serving import Request, Server
+    with Server({"plant": scene("plant")[0]}, memory_budget_gb=8.0, fold_ms=1.0) as srv:
+        soft = srv.submit(Request("soft", "plant", 512, 512, light_scale=4.0))
+        time.sleep(0.004)
+        prim = srv.submit(Request("primary", "plant", 64, 64))
+        assert soft.event.wait(120) and prim.event.wait(120)
+        assert soft.error is None and prim.error is None
+        assert prim.done < soft.done
+        assert _same(prim, _alone(srv, prim))
+
+
+@pytest.mark.gpu
+def test_admission_by_memory_budget(gpu):
+    """A budget that holds the resident scene and a few requests: the
+    library refuses the rest for a while (BT_ERR_BUSY), the front submits
+    them again as memory frees, every request completes and equals the
+    request alone, and the memory charged to admitted requests never exceeds
+    what the budget leaves."""
+    from beamtrace2007_b200.serving import Request, Server
+    s, ps = scene("room")
+    with Server({"room": s}, memory_budget_gb=8.0, queue_records=1 << 16) as srv:
+        scene_bytes = srv.stats()["scene_bytes"]
+    one = 128 * 128 * 40 + 128 * 128 * 68   # what admission charges a 128^2 soft request
+    budget = scene_bytes + 3 * one + one // 2
+    with Server({"room": s}, memory_budget_gb=budget / (1 << 30), queue_records=1 << 16) as srv:
+        reqs = [srv.submit(Request("soft" if i % 3 else "primary", "room", 128, 128, light_scale=0.5 + 0.1 * i))
+                for i in range(18)]
+        peak = 0
+        while not all(r.event.is_set() for r in reqs):
+            peak = max(peak, srv.stats()["admitted_bytes"])
+            time.sleep(0.001)
+        assert all(r.error is None for r in reqs), [r.error for r in reqs if r.error]
+        st = srv.stats()
+        assert st["refused"] > 0 and st["completed"] == len(reqs), st
+        assert peak <= budget - scene_bytes, (peak, st)
+        for r in reqs:
+            assert _same(r, _alone(srv, r))
+
+
+@pytest.mark.gpu
+def test_config_scenes_through_the_cache(gpu, tmp_path):
     """Scenes given as the reference's configs are ingested and prepared
     once; a second server on the same cache directory admits them from the
-    stored arrays.  Requests use the config's views and lights."""
+    stored arrays.  Requests use the config's views and lights and give the
+    same results from both."""
     from beamtrace2007_b200.ingest import SceneCache
     from beamtrace2007_b200.serving import Request, Server
     cfg = tmp_path / "room.cfg"
@@ -125,48 +145,33 @@ def test_config_scenes_through_the_cache(native_lib, tmp_path):
     results = []
     for run in range(2):
         cache = SceneCache(store)
-        with Server({"room": str(cfg)}, memory_budget_gb=1.0, queue_records=1 << 10, engine_factory=FakeEngine,
-                    cache=cache, kd_on_gpu=False) as srv:
-            slot = srv.slots["room"]
-            assert len(slot.data.views) == 8
-            assert np.array_equal(np.float32(slot.data.point_light), np.float32([5.5, 2.6, 2.5]))
+        with Server({"room": str(cfg)}, memory_budget_gb=1.0, queue_records=1 << 16, cache=cache) as srv:
+            sc = srv.scenes["room"]
+            assert len(sc.data.views) == 8
+            assert np.array_equal(np.float32(sc.data.point_light), np.float32([5.5, 2.6, 2.5]))
             reqs = [srv.submit(Request(k, "room", 64, 48, view=3)) for k in ("primary", "point", "soft")]
             for r in reqs:
-                assert r.event.wait(30) and r.error is None
+                assert r.event.wait(60) and r.error is None
             results.append([r.result for r in reqs])
         assert (cache.misses, cache.disk_hits) == ((1, 0) if run == 0 else (0, 1))
-    assert np.array_equal(results[0][0], results[1][0])
+    assert np.array_equal(results[0][0], results[1][0]) and np.array_equal(results[0][1], results[1][1])
+    assert np.array_equal(results[0][2].vis, results[1][2].vis)
 
 
 @pytest.mark.gpu
-def test_mixed_stream_same_as_alone(gpu):
-    from beamtrace2007_b200.serving import Server, poisson_stream
-    scenes = {"room": scene("room")[0], "plant": scene("plant")[0],
-              "building": scene("building", floors=1, furniture=2)[0]}
-    with Server(scenes, memory_budget_gb=8.0) as srv:
-        tuned = srv.tune(sizes=(64, 128), tiles=(8, 16))
-        assert set(tuned) == {f"{s}/{w}" for s in scenes for w in (64, 128)}
-        reqs, summary = poisson_stream(srv, rate=200.0, n=30, sizes=(64, 96, 128), seed=3)
-        assert summary["errors"] == 0, [r.error for r in reqs if r.error]
-        assert summary["p99_ms"] >= summary["p50_ms"] > 0
-        # each request again, alone, on the same resident scene
-        for r in reqs:
-            slot = srv.slots[r.scene]
-            cam = srv._camera(slot, r)
-            if r.kind == "soft":
-                alone = slot.engine.soft_shadows(cam, slot.data.light_array(r.light_scale), exact=r.exact)
-                for k in ("tri", "vis", "E", "Eu"):
-                    assert np.array_equal(getattr(r.result, k), getattr(alone, k)), (r.kind, k)
-            else:
-                # alone, and through the host polygon path
-                prim = slot.engine.primary(cam, tile=r.tile)
-                if r.kind == "primary":
-                    tri, _ = slot.engine.raster(cam, prim, None)
-                    assert np.array_equal(r.result, tri)
-                else:
-                    sh = slot.engine.point_shadows(cam, prim, np.asarray(slot.data.point_light, np.float32))
-                    _, flag = slot.engine.raster(cam, prim, sh)
-                    assert np.array_equal(r.result, flag)
+def test_c_host_submits_and_polls(gpu):
+    """tests/native/serve_c_test.c, built here against libbt_gpu.so: three
+    mixed requests through bt_gpu_submit / bt_gpu_poll, each bitwise the
+    synchronous call's result."""
+    out = os.path.join(ROOT, "tests", "native", "_serve_c_test")
+    src = os.path.join(ROOT, "tests", "native", "serve_c_test.c")
+    lib = os.path.join(ROOT, "beamtrace2007_b200")
+    subprocess.run(["gcc", "-std=c11", "-O2", "-I" + os.path.join(ROOT, "include"), src, "-L" + lib, "-lbt_gpu",
+                    "-Wl,-rpath," + lib, "-o", out], check=True)
+    r = subprocess.run([out, "96"], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "serve_c_test: ok" in r.stdout
 
 
 @pytest.mark.gpu

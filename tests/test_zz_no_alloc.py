@@ -124,20 +124,113 @@ def test_noalloc_matches_device_entry_point(gpu):
         assert np.all(vis[~m] == -1)
 
 
+def _defect(ps, what):
+    """Host copies of the kd-tree and triangle arrays with one index made
+    invalid; returns (array name, the bad copy, the phrase the error names)."""
+    if what == "child":
+        # an interior node whose child index points back at itself
+        data = ps.kd_data.copy()
+        i = int(np.nonzero((data & 3) != 3)[0][-1])
+        data[i] = (np.uint32(i) << np.uint32(2)) | (data[i] & np.uint32(3))
+        return "data", data, (b"kd node",)
+    if what == "leaf":
+        # a leaf whose reference range runs one past the end of the list
+        data, offset = ps.kd_data, ps.kd_offset.copy()
+        leaves = np.nonzero(((data & 3) == 3) & ((data >> 2) > 0))[0]
+        i = int(leaves[0])
+        offset[i] = np.uint32(len(ps.kd_tri_indices) - int(data[i] >> 2) + 1)
+        return "offset", offset, (b"kd node",)
+    if what == "reference":
+        # a leaf reference to a triangle past the last one
+        idx = ps.kd_tri_indices.copy()
+        idx[0] = np.uint32(len(ps.tris))
+        return "idx", idx, (b"kd reference",)
+    # a referenced triangle whose last vertex index is past the last vertex
+    # (found through its reference, or through the triangle itself when the
+    # index is its first)
+    tris = ps.tris.copy()
+    tris[int(ps.kd_tri_indices[0]), 2] = np.uint32(len(ps.pos) + 5)
+    return "tris", tris, (b"kd reference", b"triangle")
+
+
 @pytest.mark.gpu
-def test_noalloc_rejects_a_malformed_tree(gpu):
-    """A kd node whose child index points backwards: BT_ERR_INVALID from the
-    packing kernel's own index checks (no access goes out of range)."""
+def test_noalloc_rejects_malformed_inputs(gpu):
+    """A child index pointing backwards, a leaf range past the reference
+    list, a reference past the last triangle and a vertex index past the
+    last vertex: each returns BT_ERR_INVALID naming what is malformed (the
+    packing kernel checks every index before it uses it, so no access goes
+    out of range), and a valid call after them still gives the context
+    entry point's results."""
     import torch
     from beamtrace2007_b200 import _native as N
+    from beamtrace2007_b200.renderer import GpuRenderer, make_camera
     s, ps = scene("room")
-    sd, kd, keep = _device_scene(ps)
-    data = ps.kd_data.copy()
-    i = int(np.nonzero((data & 3) != 3)[0][-1])
-    data[i] = (np.uint32(i) << np.uint32(2)) | (data[i] & np.uint32(3))
-    bad = torch.from_numpy(data.view(np.int32)).cuda()
-    kd.data = bad.data_ptr()
+    light = N.AreaLight.from_array(s.light_array())
     opts = N.SoftOpts()
+    opts.exact = 1
+    fields = {"data": "data", "offset": "offset", "idx": "tri_indices", "tris": "tris"}
+    for what in ("child", "leaf", "reference", "vertex"):
+        sd, kd, keep = _device_scene(ps)
+        name, arr, phrases = _defect(ps, what)
+        bad = torch.from_numpy(np.ascontiguousarray(arr).view(np.int32)).cuda()
+        setattr(sd if name == "tris" else kd, fields[name], bad.data_ptr())
+        torch.cuda.synchronize()
+        assert _call(sd, kd, light, opts, 0, None, None, None, None, None, None) == -1, what
+        msg = N.lib().bt_gpu_last_error()
+        assert any(p in msg for p in phrases), (what, msg)
+    # the next valid call, on points, against the context entry point
+    v = s.views[0]
+    W, H = 48, 40
+    n = W * H
+    cam = make_camera(v.eye, v.target, v.fov, s.up, W, H)
+    dev = torch.device("cuda:0")
+    with GpuRenderer(ps) as g:
+        tri = np.zeros(n, np.int32)
+        X = np.zeros(3 * n, np.float32)
+        Nn = np.zeros(3 * n, np.float32)
+        N.check(N.lib().bt_gpu_primary_rays(g._h, C.byref(cam), N.ptr(tri), N.ptr(X), N.ptr(Nn)))
+        dtri, dX, dN = (torch.from_numpy(a).to(dev) for a in (tri, X, Nn))
+        ref = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
+        torch.cuda.synchronize()
+        N.check(N.lib().bt_gpu_soft_points_device(g._h, C.byref(light), C.byref(opts), n, dtri.data_ptr(),
+                                                  dX.data_ptr(), dN.data_ptr(), *(r.data_ptr() for r in ref), None))
+    sd, kd, keep = _device_scene(ps)
+    out = [torch.full((n,), 7.0, dtype=torch.float32, device=dev) for _ in range(3)]
     torch.cuda.synchronize()
-    assert _call(sd, kd, N.AreaLight.from_array(s.light_array()), opts, 0, None, None, None, None, None, None) == -1
-    assert b"kd node" in N.lib().bt_gpu_last_error()
+    N.check(_call(sd, kd, light, opts, n, dtri.data_ptr(), dX.data_ptr(), dN.data_ptr(),
+                  *(o.data_ptr() for o in out)))
+    rv, rE, _ = (r.cpu().numpy() for r in ref)
+    vis, E, _ = (o.cpu().numpy() for o in out)
+    assert (tri >= 0).sum() > n // 4
+    assert np.abs(vis - rv).max() <= VIS_TOL
+    assert np.abs(E - rE).max() <= E_REL * np.abs(rE).max()
+
+
+def test_retry_reserve_of_the_fixed_queues(native_lib):
+    """The queues of the allocation-free call get what the scratch array
+    leaves after the scene and the points (the layout of the header's limit:
+    44 B per kd node, 64 per reference, 32 per triangle, 164 per point, each
+    section rounded up to 256 B, plus a few small sections of counters); a
+    root over its live sub-beam budget is retried with 16 times the budget
+    only while that reserve fits one queue.  For the room scene at 128 x 96
+    points that is two retries (budget 128 -> 2048 -> 32768; 524288 does not
+    fit), against four on a context's 2^23-record queues, as the header
+    states."""
+    from beamtrace2007_b200 import _native as N
+    _, ps = scene("room")
+    cfg = N.GpuConfig()
+    N.lib().bt_gpu_config_default(C.byref(cfg))
+
+    def r256(b):
+        return (b + 255) // 256 * 256
+    nn, nr, nt, n = len(ps.kd_split), len(ps.kd_tri_indices), len(ps.tris), 128 * 96
+    scene_and_points = (r256(8 * nn) + r256(32 * nn) + r256(4 * nn) + r256(64 * nr) + r256(32 * nt) + r256(96 * n)
+                        + 5 * r256(4 * n) + 2 * r256(8 * n) + r256(32 * n))
+    limit = 64 << 20
+    caps = [(limit - scene_and_points - small) // (3 * 64) for small in (0, 16 << 10)]
+
+    def retries(cap):
+        return max(p for p in range(8) if max(cfg.budget, 32) * 16 ** p <= cap)
+    assert [retries(c) for c in caps] == [2, 2]
+    assert retries(1 << 23) == cfg.max_retries == 4
+    assert all(300_000 < c < 349_526 for c in caps)
