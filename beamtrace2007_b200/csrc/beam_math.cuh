@@ -522,12 +522,11 @@ BT_HD int decide(const Query& q, const Beam& b, int a, float Ns, const Box& box)
     float exit = pos ? boxHi(box, c) : boxLo(box, c);
     float Nmin = s * (entry - Oc);
     float Nmax = s * (exit - Oc);
-    float lhs[4], rhs[4], tl[4];
+    float lhs[4], tl[4];
     for (int i = 0; i < 4; ++i) {
       lhs[i] = awAt(b, c, i) * Ns;
       float r = awAt(b, a, i) * Nmin;
       float tol = (fabs_(lhs[i]) + fabs_(r)) * kKdRel;
-      rhs[i] = r;
       tl[i] = r - tol;
     }
     if (all4lt(lhs, tl)) return kFar;

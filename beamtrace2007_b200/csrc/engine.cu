@@ -1908,13 +1908,18 @@ int bt_gpu_create(const bt_scene_desc* scene, const bt_kd_desc* kd, const bt_gpu
     for (auto& ev : c->kev)
       if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   if ((e = uploadScene(c, scene, kd))) return fail(e);
-  // Sub-beam queues: three of `capacity` 64-byte records.  Default 2^23
-  // records (512 MiB each), at most 10% of the free memory.
+  // Sub-beam queues: three of `capacity` 64-byte records.  Default 2^25
+  // records (2 GiB each), at most 10% of the free memory.  Admission
+  // reserves a root's whole budget of queue slots, so the capacity bounds
+  // the roots in flight: primary tiles (budget 4096) over dense meshes need
+  // 2^25 to admit 1024^2 at 8 x 8 tiles at once (2^23 left them to four
+  // waves of admission and 1.3-1.8x the time; soft roots of budget 128 are
+  // not bound by it).
   int64_t cap = c->cfg.capacity;
   if (cap <= 0) {
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    cap = std::min<int64_t>(int64_t(1) << 23, int64_t(fr / 10 / (3 * sizeof(SubBeam))));
+    cap = std::min<int64_t>(int64_t(1) << 25, int64_t(fr / 10 / (3 * sizeof(SubBeam))));
   }
   cap = std::max<int64_t>(cap, 1024);
   cap = std::min<int64_t>(cap, int64_t(1) << 30);

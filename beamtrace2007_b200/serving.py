@@ -73,9 +73,10 @@ class Request:
 
 def primary_tile(r: Request) -> int:
     """Pixels per side of a primary root when the scene and size were not
-    tuned: 16 (the reference's tile) from 512 pixels up; 8 below, where 16
-    leaves too few roots to fill the GPU."""
-    return 16 if min(r.W, r.H) >= 512 else 8
+    tuned: 8 from 512 pixels up, 4 below (the reference's 16 leaves too few
+    roots to fill the GPU on dense meshes: 1024^2 of the displaced sphere in
+    26 ms at 8 against 34 ms at 16; 256^2 in 34 ms at 4 against 126 at 16)."""
+    return 8 if min(r.W, r.H) >= 512 else 4
 
 
 class _Scene:
@@ -89,7 +90,7 @@ class _Scene:
 class Server:
     """Resident scenes on one GPU behind the library's request loop."""
 
-    def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 21,
+    def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 24,
                  cache=None, kd_on_gpu: bool = True, vis_lanes: int = 2, fold_ms: float = 100.0,
                  soft_pixels: int = 8 << 20):
         from .ingest import SceneCache
@@ -130,7 +131,7 @@ class Server:
     def slots(self):
         return self.scenes
 
-    def tune(self, sizes=(256, 512, 1024), tiles=(8, 16, 32), reps: int = 2):
+    def tune(self, sizes=(256, 512, 1024), tiles=(4, 8, 16, 32), reps: int = 2):
         """Autotunes the primary tile of every resident scene at each square
         size: each candidate's primary request is timed through the serving
         lanes (the fastest of `reps` after a warm-up).  Call before the

@@ -111,7 +111,8 @@ typedef struct {
   int32_t device;           /* CUDA device ordinal */
   int32_t budget;           /* live sub-beams per soft/point root before a retry (wfBudget) */
   int32_t primary_budget;   /* live sub-beams per primary tile (wfPrimaryBudget) */
-  int64_t capacity;         /* sub-beam records per spill queue (wfCapacity); 0 = from free memory */
+  int64_t capacity;         /* sub-beam records per spill queue (wfCapacity); 0 = 2^25, at most a tenth of
+                               the free device memory over the three queues */
   int32_t blocks_per_sm;    /* persistent CTAs per SM; 0 = occupancy */
   int32_t kernel_timing;    /* nonzero: CUDA events around the trace kernels fill ms_kernel_trace */
   int32_t max_retries;      /* budget x16 retries before BT_ERR_CAPACITY */
