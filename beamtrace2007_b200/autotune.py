@@ -33,22 +33,31 @@ def _best(timings: dict):
 
 
 def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, 30000, -1),
-                capacities=(0,), yield_pcts=(0,), reps: int = 2, device: int = 0):
+                capacities=(0,), yield_pcts=(0,), budgets=None, reps: int = 2, device: int = 0):
     """Times `reps` soft-shadow frames (after one warm-up) for every
     combination of the candidate settings; returns (best settings as
-    GpuRenderer keyword arguments, {settings tuple: best ms})."""
+    GpuRenderer keyword arguments, {settings tuple: best ms}).  `budgets`:
+    candidate live sub-beam budgets per root (a root over it is retried with
+    16x; dense meshes under large lights prefer larger ones); None keeps the
+    default and the 4-tuple keys."""
     from .renderer import GpuRenderer
     timings = {}
-    for bps, tail, cap, yp in itertools.product(blocks_per_sm, tail_records, capacities, yield_pcts):
+    for bps, tail, cap, yp, bud in itertools.product(blocks_per_sm, tail_records, capacities, yield_pcts,
+                                                     budgets or (None,)):
+        kw = {} if bud is None else {"budget": bud}
         with GpuRenderer(scene, device=device, blocks_per_sm=bps, tail_records=tail, capacity=cap,
-                         yield_pct=yp) as g:
+                         yield_pct=yp, **kw) as g:
             g.soft_shadows(cam, light, exact=exact)
             ms = []
             for _ in range(reps):
                 ms.append(g.soft_shadows(cam, light, exact=exact).info["ms_total"])
-        timings[(bps, tail, cap, yp)] = min(ms)
-    bps, tail, cap, yp = _best(timings)
-    return {"blocks_per_sm": bps, "tail_records": tail, "capacity": cap, "yield_pct": yp}, timings
+        key = (bps, tail, cap, yp) if budgets is None else (bps, tail, cap, yp, bud)
+        timings[key] = min(ms)
+    best = _best(timings)
+    out = {"blocks_per_sm": best[0], "tail_records": best[1], "capacity": best[2], "yield_pct": best[3]}
+    if budgets is not None:
+        out["budget"] = best[4]
+    return out, timings
 
 
 def tune_tile(renderer, cam, tiles=(8, 16, 32), reps: int = 2):

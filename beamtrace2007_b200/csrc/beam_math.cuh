@@ -842,9 +842,12 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
     }
   }
   bool ok = true;
-  // pending pentagon halves (LIFO), with the line each resumes at
-  Poly<N> stack[8];
-  int stackLine[8];
+  // pending pentagon halves (LIFO), with the line each resumes at.  A half
+  // pushed at line li resumes at li + 1 and everything pushed above it
+  // resumes later still, so the lines on the stack rise strictly from
+  // bottom to top: at most one entry per line, five at most.
+  Poly<N> stack[5];
+  int stackLine[5];
   int sp = 0;
   Poly<N> p;
   p.n = B.n;
@@ -881,7 +884,7 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
         Poly<N> a, b;
         splitFive(in, a, b);
         fiveSplits++;
-        if (sp >= 8) return false;
+        if (sp >= 5) return false;
         stack[sp] = b;
         stackLine[sp] = li + 1;
         ++sp;

@@ -104,8 +104,10 @@ struct Mesh {
     tri(i, k, l, m);
   }
 
-  // Axis box on 8 shared corners (corner k takes hi on the axes of its set
-  // bits); faces counter-clockwise seen from outside, or from inside.
+  // The box lo..hi on its eight corners (bit a of a corner's number picks
+  // hi on axis a), so neighbouring faces share vertices; each face is two
+  // triangles wound counter-clockwise when looked at from outside (with
+  // `inward`, from inside).
   void box(V lo, V hi, uint16_t m, bool inward = false) {
     static const int kFaces[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4},
                                      {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
@@ -188,8 +190,9 @@ struct Mesh {
     }
   }
 
-  // Wall slab along x (axis 0) or z (axis 2), with a 1.2 x 2.2 m door gap
-  // in the middle when `door`.
+  // A wall: a box `thick` deep running `len` from o along x (axis 0) or z
+  // (axis 2); with `door`, two side slabs and a lintel leave a 1.2 m wide,
+  // 2.2 m high opening at the middle.
   void wall(V o, int axis, float len, float height, float thick, bool door, uint16_t m) {
     auto slab = [&](float a0, float a1, float y0, float y1) {
       if (axis == 0)

@@ -401,14 +401,20 @@ def batched_measure(g, s, N, lib, C, steps):
 
 
 def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: int = 200_000, reps: int = 1,
-                         seed: int = 2024):
+                         seed: int = 2024, tune: bool = True):
     """The batched-jobs workload: receiver/occluder pairs (icosphere or
     torus, meshes log-uniform between 100 and `max_tris` triangles, plus a
     ground quad), square resolutions from `sizes`, light scale U[0.25, 4],
     exact; all jobs in one engine run (scene pool, bt_gpu_batch_soft)
     against the same jobs one by one; device time from the engine's CUDA
-    events."""
+    events.  kd-trees are built on the GPU.  With `tune`, the autotuner
+    (autotune.tune_engine) picks the live sub-beam budget on the heaviest
+    job at 64x64 before the runs.  The warm-up is one small job (a pass of
+    the whole mix can take tens of seconds); `heaviest`: the two longest
+    jobs alone, with their triangle tests (the algorithm's work: the engine's
+    counters equal the reference's)."""
     from beamtrace2007_b200 import scenes
+    from beamtrace2007_b200.autotune import tune_engine
     from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
     rng = np.random.default_rng(seed)
     specs = [(int(np.exp(rng.uniform(np.log(100), np.log(max_tris)))), int(rng.choice(list(sizes))),
@@ -417,32 +423,48 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
     jobs = []
     for i, (tris, res, scale) in enumerate(specs):
         sd = scenes.shadow_job(100 + i, tris)
-        jobs.append((sd, PreparedScene(sd.pos, sd.tris), res, scale))
+        jobs.append((sd, PreparedScene(sd.pos, sd.tris, kd_device=0), res, scale))
     prep_s = time.perf_counter() - t0
-    g = GpuRenderer(jobs[0][1])
-    ids = [0] + [g.add_scene(ps) for _, ps, _, _ in jobs[1:]]
     cams, lights = [], []
     for sd, ps, res, scale in jobs:
         v = sd.views[0]
         cams.append(make_camera(v.eye, v.target, v.fov, sd.up, res, res))
         lights.append(sd.light_array(scale))
+    settings, tuned = {}, None
+    if tune:
+        h = max(range(len(jobs)), key=lambda k: jobs[k][1].num_tris * lights[k][3:6].dot(lights[k][3:6]))
+        sd, ps, _, _ = jobs[h]
+        v = sd.views[0]
+        probe = make_camera(v.eye, v.target, v.fov, sd.up, 64, 64)
+        settings, timings = tune_engine(ps, probe, lights[h], budgets=(128, 512, 2048), blocks_per_sm=(0,),
+                                        tail_records=(0,), reps=1)
+        tuned = {"settings": settings, "probe": f"job {h} ({ps.num_tris} tris) at 64x64",
+                 "ms": {str(k): round(t, 2) for k, t in timings.items()}}
+    g = GpuRenderer(jobs[0][1], **settings)
+    ids = [0] + [g.add_scene(ps) for _, ps, _, _ in jobs[1:]]
     px = sum(c.W * c.H for c in cams)
-    batch, plain = [], []
-    for rep in range(reps + 1):
+    small = min(range(len(jobs)), key=lambda k: cams[k].W * jobs[k][1].num_tris)
+    g.batch_soft([cams[small]], [lights[small]], exact=True, scenes=[ids[small]], device_outputs=True)  # warm-up
+    batch, plain, alone = [], [], {}
+    for rep in range(reps):
         _, info = g.batch_soft(cams, lights, exact=True, scenes=ids, device_outputs=True)
+        batch.append(info["ms_total"])
         t = 0.0
         for k in range(len(cams)):
             _, i1 = g.batch_soft([cams[k]], [lights[k]], exact=True, scenes=[ids[k]], device_outputs=True)
             t += i1["ms_total"]
-        if rep:  # the first pass warms up
-            batch.append(info["ms_total"])
-            plain.append(t)
+            alone[k] = (i1["ms_total"], i1["tri_tests"])
+        plain.append(t)
     g.close()
     pb, pp = float(np.median(batch)), float(np.median(plain))
+    top = sorted(alone, key=lambda k: -alone[k][0])[:2]
     return {"jobs": len(jobs), "triangles": int(sum(ps.num_tris for _, ps, _, _ in jobs)), "pixels": int(px),
-            "sizes": list(sizes), "max_tris": max_tris,
+            "sizes": list(sizes), "max_tris": max_tris, "reps": reps,
             "value": px / pb * 1e3, "unit": "px/s", "one_by_one_value": px / pp * 1e3, "ratio_vs_one_by_one": pp / pb,
-            "ms_batch": pb, "ms_one_by_one": pp, "host_prep_s": prep_s}
+            "ms_batch": pb, "ms_one_by_one": pp, "host_prep_s": prep_s, "autotuned": tuned,
+            "heaviest": [{"job": k, "tris": jobs[k][1].num_tris, "res": cams[k].W, "light_scale": round(specs[k][2], 3),
+                          "ms": round(alone[k][0], 1), "tri_tests": int(alone[k][1]),
+                          "share_of_one_by_one": round(alone[k][0] / pp, 3)} for k in top]}
 
 
 def serving_measure(n: int = 300):
@@ -489,6 +511,9 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--capacity", type=int, default=0,
                     help="sub-beam records per queue (0: the engine's default); small values for profiler captures")
+    ap.add_argument("--scene", default="plant", choices=["plant", "sphere"],
+                    help="profiling only: 'sphere' renders the displaced icosphere (327,680 triangles, larger than "
+                         "L2 with its tree) instead of the plant; the benchmark's workload is the plant")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -503,7 +528,7 @@ def main():
     from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
 
     torch.cuda.set_device(local)
-    s = scenes.plant()
+    s = scenes.plant() if args.scene == "plant" else scenes.displaced_sphere()
     ps = PreparedScene(s.pos, s.tris)
     v = s.views[0]
     cam = make_camera(v.eye, v.target, v.fov, s.up, W, H)
@@ -572,7 +597,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "px/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plant scene)",
-            "config": dict(workload_config(), parallelism=f"replicas{ws}"),
+            "config": dict(workload_config(), parallelism=f"replicas{ws}") if args.scene == "plant" else
+            {"workload": "profiling run: displaced icosphere 327,680 tris, exact soft shadows 512x512 (not the "
+                         "benchmark's workload)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "traceKernel<soft>",
@@ -594,9 +621,12 @@ def main():
             "ms_trace": float(np.mean([d["ms_trace"] for d in infos]))}
     if not args.no_extras and ws == 1:  # (at N > 1 the other GPUs would wait on rank 0's extras)
         line["batched"] = batched_measure(g, s, N, lib, C, steps=3)
-        # the batched-jobs workload at bounded size (the full 64 jobs of up to
-        # 200K triangles at up to 512^2 take minutes per batch)
-        line["batched_jobs"] = batched_jobs_measure(n_jobs=32, max_tris=20_000, sizes=(64, 128))
+        # the batched-jobs workload as configured (64 jobs of up to 200K
+        # triangles at up to 512^2), one repetition; and a mix of small jobs
+        # (32 jobs of <= 20K triangles at 64-128^2) with three
+        line["batched_jobs"] = batched_jobs_measure()
+        line["batched_jobs_small"] = batched_jobs_measure(n_jobs=32, max_tris=20_000, sizes=(64, 128), reps=3,
+                                                          tune=False)
         line["visibility"] = visibility_measure()
         line["serving"] = serving_measure()
     if not args.no_cpu_baseline and ws == 1:
