@@ -193,6 +193,7 @@ SIGNATURES = {
     "bt_gpu_point_mask_device": (_I, [_P, C.POINTER(Camera), C.c_int32, C.c_int32, _P, _P, _P,
                                       C.POINTER(RunInfo)]),
     "bt_gpu_raster": (_I, [_P, C.POINTER(Camera), C.POINTER(Polys), _I64, C.POINTER(Polys), _I64, _P, _P]),
+    "bt_gpu_last_polys": (_I, [_P, C.POINTER(Polys), C.POINTER(_I64)]),
     "bt_gpu_serve_start": (_I, [_P, C.POINTER(ServeConfig)]),
     "bt_gpu_submit": (_I, [_P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
     "bt_gpu_poll": (_I, [_P, C.POINTER(Completion), C.c_int32, C.POINTER(C.c_int32), C.c_int32]),

@@ -1258,6 +1258,8 @@ struct bt_gpu_ctx {
   int* dKillCount = nullptr;
   // outputs
   int64_t outCap = 0;
+  int64_t lastProduced = -1;  // polygons of the last bt_gpu_primary / bt_gpu_point (bt_gpu_last_polys)
+  int lastRoots = 0;
   float *dOx = nullptr, *dOy = nullptr, *dOarea = nullptr;
   int32_t *dOn = nullptr, *dOtri = nullptr, *dOroot = nullptr, *dOatt = nullptr;
   // per-image scratch
@@ -1458,6 +1460,7 @@ struct RoundRunner {
 
   // Clears the per-run state of R roots and sets the launch parameters.
   int begin(const AppParams& app0, int R) {
+    c->lastProduced = -1;  // a new run overwrites what bt_gpu_last_polys would read
     int e = ensureRoots(c, size_t(R));
     if (e) return e;
     CK(cudaMemsetAsync(c->dAttempt, 0, sizeof(int32_t) * size_t(R), c->stream));
@@ -2418,6 +2421,8 @@ int bt_gpu_primary(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t ti
       info->ms_trace = b;
       info->ms_total = b;
     }
+    c->lastProduced = hc.outCount;
+    c->lastRoots = R;
     return downloadPolys(c, hc.outCount, R, out, count);
   }
 }
@@ -2471,8 +2476,23 @@ int bt_gpu_point(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* hits, int6
       info->ms_trace = b;
       info->ms_total = b;
     }
+    c->lastProduced = hc.outCount;
+    c->lastRoots = int(nh);
     return downloadPolys(c, hc.outCount, int(nh), out, count);
   }
+}
+
+int bt_gpu_last_polys(bt_gpu_ctx* c, bt_polys* out, int64_t* count) {
+  if (!c || !out || !count) {
+    setErr("bt_gpu_last_polys: bad arguments");
+    return BT_ERR_INVALID;
+  }
+  if (c->lastProduced < 0) {
+    setErr("bt_gpu_last_polys: no polygons kept (the last engine call was not bt_gpu_primary / bt_gpu_point)");
+    return BT_ERR_INVALID;
+  }
+  CK(cudaSetDevice(c->device));
+  return downloadPolys(c, c->lastProduced, c->lastRoots, out, count);
 }
 
 int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int64_t np, const bt_polys* shadow,

@@ -328,35 +328,40 @@ class GpuRenderer:
         return SoftResult(tri, vis[:n], E[:n], Eu[:n], self._record(info))
 
     # ---- primary visibility and point shadows
+    def _fetch_rest(self, out: PolyList, n: int) -> PolyList:
+        """The last call produced n > len(out) polygons: fetch them all again
+        from the device (bt_gpu_last_polys) instead of repeating the call."""
+        if n <= len(out):
+            return out.head(n)
+        out = PolyList.alloc(n)
+        s = out.struct()
+        cnt = C.c_int64()
+        check(N.lib().bt_gpu_last_polys(self._h, C.byref(s), C.byref(cnt)))
+        return out.head(cnt.value)
+
     def primary(self, cam: N.Camera, cull: bool = False, tile: int = 16, cap: int = 0) -> PolyList:
         cap = cap or max(1 << 16, 2 * cam.W * cam.H)
-        while True:
-            out = PolyList.alloc(cap)
-            s = out.struct()
-            cnt = C.c_int64()
-            info = N.RunInfo()
-            check(N.lib().bt_gpu_primary(self._h, C.byref(cam), int(cull), int(tile), C.byref(s), C.byref(cnt),
-                                         C.byref(info)))
-            self._record(info)
-            if cnt.value <= cap:
-                return out.head(cnt.value)
-            cap = cnt.value
+        out = PolyList.alloc(cap)
+        s = out.struct()
+        cnt = C.c_int64()
+        info = N.RunInfo()
+        check(N.lib().bt_gpu_primary(self._h, C.byref(cam), int(cull), int(tile), C.byref(s), C.byref(cnt),
+                                     C.byref(info)))
+        self._record(info)
+        return self._fetch_rest(out, cnt.value)
 
     def point_shadows(self, cam: N.Camera, hits: PolyList, light, cap: int = 0) -> PolyList:
         light = np.asarray(light, np.float32)
         cap = cap or max(1 << 16, 4 * len(hits))
         hs = hits.struct()
-        while True:
-            out = PolyList.alloc(cap)
-            s = out.struct()
-            cnt = C.c_int64()
-            info = N.RunInfo()
-            check(N.lib().bt_gpu_point(self._h, C.byref(cam), C.byref(hs), len(hits), ptr(light), C.byref(s),
-                                       C.byref(cnt), C.byref(info)))
-            self._record(info)
-            if cnt.value <= cap:
-                return out.head(cnt.value)
-            cap = cnt.value
+        out = PolyList.alloc(cap)
+        s = out.struct()
+        cnt = C.c_int64()
+        info = N.RunInfo()
+        check(N.lib().bt_gpu_point(self._h, C.byref(cam), C.byref(hs), len(hits), ptr(light), C.byref(s),
+                                   C.byref(cnt), C.byref(info)))
+        self._record(info)
+        return self._fetch_rest(out, cnt.value)
 
     def primary_ids(self, cam: N.Camera, cull: bool = False, tile: int = 16) -> np.ndarray:
         """Per-pixel hit-triangle ids, polygons kept on the GPU (bt_gpu_primary_ids)."""

@@ -90,7 +90,7 @@ class _Scene:
 class Server:
     """Resident scenes on one GPU behind the library's request loop."""
 
-    def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 24,
+    def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 25,
                  cache=None, kd_on_gpu: bool = True, vis_lanes: int = 2, fold_ms: float = 100.0,
                  soft_pixels: int = 8 << 20):
         from .ingest import SceneCache

@@ -243,12 +243,13 @@ void GpuRenderer::primary(const Camera& cam, bool cull, std::vector<OutBeam>& hi
   PolyBuf buf;
   bt_run_info info;
   int64_t count = 0;
-  for (;;) {
-    buf.resize(cap);
-    bt_polys out = buf.view();
-    check(bt_gpu_primary(impl_->ctx, &c, cull ? 1 : 0, tile, &out, &count, &info), "bt_gpu_primary");
-    if (size_t(count) <= cap) break;
-    cap = size_t(count);
+  buf.resize(cap);
+  bt_polys out = buf.view();
+  check(bt_gpu_primary(impl_->ctx, &c, cull ? 1 : 0, tile, &out, &count, &info), "bt_gpu_primary");
+  if (size_t(count) > cap) {  // more than fit: the polygons are still on the device
+    buf.resize(size_t(count));
+    out = buf.view();
+    check(bt_gpu_last_polys(impl_->ctx, &out, &count), "bt_gpu_last_polys");
   }
   hitBeams.clear();
   buf.append(size_t(count), hitBeams);
@@ -284,12 +285,13 @@ void GpuRenderer::pointShadows(const Camera& cam, const std::vector<OutBeam>& pr
   PolyBuf buf;
   bt_run_info info;
   int64_t count = 0;
-  for (;;) {
-    buf.resize(cap);
-    bt_polys out = buf.view();
-    check(bt_gpu_point(impl_->ctx, &c, &hv, int64_t(primaryHits.size()), Lp, &out, &count, &info), "bt_gpu_point");
-    if (size_t(count) <= cap) break;
-    cap = size_t(count);
+  buf.resize(cap);
+  bt_polys out = buf.view();
+  check(bt_gpu_point(impl_->ctx, &c, &hv, int64_t(primaryHits.size()), Lp, &out, &count, &info), "bt_gpu_point");
+  if (size_t(count) > cap) {  // more than fit: the polygons are still on the device
+    buf.resize(size_t(count));
+    out = buf.view();
+    check(bt_gpu_last_polys(impl_->ctx, &out, &count), "bt_gpu_last_polys");
   }
   buf.append(size_t(count), shadowPolys);
   toStats(info, rs.trace);

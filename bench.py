@@ -181,7 +181,9 @@ def accuracy(scene, ps, cam, light, vis, ray_sample: int = 16384):
     the frame's own shading points, every covered pixel (max, mean and a
     histogram of |vis - fp64|); and, beside it, the error of the reference's
     256-ray sampled visibility (--method ray --samples 256) on an even
-    sample of the covered pixels.  The FP64 run is timed on the host cores."""
+    sample of the covered pixels, and the same frame with the opt-in FP64
+    re-decision of band corners (eps_fp64): its error and frame time.  The
+    FP64 run is timed on the host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from ref import RefTracer, ref_available
     if not (ref_available("f") and ref_available("d")):
@@ -203,6 +205,18 @@ def accuracy(scene, ps, cam, light, vis, ray_sample: int = 16384):
                             threads=threads)
     ray_s = time.perf_counter() - t0
     er = np.abs(vr - vd[pick])
+    # the opt-in FP64 re-decision of band corners on the same frame
+    from beamtrace2007_b200.renderer import GpuRenderer
+    with GpuRenderer(ps, eps_fp64=True) as g64:
+        g64.soft_shadows(cam, light, exact=True)
+        r64 = [g64.soft_shadows(cam, light, exact=True) for _ in range(3)]
+    e64 = np.abs(r64[-1].vis[cov].astype(np.float64) - vd[cov])
+    fp64_band = {"max_abs_err_vs_fp64": float(e64.max()), "mean_abs_err_vs_fp64": float(e64.mean()),
+                 "pixels_over_1e-4": int((e64 > 1e-4).sum()),
+                 "ms_per_frame": float(np.median([r.info["ms_total"] for r in r64])),
+                 "band_corners": int(r64[-1].info["eps_band_corners"]),
+                 "re_decided": int(r64[-1].info["eps_fp64_flips"]),
+                 "pixels_changed": int((r64[-1].vis != vis).sum())}
     return {"pixels": int(len(cov)), "max_abs_err_vs_fp64": float(err.max()), "mean_abs_err_vs_fp64": float(err.mean()),
             "pixels_over_1e-4": int((err > 1e-4).sum()),
             "histogram": {"edges": ["0", "1e-7", "1e-6", "1e-5", "1e-4", "1e-3", "inf"],
@@ -211,6 +225,7 @@ def accuracy(scene, ps, cam, light, vis, ray_sample: int = 16384):
                        "mean_abs_err_vs_fp64": float(er.mean()), "seconds": ray_s, "cores": threads},
             "fp64_oracle": {"seconds": fp64_s, "px_per_s": len(cov) / fp64_s, "cores": threads,
                             "what": "reference double build, exact, the frame's shading points"},
+            "eps_fp64_mode": fp64_band,
             "oracle": "oracle/_ref (the reference compiled from its sources)"}
 
 

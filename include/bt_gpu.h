@@ -368,6 +368,14 @@ BT_API int bt_gpu_primary(bt_gpu_ctx* ctx, const bt_camera* cam, int32_t cull, i
 BT_API int bt_gpu_point(bt_gpu_ctx* ctx, const bt_camera* cam, const bt_polys* hits, int64_t num_hits,
                         const float* light, bt_polys* out, int64_t* count, bt_run_info* info);
 
+/* The polygons of the last bt_gpu_primary / bt_gpu_point call on ctx
+ * again, into a (larger) buffer: when a call reports more polygons than
+ * out->cap held, fetch them with this instead of repeating the call.  They
+ * stay on the device until the context's next engine call (BT_ERR_INVALID
+ * after it).  Serves the retry loops of GpuRenderer::primary / pointShadows
+ * (cuda/gpu_render.h:41-46), which the reference sizes on the host. */
+BT_API int bt_gpu_last_polys(bt_gpu_ctx* ctx, bt_polys* out, int64_t* count);
+
 /* Primary visibility to per-pixel hit-triangle ids (-1 background) with the
  * polygons kept in device memory: the engine's tile roots, then the pixel-
  * centre raster of the final polygons on the GPU (rasterize,

@@ -290,3 +290,32 @@ def test_fused_primary_rays_same_as_separate(name, kw, budget, gpu):
         assert np.array_equal(x, getattr(sep[0], f)), f
     if budget < 16:
         assert fus[0].info["retried_roots"] > 0
+
+
+def test_last_polys_instead_of_a_second_run(gpu):
+    """A polygon buffer too small for bt_gpu_primary / bt_gpu_point: the
+    polygons are fetched from the device afterwards (bt_gpu_last_polys),
+    bitwise the same as with a buffer large enough, without running the
+    engine again; any other engine call drops them (BT_ERR_INVALID)."""
+    import ctypes as C
+    from beamtrace2007_b200 import _native as N
+    from beamtrace2007_b200.renderer import GpuRenderer, PolyList, make_camera
+    from conftest import piece_keys
+    s, ps = scene("plant")
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 96, 72)
+    light = np.array(s.point_light, np.float32)
+    with GpuRenderer(ps) as g:
+        big = g.primary(cam, tile=16, cap=1 << 20)
+        small = g.primary(cam, tile=16, cap=16)
+        launches = g.last_info["launches"]
+        assert len(big) > 16 and np.array_equal(piece_keys(small, True), piece_keys(big, True))
+        sh_big = g.point_shadows(cam, big, light, cap=1 << 20)
+        sh_small = g.point_shadows(cam, big, light, cap=4)
+        assert len(sh_big) > 4 and np.array_equal(piece_keys(sh_small), piece_keys(sh_big))
+        g.soft_shadows(cam, s.light_array(), exact=False)
+        out = PolyList.alloc(8)
+        st = out.struct()
+        cnt = C.c_int64()
+        assert N.lib().bt_gpu_last_polys(g._h, C.byref(st), C.byref(cnt)) == -1
+    assert launches > 0
