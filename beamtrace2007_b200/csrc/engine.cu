@@ -70,6 +70,11 @@ constexpr double kFixG = 1152921504606846976.0;     // 2^60: Lambert integral, f
 // making progress, far above what long batches need (a 64-job batch of
 // 100-200K-triangle scenes with large lights takes thousands of rounds).
 constexpr int kMaxLaunches = 1000000;
+// Queue slots a root reserves when it is admitted (its budget if smaller);
+// it takes more from the pool as it grows.  Roots admitted at once are
+// bounded by capacity / this: 128 admits a whole 512^2 soft frame into
+// 2^25-record queues, and primary tiles (budget 4096) as many.
+constexpr int kInitialReserve = 128;
 
 enum App { kAppSoft = 0, kAppPrimary = 1, kAppPoint = 2 };
 enum RootState { kRootNone = 0, kRootTraced = 1, kRootKilled = 2 };
@@ -163,14 +168,17 @@ struct RoundParams {
   SubBeam* cq;     // clip queue of the round
   int cur;
   int capacity;
-  int budget;
-  int reserve;  // queue slots reserved per root: max(budget, 32) (a root's pre-split pieces always fit)
+  int budget;   // live sub-beams a root may hold before it is abandoned (and retried with 16x)
+  int reserve;  // queue slots a root reserves when admitted: min(budget, kInitialReserve), at least 32 (its
+                // pre-split pieces always fit); it grows from the pool, up to the budget, as the root needs
+
   int numRoots;
   int rootCap;  // size of the per-root arrays
   int yieldAt;  // exited trace warps at which the rest hand their records on (INT_MAX: never)
   const int32_t* rootList;
   RootRec* roots;  // per-root query records
   int32_t* live;
+  int32_t* resv;  // per root: queue slots it holds reserved
   int32_t* state;
   int32_t* attempt;
   Counters* ctr;
@@ -218,13 +226,32 @@ __device__ __forceinline__ void loadRoot(const RootRec* R, Query& q, float& ligh
   querySetup(q, a.w);
 }
 
-__device__ __forceinline__ void rootDone(const RoundParams& p) {
-  atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)p.reserve));
+// A root is finished: its reservation goes back to the pool.
+__device__ __forceinline__ void rootDone(const RoundParams& p, int root) {
+  atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)__ldcg(&p.resv[root])));
   atomicSub(&p.ctr->inflight, 1);
 }
 
 __device__ __forceinline__ void liveSub(const RoundParams& p, int root, int n) {
-  if (n > 0 && atomicSub(&p.live[root], n) == n) rootDone(p);
+  if (n > 0 && atomicSub(&p.live[root], n) == n) rootDone(p, root);
+}
+
+// A root now holds `need` live sub-beams: its reservation covers them, or
+// grows from the pool (at least doubling, never past the budget) while the
+// queues' capacity allows.  False: the pool cannot cover it (the caller
+// abandons the root).  Lanes that grow one root at once may both add;
+// rootDone gives back whatever the root holds.
+__device__ __forceinline__ bool coverLive(const RoundParams& p, int root, int need) {
+  const int have = __ldcg(&p.resv[root]);
+  if (need <= have) return true;
+  const int grow = min(max(need - have, have), p.budget - have);  // need <= budget: at least need - have
+  const unsigned long long old = atomicAdd(&p.ctr->reserved, (unsigned long long)grow);
+  if (old + (unsigned long long)grow > (unsigned long long)p.capacity) {
+    atomicAdd(&p.ctr->reserved, (unsigned long long)(-(long long)grow));
+    return false;
+  }
+  atomicAdd(&p.resv[root], grow);
+  return true;
 }
 
 __device__ __forceinline__ void killRoot(const RoundParams& p, int root) {
@@ -540,6 +567,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   float& lightArea = out->lightArea;
   Stats& st = out->st;
   p.live[k] = 0;
+  p.resv[k] = p.reserve;  // what the admission claimed for it
   p.state[k] = kRootNone;
   const int att = p.attempt[k] + 1;
   p.attempt[k] = att;
@@ -570,7 +598,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
     const AppParams& a = *ap;
     int pix;
     if (!softPixel(a, kl, pix)) {
-      rootDone(p);
+      rootDone(p, k);
       return false;
     }
     int T;
@@ -591,7 +619,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
       if (a.vis) a.vis[pix] = -1;
       if (a.E) a.E[pix] = 0;
       if (a.Eu) a.Eu[pix] = 0;
-      rootDone(p);
+      rootDone(p, k);
       return false;
     }
     if (!a.fusedPrimary) {
@@ -603,7 +631,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
     if (!lightBeamSetup(a.Lc, a.LU, a.LV, x, ns, T, a.offset, q, poly, lightArea)) {
       if (a.vis) a.vis[pix] = 0;
       if (a.E) a.E[pix] = 0;
-      rootDone(p);
+      rootDone(p, k);
       return false;
     }
     p.app.shade[2 * k] = make_float4(x.x, x.y, x.z, 0.f);
@@ -634,7 +662,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
       py[i] = p.app.hy[4 * k + i];
     }
     if (T < 0) {
-      rootDone(p);
+      rootDone(p, k);
       return false;
     }
     V3 nT, v0;
@@ -643,7 +671,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
                           poly)) {
       appendPoly(p, k, px, py, n, T, 0.f);  // receiver faces away from the light: all in shadow
       p.state[k] = kRootTraced;
-      rootDone(p);
+      rootDone(p, k);
       return false;
     }
   }
@@ -654,7 +682,7 @@ __device__ __noinline__ bool admit(const RoundParams& p, int k, AdmitOut* out) {
   const bool ok = admitRoot(sj, q, poly, k, env, st);
   p.live[k] = env.queued;  // the pieces are traced by a later kernel
   if (!ok || env.queued > p.budget) killRoot(p, k);
-  if (env.queued == 0) rootDone(p);
+  if (env.queued == 0) rootDone(p, k);
   return env.queued > 0;
 }
 
@@ -737,12 +765,12 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
     return true;
   }
   const int old = atomicAdd(&p.live[root], slots - 1);
-  if (old + slots - 1 > p.budget) {
+  if (old + slots - 1 > p.budget || !coverLive(p, root, old + slots - 1)) {
     killRoot(p, root);
     liveSub(p, root, slots);
     return false;
   }
-  if (old + slots - 1 == 0) rootDone(p);  // every piece occluded: the root is finished
+  if (old + slots - 1 == 0) rootDone(p, root);  // every piece occluded: the root is finished
   SplitEnv<App> env;
   env.p = &p;
   env.q = &q;
@@ -1253,6 +1281,7 @@ struct bt_gpu_ctx {
   size_t rootCap = 0;
   RootRec* dRoots = nullptr;
   int32_t *dLive = nullptr, *dState = nullptr, *dAttempt = nullptr, *dList[2] = {nullptr, nullptr};
+  int32_t* dResv = nullptr;  // queue slots each root holds reserved
   unsigned long long *dMiss = nullptr, *dG = nullptr;
   float4* dShade = nullptr;
   int* dKillCount = nullptr;
@@ -1303,7 +1332,7 @@ const char* bt_gpu_last_error(void) { return g_err; }
 
 void bt_gpu_config_default(bt_gpu_config* c) {
   c->device = 0;
-  c->budget = 128;
+  c->budget = 2048;
   c->primary_budget = 4096;
   c->capacity = 0;
   c->blocks_per_sm = 0;
@@ -1343,6 +1372,7 @@ int ensureRoots(bt_gpu_ctx* c, size_t R) {
   if (c->rootCap >= R) return BT_OK;
   cudaFree(c->dRoots);
   cudaFree(c->dLive);
+  cudaFree(c->dResv);
   cudaFree(c->dState);
   cudaFree(c->dAttempt);
   cudaFree(c->dList[0]);
@@ -1352,7 +1382,8 @@ int ensureRoots(bt_gpu_ctx* c, size_t R) {
   cudaFree(c->dShade);
   c->rootCap = 0;
   int e;
-  if ((e = devAlloc(&c->dRoots, R)) || (e = devAlloc(&c->dLive, R)) || (e = devAlloc(&c->dState, R)) ||
+  if ((e = devAlloc(&c->dRoots, R)) || (e = devAlloc(&c->dLive, R)) || (e = devAlloc(&c->dResv, R)) ||
+      (e = devAlloc(&c->dState, R)) ||
       (e = devAlloc(&c->dAttempt, R)) || (e = devAlloc(&c->dList[0], R)) || (e = devAlloc(&c->dList[1], R)) ||
       (e = devAlloc(&c->dMiss, R)) || (e = devAlloc(&c->dG, R)) || (e = devAlloc(&c->dShade, 2 * R)))
     return e;
@@ -1478,6 +1509,7 @@ struct RoundRunner {
     p.roots = c->dRoots;
     p.rootCap = R;
     p.live = c->dLive;
+    p.resv = c->dResv;
     p.state = c->dState;
     p.attempt = c->dAttempt;
     p.ctr = c->dCtr;
@@ -1511,7 +1543,14 @@ struct RoundRunner {
   int startPass(int n, const int32_t* list, int budget) {
     ++pass;
     p.budget = budget;
-    p.reserve = std::max(budget, 32);
+    // Roots reserve little when admitted and grow (a root over its budget,
+    // or one the free capacity cannot cover, is retried in the next pass
+    // with 16x the budget); the last retry pass admits roots holding their
+    // whole budget, or the whole queue, so that no root is squeezed there:
+    // every root that fits a queue finishes.
+    const bool strict = pass >= c->cfg.max_retries;
+    p.reserve = strict ? int(std::max<int64_t>(std::min<int64_t>(budget, c->capacity), 32))
+                       : std::max(std::min(budget, kInitialReserve), 32);
     if (int64_t(p.reserve) > c->capacity) {
       setErr("a root needs more than %d live sub-beams (queue capacity %d)", budget / 16, c->capacity);
       return BT_ERR_CAPACITY;
@@ -1948,7 +1987,8 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
     c->dTriNV = nullptr;
   }
   void* ptrs[] = {c->dNode, c->dBox, c->dParent, c->dRef, c->dTriNV, c->dQ[0], c->dQ[1], c->dQ[2], c->dCtr, c->dStats,
-                  c->dRoots, c->dLive, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG, c->dShade,
+                  c->dRoots, c->dLive, c->dResv, c->dState, c->dAttempt, c->dList[0], c->dList[1], c->dMiss, c->dG,
+                  c->dShade,
                   c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart, c->dHx, c->dHy, c->dHn,
                   c->dHt, c->dHitCount, c->dFlag, c->dRanges, c->dJobCounts};
@@ -3054,7 +3094,7 @@ std::mutex g_noallocSetup;
 struct NoAllocLayout {
   size_t err, ctr, stats, kill;
   size_t node, box, parent, ref, triNV;
-  size_t roots, live, state, attempt, list0, list1, miss, g, shade;
+  size_t roots, live, resv, state, attempt, list0, list1, miss, g, shade;
   size_t queues;
   int64_t cap;  // records per queue
 };
@@ -3081,6 +3121,7 @@ bool noallocLayout(int64_t nn, int64_t nr, int64_t nt, int64_t n, NoAllocLayout*
   L->triNV = take(size_t(2 * nt) * sizeof(float4));
   L->roots = take(R * sizeof(RootRec));
   L->live = take(R * sizeof(int32_t));
+  L->resv = take(R * sizeof(int32_t));
   L->state = take(R * sizeof(int32_t));
   L->attempt = take(R * sizeof(int32_t));
   L->list0 = take(R * sizeof(int32_t));
@@ -3339,6 +3380,7 @@ int bt_gpu_soft_points_noalloc(const bt_scene_desc* sc, const bt_kd_desc* kd, co
   c.rootCap = size_t(std::max<int64_t>(n, 1));
   c.dRoots = static_cast<RootRec*>(at(lay.roots));
   c.dLive = static_cast<int32_t*>(at(lay.live));
+  c.dResv = static_cast<int32_t*>(at(lay.resv));
   c.dState = static_cast<int32_t*>(at(lay.state));
   c.dAttempt = static_cast<int32_t*>(at(lay.attempt));
   c.dList[0] = static_cast<int32_t*>(at(lay.list0));

@@ -210,7 +210,7 @@ class GpuRenderer:
     """bt::GpuRenderer over the C-ABI: the scene and its kd-tree are resident
     on one GPU for the renderer's lifetime."""
 
-    def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 128, primary_budget: int = 4096,
+    def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 2048, primary_budget: int = 4096,
                  capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
                  tail_records: int = 0, eps_stats: bool = False, yield_pct: int = 0, fuse_primary: bool = False,
                  eps_fp64: bool = False):

@@ -109,8 +109,13 @@ typedef struct {
 /* Engine tunables (GpuRenderer public fields, gpu_render.h:50-58). */
 typedef struct {
   int32_t device;           /* CUDA device ordinal */
-  int32_t budget;           /* live sub-beams per soft/point root before a retry (wfBudget) */
-  int32_t primary_budget;   /* live sub-beams per primary tile (wfPrimaryBudget) */
+  int32_t budget;           /* live sub-beams per soft/point root before it is abandoned and retried with 16x
+                               (wfBudget; default 2048, the reference's 128 x 16) */
+  int32_t primary_budget;   /* live sub-beams per primary tile (wfPrimaryBudget; default 4096).  A root
+                               reserves min(budget, 128) queue slots when admitted and takes more from the
+                               queues' free capacity as it grows; past its budget, or when the queues
+                               cannot cover it, it is abandoned and retried with 16x the budget; the last
+                               retry pass (max_retries) reserves each root's whole budget, at most a queue */
   int64_t capacity;         /* sub-beam records per spill queue (wfCapacity); 0 = 2^25, at most a tenth of
                                the free device memory over the three queues */
   int32_t blocks_per_sm;    /* persistent CTAs per SM; 0 = occupancy */
@@ -288,7 +293,7 @@ BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light
  * the same inputs.
  *
  * Limit: the scene in the engine's layout (44 bytes per kd node, 64 per
- * reference, 32 per triangle), 164 bytes per point and three sub-beam queues
+ * reference, 32 per triangle), 168 bytes per point and three sub-beam queues
  * of at least 8192 64-byte records must fit in BT_NOALLOC_SCRATCH_BYTES
  * (each section rounded up to 256 bytes); larger calls return
  * BT_ERR_TOO_LARGE before any GPU work.  A kd-tree whose indices are out of
@@ -297,11 +302,13 @@ BT_API int bt_gpu_soft_points_device(bt_gpu_ctx* ctx, const bt_area_light* light
  *
  * BT_ERR_CAPACITY can come back here where bt_gpu_soft_points_device
  * succeeds: the queues get what the fixed array leaves over (at most about
- * 349,000 records each, against 2^23 on a context), and a root
- * that outgrows its live sub-beam budget is retried with 16 times the
- * budget only while that budget (128, 2048, 32768, ...) fits one queue --
- * two retries here, four on a context.  The message then names the queue
- * size.
+ * 349,000 records each, against 2^25 on a context).  Roots take queue slots
+ * from that pool as they grow; a root over its budget (2048 live
+ * sub-beams) or one the pool cannot cover is abandoned and retried with
+ * 16 times the budget, and the last of four retries admits roots one queue
+ * at a time: the call fails, with a message that names the queue size,
+ * only for a root that needs more live sub-beams than one queue of the
+ * pool holds, and takes longer the more roots the small pool squeezes.
  *
  * Runs on the current device's legacy default stream and returns when the
  * results are complete.  That stream waits for all work already queued on

@@ -48,7 +48,7 @@ def test_sizes_over_the_limit_are_rejected(native_lib):
     sd, kd = _descs(p, p, p, b, p, p, p, p, p, p, b, 3, 1, 1 << 21, 1)
     assert _call(sd, kd, light, opts, 0, None, None, None, None, None, None) == -8
     assert b"BT_NOALLOC_SCRATCH_BYTES" in N.lib().bt_gpu_last_error()
-    # a small scene with a million points: 164 MB of root records
+    # a small scene with a million points: 168 MB of root records
     sd, kd = _descs(p, p, p, b, p, p, p, p, p, p, b, 3, 1, 1, 1)
     assert _call(sd, kd, light, opts, 1 << 20, p, p, p, p, p, p) == -8
     # bad arguments stay BT_ERR_INVALID
@@ -206,31 +206,24 @@ def test_noalloc_rejects_malformed_inputs(gpu):
     assert np.abs(E - rE).max() <= E_REL * np.abs(rE).max()
 
 
-def test_retry_reserve_of_the_fixed_queues(native_lib):
+def test_fixed_queue_pool(native_lib):
     """The queues of the allocation-free call get what the scratch array
     leaves after the scene and the points (the layout of the header's limit:
-    44 B per kd node, 64 per reference, 32 per triangle, 164 per point, each
-    section rounded up to 256 B, plus a few small sections of counters); a
-    root over its live sub-beam budget is retried with 16 times the budget
-    only while that reserve fits one queue.  For the room scene at 128 x 96
-    points that is two retries (budget 128 -> 2048 -> 32768; 524288 does not
-    fit), against four on a context's 2^23-record queues, as the header
-    states."""
-    from beamtrace2007_b200 import _native as N
+    44 B per kd node, 64 per reference, 32 per triangle, 168 per point, each
+    section rounded up to 256 B, plus a few small sections of counters):
+    for the room scene at 128 x 96 points, 300,000 to 349,525 records per
+    queue, as the header states -- about a hundredth of a context's 2^25 --
+    and room for the admission of a warp's 32 roots at their initial
+    reservation of 128 slots each, many times over."""
     _, ps = scene("room")
-    cfg = N.GpuConfig()
-    N.lib().bt_gpu_config_default(C.byref(cfg))
 
     def r256(b):
         return (b + 255) // 256 * 256
     nn, nr, nt, n = len(ps.kd_split), len(ps.kd_tri_indices), len(ps.tris), 128 * 96
     scene_and_points = (r256(8 * nn) + r256(32 * nn) + r256(4 * nn) + r256(64 * nr) + r256(32 * nt) + r256(96 * n)
-                        + 5 * r256(4 * n) + 2 * r256(8 * n) + r256(32 * n))
+                        + 6 * r256(4 * n) + 2 * r256(8 * n) + r256(32 * n))
     limit = 64 << 20
     caps = [(limit - scene_and_points - small) // (3 * 64) for small in (0, 16 << 10)]
-
-    def retries(cap):
-        return max(p for p in range(8) if max(cfg.budget, 32) * 16 ** p <= cap)
-    assert [retries(c) for c in caps] == [2, 2]
-    assert retries(1 << 23) == cfg.max_retries == 4
     assert all(300_000 < c < 349_526 for c in caps)
+    assert all(c >= 64 * 32 * 128 for c in caps)
+    assert (1 << 25) // caps[0] >= 90
