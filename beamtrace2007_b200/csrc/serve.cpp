@@ -68,11 +68,11 @@ int64_t softRootsOf(const bt_camera& cam) { return int64_t((cam.W + 7) / 8) * ((
 
 // Device bytes a request's pixels need, as admission charges them: soft
 // 40 B/px of arena (ids, shading point and normal in; vis, E, Eu out) and
-// 68 B per root; primary ids and point masks 9 B/px (ids, mask, ids for the
+// 72 B per root; primary ids and point masks 9 B/px (ids, mask, ids for the
 // raster) and about two output polygons of 52 B per pixel.
 int64_t chargeOf(const bt_request& r) {
   const int64_t px = int64_t(r.cam.W) * r.cam.H;
-  if (r.kind == BT_REQ_SOFT) return px * 40 + softRootsOf(r.cam) * 68;
+  if (r.kind == BT_REQ_SOFT) return px * 40 + softRootsOf(r.cam) * 72;
   return px * (9 + 2 * 52);
 }
 

@@ -113,7 +113,7 @@ def test_admission_by_memory_budget(gpu):
     s, ps = scene("room")
     with Server({"room": s}, memory_budget_gb=8.0, queue_records=1 << 16) as srv:
         scene_bytes = srv.stats()["scene_bytes"]
-    one = 128 * 128 * 40 + 128 * 128 * 68   # what admission charges a 128^2 soft request
+    one = 128 * 128 * 40 + 128 * 128 * 72   # what admission charges a 128^2 soft request
     budget = scene_bytes + 3 * one + one // 2
     with Server({"room": s}, memory_budget_gb=budget / (1 << 30), queue_records=1 << 16) as srv:
         reqs = [srv.submit(Request("soft" if i % 3 else "primary", "room", 128, 128, light_scale=0.5 + 0.1 * i))
