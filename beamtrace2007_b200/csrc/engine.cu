@@ -1103,6 +1103,107 @@ __global__ void compactHitsKernel(const float* ox, const float* oy, const int32_
   htri[k] = otri[i];
 }
 
+// Polygons of the roots' final attempts, compacted on the device in output
+// order for the host-polygon calls: the number each block of kKeepBlock
+// records keeps, an exclusive scan of those counts (the total after them),
+// then every kept polygon written at its rank.
+constexpr int kKeepBlock = 1024;
+
+__device__ __forceinline__ bool finalPoly(const int32_t* oroot, const int32_t* oatt, const int32_t* state,
+                                          const int32_t* attempt, int64_t i) {
+  const int r = oroot[i];
+  return state[r] == kRootTraced && oatt[i] == attempt[r];
+}
+
+__global__ void __launch_bounds__(kKeepBlock) keepCountKernel(const int32_t* oroot, const int32_t* oatt, int64_t n,
+                                                              const int32_t* state, const int32_t* attempt,
+                                                              int* blockCount) {
+  __shared__ int warpCount[kKeepBlock / 32];
+  const int64_t i = int64_t(blockIdx.x) * kKeepBlock + threadIdx.x;
+  const unsigned m = __ballot_sync(kFull, i < n && finalPoly(oroot, oatt, state, attempt, i));
+  if ((threadIdx.x & 31) == 0) warpCount[threadIdx.x >> 5] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = warpCount[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    if (threadIdx.x == 0) blockCount[blockIdx.x] = v;
+  }
+}
+
+// One block: blockCount[0..nb) becomes its exclusive prefix sums and
+// blockCount[nb] the total.
+__global__ void __launch_bounds__(kKeepBlock) keepScanKernel(int* blockCount, int nb) {
+  __shared__ int warpSum[kKeepBlock / 32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += kKeepBlock) {
+    const int j = base + threadIdx.x;
+    const int v = j < nb ? blockCount[j] : 0;
+    int x = v;  // inclusive scan within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = warpSum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, w, o);
+        if (lane >= o) w += y;
+      }
+      warpSum[lane] = w;
+    }
+    __syncthreads();
+    const int before = carry + (warp ? warpSum[warp - 1] : 0) + x - v;
+    if (j < nb) blockCount[j] = before;
+    __syncthreads();
+    if (threadIdx.x == kKeepBlock - 1) carry = before + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) blockCount[nb] = carry;
+}
+
+struct KeepOut {
+  float4 *x, *y;
+  float* area;
+  int32_t *n, *tri, *root;
+};
+
+__global__ void __launch_bounds__(kKeepBlock) keepWriteKernel(const float4* ox, const float4* oy, const float* oarea,
+                                                              const int32_t* on, const int32_t* otri,
+                                                              const int32_t* oroot, const int32_t* oatt, int64_t n,
+                                                              const int32_t* state, const int32_t* attempt,
+                                                              const int* blockOff, KeepOut k) {
+  __shared__ int warpOff[kKeepBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i = int64_t(blockIdx.x) * kKeepBlock + threadIdx.x;
+  const bool keep = i < n && finalPoly(oroot, oatt, state, attempt, i);
+  const unsigned m = __ballot_sync(kFull, keep);
+  if (lane == 0) warpOff[warp] = __popc(m);
+  __syncthreads();
+  if (warp == 0) {
+    const int v = warpOff[lane];
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    warpOff[lane] = x - v;
+  }
+  __syncthreads();
+  if (!keep) return;
+  const int at = blockOff[blockIdx.x] + warpOff[warp] + __popc(m & ((1u << lane) - 1u));
+  k.x[at] = ox[i];
+  k.y[at] = oy[i];
+  k.area[at] = oarea[i];
+  k.n[at] = on[i];
+  k.tri[at] = otri[i];
+  k.root[at] = oroot[i];
+}
+
 // Roots abandoned in a pass, compacted for the retry pass.
 __global__ void collectKilledKernel(const int32_t* state, const int32_t* list, int n, int32_t* out, int* count) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1288,7 +1389,6 @@ struct bt_gpu_ctx {
   // outputs
   int64_t outCap = 0;
   int64_t lastProduced = -1;  // polygons of the last bt_gpu_primary / bt_gpu_point (bt_gpu_last_polys)
-  int lastRoots = 0;
   float *dOx = nullptr, *dOy = nullptr, *dOarea = nullptr;
   int32_t *dOn = nullptr, *dOtri = nullptr, *dOroot = nullptr, *dOatt = nullptr;
   // per-image scratch
@@ -1301,6 +1401,12 @@ struct bt_gpu_ctx {
   float *dHx = nullptr, *dHy = nullptr;
   int32_t *dHn = nullptr, *dHt = nullptr;
   int* dHitCount = nullptr;
+  // host-polygon calls: the final attempts' polygons compacted on the device
+  int64_t keepCap = 0;
+  int keepBlocksCap = 0;
+  float *dKx = nullptr, *dKy = nullptr, *dKarea = nullptr;
+  int32_t *dKn = nullptr, *dKtri = nullptr, *dKroot = nullptr;
+  int* dKeepBlocks = nullptr;
   uint8_t* dFlag = nullptr;  // host-output variants: the mask in device memory
   int64_t flagCap = 0;
   // batched soft shadows: per-job parameter table and root offsets
@@ -1991,7 +2097,8 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
                   c->dShade,
                   c->dKillCount, c->dOx, c->dOy, c->dOarea, c->dOn, c->dOtri, c->dOroot, c->dOatt, c->dPixTri,
                   c->dPixX, c->dPixN, c->dVis, c->dE, c->dEu, c->dJobs, c->dJobStart, c->dHx, c->dHy, c->dHn,
-                  c->dHt, c->dHitCount, c->dFlag, c->dRanges, c->dJobCounts};
+                  c->dHt, c->dHitCount, c->dFlag, c->dRanges, c->dJobCounts, c->dKx, c->dKy, c->dKarea,
+                  c->dKn, c->dKtri, c->dKroot, c->dKeepBlocks};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& ev : c->ev)
@@ -2298,39 +2405,71 @@ namespace {
 
 // Copies the polygons of roots that finished in their last attempt to the
 // host (downloadPolys, cuda/wavefront.cu:766-783).
-int downloadPolys(bt_gpu_ctx* c, int64_t produced, int R, bt_polys* out, int64_t* count) {
+int ensureKeep(bt_gpu_ctx* c, int64_t n, int blocks) {
+  if (c->keepBlocksCap < blocks + 1) {
+    cudaFree(c->dKeepBlocks);
+    c->keepBlocksCap = 0;
+    int e = devAlloc(&c->dKeepBlocks, size_t(blocks + 1));
+    if (e) return e;
+    c->keepBlocksCap = blocks + 1;
+  }
+  if (c->keepCap >= n) return BT_OK;
+  cudaFree(c->dKx);
+  cudaFree(c->dKy);
+  cudaFree(c->dKarea);
+  cudaFree(c->dKn);
+  cudaFree(c->dKtri);
+  cudaFree(c->dKroot);
+  c->keepCap = 0;
+  int e;
+  if ((e = devAlloc(&c->dKx, size_t(4 * n))) || (e = devAlloc(&c->dKy, size_t(4 * n))) ||
+      (e = devAlloc(&c->dKarea, size_t(n))) || (e = devAlloc(&c->dKn, size_t(n))) ||
+      (e = devAlloc(&c->dKtri, size_t(n))) || (e = devAlloc(&c->dKroot, size_t(n))))
+    return e;
+  c->keepCap = n;
+  return BT_OK;
+}
+
+// The polygons of the roots' final attempts (of the first `produced` output
+// records) into the caller's host buffers, in output order: compacted on
+// the device, then copied straight into out (its first out->cap entries);
+// *count = all kept polygons.
+int downloadPolys(bt_gpu_ctx* c, int64_t produced, bt_polys* out, int64_t* count) {
   const int64_t n = std::min<int64_t>(produced, c->outCap);
-  std::vector<float> x(static_cast<size_t>(4 * n)), y(static_cast<size_t>(4 * n)), area(static_cast<size_t>(n));
-  std::vector<int32_t> nn(static_cast<size_t>(n)), tri(static_cast<size_t>(n)), root(static_cast<size_t>(n)), att(static_cast<size_t>(n)), state(static_cast<size_t>(R)),
-      attempt(static_cast<size_t>(R));
-  if (n > 0) {
-    CK(cudaMemcpy(x.data(), c->dOx, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(y.data(), c->dOy, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(area.data(), c->dOarea, sizeof(float) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(nn.data(), c->dOn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(tri.data(), c->dOtri, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(root.data(), c->dOroot, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(att.data(), c->dOatt, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+  *count = 0;
+  if (n <= 0) return BT_OK;
+  const int64_t nb64 = (n + kKeepBlock - 1) / kKeepBlock;
+  if (nb64 > INT_MAX - 1) {
+    setErr("too many output polygons (%lld)", (long long)n);
+    return BT_ERR_TOO_LARGE;
   }
-  CK(cudaMemcpy(state.data(), c->dState, sizeof(int32_t) * R, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(attempt.data(), c->dAttempt, sizeof(int32_t) * R, cudaMemcpyDeviceToHost));
-  int64_t k = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    const int r = root[size_t(i)];
-    if (state[size_t(r)] != kRootTraced || att[size_t(i)] != attempt[size_t(r)]) continue;
-    if (k < out->cap) {
-      for (int j = 0; j < 4; ++j) {
-        out->x[4 * k + j] = x[size_t(4 * i + j)];
-        out->y[4 * k + j] = y[size_t(4 * i + j)];
-      }
-      out->n[k] = nn[size_t(i)];
-      out->tri[k] = tri[size_t(i)];
-      out->area[k] = area[size_t(i)];
-      if (out->root) out->root[k] = r;
-    }
-    ++k;
+  const int nb = int(nb64);
+  int e = ensureKeep(c, n, nb);
+  if (e) return e;
+  keepCountKernel<<<nb, kKeepBlock, 0, c->stream>>>(c->dOroot, c->dOatt, n, c->dState, c->dAttempt,
+                                                    c->dKeepBlocks);
+  keepScanKernel<<<1, kKeepBlock, 0, c->stream>>>(c->dKeepBlocks, nb);
+  KeepOut k{reinterpret_cast<float4*>(c->dKx), reinterpret_cast<float4*>(c->dKy), c->dKarea, c->dKn, c->dKtri,
+            c->dKroot};
+  keepWriteKernel<<<nb, kKeepBlock, 0, c->stream>>>(reinterpret_cast<const float4*>(c->dOx),
+                                                    reinterpret_cast<const float4*>(c->dOy), c->dOarea, c->dOn,
+                                                    c->dOtri, c->dOroot, c->dOatt, n, c->dState, c->dAttempt,
+                                                    c->dKeepBlocks, k);
+  CK(cudaGetLastError());
+  int total = 0;
+  CK(cudaMemcpyAsync(&total, c->dKeepBlocks + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int64_t m = std::min<int64_t>(total, std::max<int64_t>(out->cap, 0));
+  if (m > 0) {
+    CK(cudaMemcpyAsync(out->x, c->dKx, sizeof(float) * 4 * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->y, c->dKy, sizeof(float) * 4 * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->n, c->dKn, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->tri, c->dKtri, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->area, c->dKarea, sizeof(float) * m, cudaMemcpyDeviceToHost, c->stream));
+    if (out->root) CK(cudaMemcpyAsync(out->root, c->dKroot, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   }
-  *count = k;
+  *count = total;
   return BT_OK;
 }
 
@@ -2462,8 +2601,7 @@ int bt_gpu_primary(bt_gpu_ctx* c, const bt_camera* cam, int32_t cull, int32_t ti
       info->ms_total = b;
     }
     c->lastProduced = hc.outCount;
-    c->lastRoots = R;
-    return downloadPolys(c, hc.outCount, R, out, count);
+    return downloadPolys(c, hc.outCount, out, count);
   }
 }
 
@@ -2517,8 +2655,7 @@ int bt_gpu_point(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* hits, int6
       info->ms_total = b;
     }
     c->lastProduced = hc.outCount;
-    c->lastRoots = int(nh);
-    return downloadPolys(c, hc.outCount, int(nh), out, count);
+    return downloadPolys(c, hc.outCount, out, count);
   }
 }
 
@@ -2532,7 +2669,7 @@ int bt_gpu_last_polys(bt_gpu_ctx* c, bt_polys* out, int64_t* count) {
     return BT_ERR_INVALID;
   }
   CK(cudaSetDevice(c->device));
-  return downloadPolys(c, c->lastProduced, c->lastRoots, out, count);
+  return downloadPolys(c, c->lastProduced, out, count);
 }
 
 int bt_gpu_raster(bt_gpu_ctx* c, const bt_camera* cam, const bt_polys* prim, int64_t np, const bt_polys* shadow,

@@ -41,9 +41,12 @@ class PolyList:
 
     @staticmethod
     def alloc(cap: int) -> "PolyList":
+        # uninitialised: the library fills the first `count` entries and
+        # head() keeps only those (zeroing a frame-sized buffer costs more
+        # than a small frame's whole engine run)
         cap = max(int(cap), 1)
-        return PolyList(np.zeros((cap, 4), np.float32), np.zeros((cap, 4), np.float32), np.zeros(cap, np.int32),
-                        np.zeros(cap, np.int32), np.zeros(cap, np.float32), np.zeros(cap, np.int32))
+        return PolyList(np.empty((cap, 4), np.float32), np.empty((cap, 4), np.float32), np.empty(cap, np.int32),
+                        np.empty(cap, np.int32), np.empty(cap, np.float32), np.empty(cap, np.int32))
 
     def struct(self) -> N.Polys:
         for a in (self.x, self.y, self.n, self.tri, self.area, self.root):
