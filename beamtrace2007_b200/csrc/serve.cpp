@@ -231,7 +231,7 @@ int bt_gpu_serve_start(bt_gpu_ctx* c, const bt_serve_config* cfg) {
   if (cfg) S->cfg = *cfg;
   else memset(&S->cfg, 0, sizeof S->cfg);
   bt_serve_config& k = S->cfg;
-  if (k.vis_lanes <= 0) k.vis_lanes = 2;
+  if (k.vis_lanes <= 0) k.vis_lanes = 4;
   if (k.soft_jobs <= 0) k.soft_jobs = 256;
   if (k.soft_pixels <= 0) k.soft_pixels = int64_t(8) << 20;
   if (k.fold_ms <= 0) k.fold_ms = 100;

@@ -73,10 +73,12 @@ class Request:
 
 def primary_tile(r: Request) -> int:
     """Pixels per side of a primary root when the scene and size were not
-    tuned: 8 from 512 pixels up, 4 below (the reference's 16 leaves too few
-    roots to fill the GPU on dense meshes: 1024^2 of the displaced sphere in
-    26 ms at 8 against 34 ms at 16; 256^2 in 34 ms at 4 against 126 at 16)."""
-    return 8 if min(r.W, r.H) >= 512 else 4
+    tuned: 4 from 512 pixels up, 2 below.  The reference's 16 leaves too few
+    roots to fill the GPU on dense meshes, and a smaller root beam splits
+    fewer times in sequence: the displaced sphere's primary ids at 256^2 in
+    20 ms at tile 1, 24 at 2, 33 at 4 and 124 at 16; at 1024^2 in 18.5 ms at
+    2 and 20 at 4."""
+    return 4 if min(r.W, r.H) >= 512 else 2
 
 
 class _Scene:
@@ -91,7 +93,7 @@ class Server:
     """Resident scenes on one GPU behind the library's request loop."""
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 25,
-                 cache=None, kd_on_gpu: bool = True, vis_lanes: int = 2, fold_ms: float = 100.0,
+                 cache=None, kd_on_gpu: bool = True, vis_lanes: int = 4, fold_ms: float = 100.0,
                  soft_pixels: int = 8 << 20):
         from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
@@ -131,16 +133,17 @@ class Server:
     def slots(self):
         return self.scenes
 
-    def tune(self, sizes=(256, 512, 1024), tiles=(4, 8, 16, 32), reps: int = 2):
+    def tune(self, sizes=(256, 512, 1024), tiles=(1, 2, 4, 8, 16), reps: int = 2, max_roots: int = 1 << 18):
         """Autotunes the primary tile of every resident scene at each square
         size: each candidate's primary request is timed through the serving
-        lanes (the fastest of `reps` after a warm-up).  Call before the
-        stream starts.  Untuned sizes use `primary_tile`."""
+        lanes (the fastest of `reps` after a warm-up); tiles that would make
+        more than `max_roots` roots are not tried.  Call before the stream
+        starts.  Untuned sizes use `primary_tile`."""
         out = {}
         for name in self.scenes:
             for W in sizes:
                 ms = {}
-                for tile in tiles:
+                for tile in [t for t in tiles if -(-W // t) ** 2 <= max_roots] or [max(tiles)]:
                     t = []
                     for _ in range(reps + 1):
                         r = self.submit(Request("primary", name, W, W, tile=tile))

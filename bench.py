@@ -497,7 +497,7 @@ def serving_measure(n: int = 300):
     with Server(sc, memory_budget_gb=8.0) as srv:
         # admitting a scene: finalise + kd-tree built on the GPU (bt_kd_build_gpu)
         out["scene_prep_ms"] = {k: round(v, 1) for k, v in srv.prep_ms.items()}
-        out["tuned_tiles"] = srv.tune(sizes=(256, 512, 1024), tiles=(4, 8, 16, 32))  # the autotuner, before the stream
+        out["tuned_tiles"] = srv.tune(sizes=(256, 512, 1024))  # the autotuner, before the stream
         poisson_stream(srv, rate=50.0, n=12, sizes=(256,), seed=11)  # warm-up
         for label, rate in (("configured_50", 50.0), ("saturated_500", 500.0)):
             _, summ = poisson_stream(srv, rate=rate, n=n, sizes=(256, 512, 1024), seed=7)

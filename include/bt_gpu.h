@@ -457,7 +457,7 @@ typedef struct {
 } bt_completion;
 
 typedef struct {
-  int32_t vis_lanes;         /* lanes for primary ids and point masks (0: 2) */
+  int32_t vis_lanes;         /* lanes for primary ids and point masks (0: 4) */
   int32_t soft_jobs;         /* requests one soft run holds at most (0: 256) */
   int64_t soft_pixels;       /* pixels one soft run holds at most (0: 8M) */
   int64_t capacity;          /* sub-beam records per queue of each lane (0: the context's) */
