@@ -474,10 +474,12 @@ BT_HD void beamCorners(const Poly<N>& c, Beam& b) {
 
 // Cleaned corners and axes of a piece; false (and `dropped` = |area|) for
 // slivers below minArea (BeamCtx::beamGeom, beam_core.h:200-221).
+// `clean`: p is already a cleanPoly result, whose cleaning would change
+// nothing (cleanPoly returns only after a pass without a change).
 template <int N>
-BT_CLIP bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped) {
+BT_CLIP bool beamGeom(const Query& q, const Poly<N>& p, int negBits, Beam& b, float& dropped, bool clean = false) {
   Poly<N> c = p;
-  cleanPoly(c, q.eps);
+  if (!clean) cleanPoly(c, q.eps);
   float A = c.n >= 3 ? c.area() : 0.f;
   if (c.n < 3 || A < q.minArea) {
     float a0 = p.area();
@@ -766,8 +768,11 @@ BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* 
 }
 
 // Clips B by L[0..nl) one line at a time, most-cutting edge first; pieces
-// outside some line go to sink.push(0, p), pieces inside every line to
-// sink.push(1, p) (BeamCtx::clipTri with orderEdges, beam_core.h:420-479).
+// outside some line go to sink.push(0, p, clean), pieces inside every line
+// to sink.push(1, p, clean) (BeamCtx::clipTri with orderEdges,
+// beam_core.h:420-479).  `clean` says the piece is a cleanPoly result: the
+// beam's own corners (every beam is made from a cleaned polygon) and the
+// halves of a split, but not the halves of a pentagon.
 // Line li (run-time, < 5) of five held in registers.
 BT_HD Line lineAt(const Line* L, int li) {
   Line r = L[0];
@@ -855,6 +860,7 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
     p.x[i] = B.qx[i];
     p.y[i] = B.qy[i];
   }
+  bool pClean = true;
   int li = 0;
   for (;;) {
     bool inside = true;
@@ -867,14 +873,14 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
       int c = classifyPoly<N, F64>(p, Lk, q.eps, &Ek);
       if (!(c & 2)) continue;
       if (!(c & 1)) {
-        if (!sink.push(0, p)) ok = false;
+        if (!sink.push(0, p, pClean)) ok = false;
         inside = false;
         break;
       }
       Poly<N> in, out;
       if (!splitPoly<N, F64>(p, Lk, q.eps, in, out, &Ek)) return false;
       cleanPoly(out, q.eps);
-      if (out.n >= 3 && !sink.push(0, out)) ok = false;
+      if (out.n >= 3 && !sink.push(0, out, true)) ok = false;
       cleanPoly(in, q.eps);
       if (in.n < 3) {
         inside = false;
@@ -889,14 +895,17 @@ BT_CLIP bool clipTri(const Query& q, const Beam& B, const Line* Lin, int nl, Sin
         stackLine[sp] = li + 1;
         ++sp;
         p = a;
+        pClean = false;
       } else {
         p = in;
+        pClean = true;
       }
     }
-    if (inside && !sink.push(1, p)) ok = false;
+    if (inside && !sink.push(1, p, pClean)) ok = false;
     if (sp == 0) break;
     --sp;
     p = stack[sp];
+    pClean = false;
     li = stackLine[sp];
   }
   return ok;

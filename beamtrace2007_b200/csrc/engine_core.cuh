@@ -516,7 +516,7 @@ BT_HD int testOne(const SceneDev& s, const Query& q, SubBeam& r, Beam& B, Stats&
 struct AreaSink {
   float newArea;
   int slots0, slots1;
-  BT_HD bool push(int l, const Poly<kPolyMax>& p) {
+  BT_HD bool push(int l, const Poly<kPolyMax>& p, bool) {
     if (p.n > 5) return false;
     if (l == 1)
       newArea += p.area();
@@ -543,10 +543,10 @@ struct EmitSink {
   int t;
   Env* env;
   Stats* st;
-  BT_HD void one(bool hitNow, bool queued, const Poly<kPolyMax>& piece) {
+  BT_HD void one(bool hitNow, bool queued, const Poly<kPolyMax>& piece, bool clean) {
     Beam nb;
     float dropped = 0;
-    if (!beamGeom(*q, piece, parent->neg, nb, dropped)) {
+    if (!beamGeom(*q, piece, parent->neg, nb, dropped, clean)) {
       st->dropped += double(dropped);
       env->dropped(dropped);
       return;
@@ -560,17 +560,17 @@ struct EmitSink {
     pr.hit = hitNow ? t : parent->hit;
     env->queue(pr);
   }
-  BT_HD bool push(int l, const Poly<kPolyMax>& p0) {
+  BT_HD bool push(int l, const Poly<kPolyMax>& p0, bool clean) {
     const bool hitNow = l == 1;
     const bool queued = !(hitNow && q->mode == kModeAnyHit);
     if (p0.n == 5) {
       Poly<kPolyMax> a, b;
       splitFive(p0, a, b);
       st->fiveSplits++;
-      one(hitNow, queued, a);
-      one(hitNow, queued, b);
+      one(hitNow, queued, a, false);
+      one(hitNow, queued, b, false);
     } else {
-      one(hitNow, queued, p0);
+      one(hitNow, queued, p0, clean);
     }
     return true;
   }
@@ -582,12 +582,13 @@ struct EmitSink {
 constexpr int kPieceLog = 8;
 struct PieceLog {
   int count;
-  int8_t level[kPieceLog], n[kPieceLog];
+  int8_t level[kPieceLog], n[kPieceLog], clean[kPieceLog];
   float x[kPieceLog][5], y[kPieceLog][5];
-  BT_HD void add(int l, const Poly<kPolyMax>& p) {
+  BT_HD void add(int l, const Poly<kPolyMax>& p, bool isClean) {
     if (count < kPieceLog) {
       level[count] = int8_t(l);
       n[count] = int8_t(p.n);
+      clean[count] = int8_t(isClean);
       BT_UNROLL for (int i = 0; i < 5; ++i) {
         x[count][i] = i < p.n ? p.x[i] : 0.f;
         y[count][i] = i < p.n ? p.y[i] : 0.f;
@@ -605,10 +606,10 @@ struct ClipSink {
   AreaSink area;
   EmitSink<Env> emit;
   PieceLog* log;
-  BT_HD bool push(int l, const Poly<kPolyMax>& p) {
-    if (emitting) return emit.push(l, p);
-    if (!area.push(l, p)) return false;
-    if (log) log->add(l, p);
+  BT_HD bool push(int l, const Poly<kPolyMax>& p, bool clean) {
+    if (emitting) return emit.push(l, p, clean);
+    if (!area.push(l, p, clean)) return false;
+    if (log) log->add(l, p, clean);
     return true;
   }
 };
@@ -657,7 +658,7 @@ BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const T
         p.x[i] = i < 5 ? log->x[k][i] : 0.f;
         p.y[i] = i < 5 ? log->y[k][i] : 0.f;
       }
-      emit.push(log->level[k], p);
+      emit.push(log->level[k], p, log->clean[k] != 0);
     }
     return;
   }

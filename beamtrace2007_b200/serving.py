@@ -120,7 +120,7 @@ class Server:
         cfg = N.ServeConfig(vis_lanes=vis_lanes, soft_jobs=256, soft_pixels=soft_pixels, capacity=queue_records,
                             fold_ms=fold_ms, memory_budget=self.budget)
         N.check(N.lib().bt_gpu_serve_start(self.engine._h, C.byref(cfg)))
-        self.tiles: dict = {}   # (scene, W, H) -> primary tile chosen by `tune`
+        self.tiles: dict = {}   # (kind, scene, W, H) -> root tile chosen by `tune`
         self.lock = threading.Lock()
         self.inflight: dict[int, tuple] = {}   # ticket -> (request, its C struct and output arrays)
         self.waiting: collections.deque[Request] = collections.deque()  # refused for memory, in arrival order
@@ -133,26 +133,31 @@ class Server:
     def slots(self):
         return self.scenes
 
-    def tune(self, sizes=(256, 512, 1024), tiles=(1, 2, 4, 8, 16), reps: int = 2, max_roots: int = 1 << 18):
-        """Autotunes the primary tile of every resident scene at each square
-        size: each candidate's primary request is timed through the serving
-        lanes (the fastest of `reps` after a warm-up); tiles that would make
-        more than `max_roots` roots are not tried.  Call before the stream
-        starts.  Untuned sizes use `primary_tile`."""
+    def tune(self, sizes=(256, 512, 1024), tiles=(1, 2, 4, 8, 16), reps: int = 2, max_roots: int = 1 << 18,
+             kinds=("primary", "point")):
+        """Autotunes the root tile of every resident scene at each square
+        size, for primary-id and for point-mask requests (a point request
+        also traces a point-shadow root per primary polygon, and smaller
+        tiles make more polygons): each candidate request is timed through
+        the serving lanes (the fastest of `reps` after a warm-up); tiles that
+        would make more than `max_roots` roots are not tried.  Call before
+        the stream starts.  Untuned sizes use `primary_tile`."""
         out = {}
-        for name in self.scenes:
-            for W in sizes:
-                ms = {}
-                for tile in [t for t in tiles if -(-W // t) ** 2 <= max_roots] or [max(tiles)]:
-                    t = []
-                    for _ in range(reps + 1):
-                        r = self.submit(Request("primary", name, W, W, tile=tile))
-                        r.event.wait()
-                        t.append(r.latency * 1e3)
-                    ms[tile] = float(np.min(t[1:]))
-                best = min(ms, key=ms.get)
-                self.tiles[(name, W, W)] = best
-                out[f"{name}/{W}"] = {"tile": best, "ms": {k: round(v, 2) for k, v in ms.items()}}
+        for kind in kinds:
+            for name in self.scenes:
+                for W in sizes:
+                    ms = {}
+                    for tile in [t for t in tiles if (-(-W // t)) ** 2 <= max_roots] or [max(tiles)]:
+                        t = []
+                        for _ in range(reps + 1):
+                            r = self.submit(Request(kind, name, W, W, tile=tile))
+                            r.event.wait()
+                            t.append(r.latency * 1e3)
+                        ms[tile] = float(np.min(t[1:]))
+                    best = min(ms, key=ms.get)
+                    self.tiles[(kind, name, W, W)] = best
+                    key = f"{name}/{W}" if kind == "primary" else f"{kind}:{name}/{W}"
+                    out[key] = {"tile": best, "ms": {k: round(v, 2) for k, v in ms.items()}}
         return out
 
     def camera(self, r: Request):
@@ -169,7 +174,8 @@ class Server:
             raise ValueError(f"bad request {r.kind} / {r.scene}")
         r.arrival = time.perf_counter()
         if r.kind != "soft" and not r.tile:
-            r.tile = self.tiles.get((r.scene, r.W, r.H)) or primary_tile(r)
+            r.tile = (self.tiles.get((r.kind, r.scene, r.W, r.H)) or self.tiles.get(("primary", r.scene, r.W, r.H))
+                      or primary_tile(r))
         with self.lock:
             if self.waiting or not self._submit(r):
                 self.waiting.append(r)

@@ -58,7 +58,8 @@ def test_mixed_stream_same_as_alone(gpu):
               "building": scene("building", floors=1, furniture=2)[0]}
     with Server(scenes, memory_budget_gb=8.0) as srv:
         tuned = srv.tune(sizes=(64, 128), tiles=(8, 16), reps=1)
-        assert set(tuned) == {f"{s}/{w}" for s in scenes for w in (64, 128)}
+        assert set(tuned) == ({f"{s}/{w}" for s in scenes for w in (64, 128)}
+                              | {f"point:{s}/{w}" for s in scenes for w in (64, 128)})
         reqs, summary = poisson_stream(srv, rate=200.0, n=40, sizes=(64, 96, 128), seed=3)
         assert summary["errors"] == 0, [r.error for r in reqs if r.error]
         assert summary["p99_ms"] >= summary["p50_ms"] > 0
