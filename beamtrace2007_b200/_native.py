@@ -81,7 +81,8 @@ class GpuConfig(C.Structure):
                 ("capacity", C.c_int64), ("blocks_per_sm", C.c_int32), ("kernel_timing", C.c_int32),
                 ("max_retries", C.c_int32), ("tail_records", C.c_int64),
                 ("eps_stats", C.c_int32), ("yield_pct", C.c_int32),
-                ("fuse_primary", C.c_int32), ("eps_fp64", C.c_int32)]
+                ("fuse_primary", C.c_int32), ("eps_fp64", C.c_int32),
+                ("graph_rounds", C.c_int32)]
 
 
 class SoftOpts(C.Structure):

@@ -1416,6 +1416,13 @@ struct bt_gpu_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t rev[2] = {nullptr, nullptr};
   cudaEvent_t kev[32] = {};  // kernel_timing: 2 per round of a batch, around the trace kernel
+  // graph_rounds: the last captured batch of rounds, one for full rounds and
+  // one for tail rounds, with the launch parameters it was captured with
+  struct RoundGraph {
+    cudaGraphExec_t exec = nullptr;
+    RoundParams p;
+    int app = -1, mode = -1, grids[4] = {0, 0, 0, 0};
+  } graphs[2];
   // serving (serve.cpp): a lane views its parent's scene pool and owns only
   // its engine buffers; the parent's scene lock is held shared while a lane
   // works and exclusively while bt_gpu_add_scene replaces the arrays
@@ -1449,6 +1456,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->yield_pct = 0;
   c->fuse_primary = 0;
   c->eps_fp64 = 0;
+  c->graph_rounds = 1;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1597,6 +1605,7 @@ struct RoundRunner {
 
   // Clears the per-run state of R roots and sets the launch parameters.
   int begin(const AppParams& app0, int R) {
+    memset(&p, 0, sizeof p);  // no stray padding: graph_rounds compares launch parameters bytewise
     c->lastProduced = -1;  // a new run overwrites what bt_gpu_last_polys would read
     int e = ensureRoots(c, size_t(R));
     if (e) return e;
@@ -1688,36 +1697,91 @@ struct RoundRunner {
     return BT_OK;
   }
 
-  // One batch of kRoundsPerCheck rounds, then the counters.
-  int batch() {
+  // One batch of kRoundsPerCheck rounds as one CUDA graph (graph_rounds):
+  // the launches are captured once and replayed while their parameters stay
+  // the same (a new frame with the same camera, light and buffers replays
+  // the graph of the last one); otherwise captured again and the
+  // executable graph updated in place.
+  int graphBatch(bool tail) {
+    auto& g = c->graphs[tail ? 1 : 0];
+    RoundParams key = p;
+    key.cur = 0;
+    const int grids[4] = {gA, gT, gC, gF};
+    if (!g.exec || g.app != App || g.mode != mode || memcmp(grids, g.grids, sizeof grids) != 0 ||
+        memcmp(&key, &g.p, sizeof key) != 0) {
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      const int r0 = round, l0 = launches, t0 = tailRounds;
+      launchRounds(tail, false);
+      round = r0;
+      launches = l0;
+      tailRounds = t0;
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      if (ce != cudaSuccess || !graph) {
+        setErr("capturing a batch of rounds: %s", cudaGetErrorString(ce));
+        return BT_ERR_CUDA;
+      }
+      cudaError_t ue = cudaErrorUnknown;
+      if (g.exec) {
+        cudaGraphExecUpdateResultInfo ui;
+        ue = cudaGraphExecUpdate(g.exec, graph, &ui);
+        if (ue != cudaSuccess) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(g.exec);
+          g.exec = nullptr;
+        }
+      }
+      if (ue != cudaSuccess) {
+        const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        if (ie != cudaSuccess) {
+          cudaGraphDestroy(graph);
+          g.exec = nullptr;
+          setErr("instantiating a batch of rounds: %s", cudaGetErrorString(ie));
+          return BT_ERR_CUDA;
+        }
+      }
+      cudaGraphDestroy(graph);
+      g.p = key;
+      g.app = App;
+      g.mode = mode;
+      memcpy(g.grids, grids, sizeof grids);
+    }
+    CK(cudaGraphLaunch(g.exec, c->stream));
+    for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
+      launches += tail ? 2 : 4;
+      if (tail) tailRounds++;
+    }
+    return BT_OK;
+  }
+
+  // The launches of kRoundsPerCheck rounds on the engine's stream (full
+  // rounds: admit, trace, clip; tail rounds: the fused kernel; then the
+  // bookkeeping kernel), with the kernel_timing events when `events`.
+  void launchRounds(bool tail, bool events) {
     const int n = p.numRoots;
-    CK(cudaEventRecord(c->rev[0], c->stream));
-    // the mode of this batch of rounds, from the counters of the last one
-    const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
-                      c->cfg.tail_records >= 0;
     for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
       p.cur = round & 1;
       if (tail) {
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+        if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
           traceKernel<App, true, kVoteFp64F<App>><<<gF, kThreads, 0, c->stream>>>(p);
         else if (mode == kVoteLog)
           traceKernel<App, true, kVoteLog><<<gF, kThreads, 0, c->stream>>>(p);
         else
           traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+        if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         launches += 2;
         tailRounds++;
       } else {
         admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k], c->stream));
+        if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
           traceKernel<App, false, kVoteFp64F<App>><<<gT, kThreads, 0, c->stream>>>(p);
         else if (mode == kVoteLog)
           traceKernel<App, false, kVoteLog><<<gT, kThreads, 0, c->stream>>>(p);
         else
           traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
-        if (ktime) CK(cudaEventRecord(c->kev[2 * k + 1], c->stream));
+        if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         if (mode == kVoteFp64)
           clipKernel<App, App == kAppSoft><<<gC, kThreads, 0, c->stream>>>(p);
         else
@@ -1725,6 +1789,21 @@ struct RoundRunner {
         launches += 4;
       }
       roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
+    }
+  }
+
+  // One batch of kRoundsPerCheck rounds, then the counters.
+  int batch() {
+    const int n = p.numRoots;
+    CK(cudaEventRecord(c->rev[0], c->stream));
+    // the mode of this batch of rounds, from the counters of the last one
+    const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
+                      c->cfg.tail_records >= 0;
+    if (c->cfg.graph_rounds && !ktime) {
+      const int e = graphBatch(tail);
+      if (e) return e;
+    } else {
+      launchRounds(tail, ktime);
     }
     CK(cudaEventRecord(c->rev[1], c->stream));
     CK(cudaGetLastError());
@@ -2101,6 +2180,8 @@ int bt_gpu_destroy(bt_gpu_ctx* c) {
                   c->dKn, c->dKtri, c->dKroot, c->dKeepBlocks};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (auto& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->rev)
@@ -2937,7 +3018,14 @@ int laneCreate(bt_gpu_ctx* parent, int64_t capacity, int64_t pixels, int jobs, b
     return code;
   };
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(BT_ERR_CUDA);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(BT_ERR_CUDA);
+  // Visibility lanes (no pixel arena) take the device's highest stream
+  // priority: their CTAs are scheduled ahead of a long soft run's pending
+  // ones, so a small primary or point request does not queue behind it.
+  int prLeast = 0, prGreatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest) != cudaSuccess) return fail(BT_ERR_CUDA);
+  if (cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, pixels > 0 ? prLeast : prGreatest) !=
+      cudaSuccess)
+    return fail(BT_ERR_CUDA);
   for (auto& ev : c->ev)
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(BT_ERR_CUDA);
   for (auto& ev : c->rev)

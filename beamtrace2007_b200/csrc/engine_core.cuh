@@ -642,6 +642,19 @@ BT_CLIP int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, cons
   return sink.area.slots0 + (q.mode == kModeAnyHit ? 0 : sink.area.slots1);
 }
 
+// Pass 2 of a clip whose pieces overflowed the log: the clip again, out of
+// line (rare), with the pieces streamed to emit.
+template <class Env, bool F64>
+BT_COLD void replayClip(const Query& q, const Beam& B, Line* L, int nl, const EmitSink<Env>& emit,
+                        const Line64* e64) {
+  ClipSink<Env> sink;
+  sink.emitting = 1;
+  sink.emit = emit;
+  sink.log = nullptr;
+  uint32_t five = 0;  // counted in pass 1
+  clipTri<kPolyMax, ClipSink<Env>, F64>(q, B, L, nl, sink, five, e64);
+}
+
 template <class Env, bool F64 = false>
 BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const TriInfo& ti, Line* L, int nl, Env& env,
                         Stats& st, const PieceLog* log = nullptr, const Line64* e64 = nullptr) {
@@ -662,12 +675,7 @@ BT_CLIP void splitPass2(const Query& q, const SubBeam& r, const Beam& B, const T
     }
     return;
   }
-  ClipSink<Env> sink;
-  sink.emitting = 1;
-  sink.emit = emit;
-  sink.log = nullptr;
-  uint32_t five = 0;  // counted in pass 1
-  clipTri<kPolyMax, ClipSink<Env>, F64>(q, B, L, nl, sink, five, e64);
+  replayClip<Env, F64>(q, B, L, nl, emit, e64);
 }
 
 // Root admission: pre-split pieces become records at the kd root; pieces

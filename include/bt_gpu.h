@@ -136,6 +136,10 @@ typedef struct {
                                (from the same float vertices) in the votes and the clip, before a split;
                                results then differ from the reference's float build (eps_band_corners and
                                eps_fp64_flips count the band corners and the re-decided ones) */
+  int32_t graph_rounds;     /* nonzero (default): each batch of rounds (the admit / trace / clip /
+                               bookkeeping launches between two looks at the counters) is replayed as one
+                               CUDA graph, captured again only when the launch parameters change (the
+                               executable graph updated in place); same results.  Off with kernel_timing */
 } bt_gpu_config;
 
 typedef struct {

@@ -319,3 +319,36 @@ def test_last_polys_instead_of_a_second_run(gpu):
         cnt = C.c_int64()
         assert N.lib().bt_gpu_last_polys(g._h, C.byref(st), C.byref(cnt)) == -1
     assert launches > 0
+
+
+def test_graph_rounds_same_results(gpu):
+    """Batches of rounds replayed as CUDA graphs (graph_rounds, the default)
+    give bitwise the results of launching the rounds one by one: soft
+    shadows (a second frame replays the captured graphs), a tiny budget
+    whose retry passes change the launch parameters, a batch of jobs, and
+    primary ids and point masks."""
+    from beamtrace2007_b200.renderer import make_camera
+    s, ps = scene("plant")
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 128, 96)
+    L = s.light_array()
+    light = np.asarray(s.point_light, np.float32)
+    cams = [make_camera(v.eye, v.target, v.fov + 4 * i, s.up, 64 + 16 * i, 48) for i in range(3)]
+    lights = [s.light_array(k) for k in (0.5, 1.0, 3.0)]
+    out = {}
+    for gr in (False, True):
+        r = []
+        with _renderer(ps, graph_rounds=gr) as g:
+            for _ in range(2):
+                a = g.soft_shadows(cam, L, exact=True)
+                r += [a.vis, a.E]
+            r += [b.vis for b in g.batch_soft(cams, lights, exact=True)]
+            r += [g.primary_ids(cam, tile=8)] + list(g.point_mask(cam, light, tile=8))
+        with _renderer(ps, graph_rounds=gr, budget=4, capacity=4096) as g:
+            c = g.soft_shadows(cam, L, exact=True)
+            assert c.info["retried_roots"] > 100
+            r += [c.vis, c.E]
+        out[gr] = r
+    assert len(out[False]) == len(out[True])
+    for a, b in zip(out[False], out[True]):
+        assert np.array_equal(a, b)
