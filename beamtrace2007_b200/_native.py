@@ -132,7 +132,8 @@ class Completion(C.Structure):
 
 class ServeConfig(C.Structure):
     _fields_ = [("vis_lanes", C.c_int32), ("soft_jobs", C.c_int32), ("soft_pixels", C.c_int64),
-                ("capacity", C.c_int64), ("fold_ms", C.c_double), ("memory_budget", C.c_int64)]
+                ("capacity", C.c_int64), ("fold_ms", C.c_double), ("memory_budget", C.c_int64),
+                ("soft_blocks_per_sm", C.c_int32)]
 
 
 class ServeStats(C.Structure):

@@ -3009,6 +3009,9 @@ int laneCreate(bt_gpu_ctx* parent, int64_t capacity, int64_t pixels, int jobs, b
   *out = nullptr;
   bt_gpu_ctx* c = new bt_gpu_ctx();
   c->cfg = parent->cfg;
+  // A lane's launch parameters change with every request (camera, light,
+  // folded roots), so a captured batch of rounds would never be replayed.
+  c->cfg.graph_rounds = 0;
   c->device = parent->device;
   c->sms = parent->sms;
   c->parent = parent;
@@ -3058,6 +3061,8 @@ int laneCreate(bt_gpu_ctx* parent, int64_t capacity, int64_t pixels, int jobs, b
 }
 
 void laneDestroy(bt_gpu_ctx* lane) { bt_gpu_destroy(lane); }
+
+void laneBlocksPerSm(bt_gpu_ctx* lane, int blocks) { lane->cfg.blocks_per_sm = blocks; }
 
 int laneVisibility(bt_gpu_ctx* c, int kind, int32_t scene, const bt_camera& cam, int32_t cull, int32_t tile,
                    const float* light, int32_t* tri, uint8_t* mask, bt_run_info* info) {

@@ -238,6 +238,7 @@ int bt_gpu_serve_start(bt_gpu_ctx* c, const bt_serve_config* cfg) {
   memset(&S->st, 0, sizeof S->st);
   btserve::useDevice(c);
   int e = btserve::laneCreate(c, k.capacity, k.soft_pixels, k.soft_jobs, &S->softLane);
+  if (!e && k.soft_blocks_per_sm > 0) btserve::laneBlocksPerSm(S->softLane, k.soft_blocks_per_sm);
   for (int i = 0; !e && i < k.vis_lanes; ++i) {
     bt_gpu_ctx* l = nullptr;
     e = btserve::laneCreate(c, k.capacity, 0, 0, &l);

@@ -40,6 +40,8 @@ class SoftFeed {
 // of `capacity` records (0: the parent's), root arrays and a pixel arena
 // for `pixels` pixels in up to `jobs` jobs per run.
 int laneCreate(bt_gpu_ctx* parent, int64_t capacity, int64_t pixels, int jobs, bt_gpu_ctx** out);
+// Persistent CTAs per SM of a lane's kernels (bt_gpu_config.blocks_per_sm).
+void laneBlocksPerSm(bt_gpu_ctx* lane, int blocks);
 void laneDestroy(bt_gpu_ctx* lane);
 // Takes the parent's current scene pool (call with the parent's scene lock held).
 void laneView(bt_gpu_ctx* lane);

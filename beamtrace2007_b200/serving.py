@@ -94,7 +94,7 @@ class Server:
 
     def __init__(self, scenes: dict, memory_budget_gb: float = 8.0, device: int = 0, queue_records: int = 1 << 25,
                  cache=None, kd_on_gpu: bool = True, vis_lanes: int = 4, fold_ms: float = 100.0,
-                 soft_pixels: int = 8 << 20):
+                 soft_pixels: int = 8 << 20, soft_blocks_per_sm: int = 0):
         from .ingest import SceneCache
         from .renderer import GpuRenderer, PreparedScene
         kd_device = device if kd_on_gpu else None
@@ -118,7 +118,7 @@ class Server:
             self.prep_ms[name] = (time.perf_counter() - t0) * 1e3
             self.scenes[name] = _Scene(name, sd, ps, sid)
         cfg = N.ServeConfig(vis_lanes=vis_lanes, soft_jobs=256, soft_pixels=soft_pixels, capacity=queue_records,
-                            fold_ms=fold_ms, memory_budget=self.budget)
+                            fold_ms=fold_ms, memory_budget=self.budget, soft_blocks_per_sm=soft_blocks_per_sm)
         N.check(N.lib().bt_gpu_serve_start(self.engine._h, C.byref(cfg)))
         self.tiles: dict = {}   # (kind, scene, W, H) -> root tile chosen by `tune`
         self.lock = threading.Lock()

@@ -467,6 +467,9 @@ typedef struct {
   int64_t capacity;          /* sub-beam records per queue of each lane (0: the context's) */
   double fold_ms;            /* soft requests join a running soft run this long after it starts (0: 100) */
   int64_t memory_budget;     /* bytes (0: no limit) */
+  int32_t soft_blocks_per_sm;  /* CTAs per SM of the soft lane's persistent kernels (<= 0: as many as
+                                  fit).  Fewer leave room on every SM for the visibility lanes' kernels
+                                  beside a running soft run; measured, 1 or 2 made both kinds slower */
 } bt_serve_config;
 
 typedef struct {

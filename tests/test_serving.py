@@ -94,6 +94,10 @@ def test_primary_does_not_wait_behind_a_soft_run(gpu):
     a visibility lane at the same time and comes back first."""
     from beamtrace2007_b200.serving import Request, Server
     with Server({"plant": scene("plant")[0]}, memory_budget_gb=8.0, fold_ms=1.0) as srv:
+        # every lane has served a request (its buffers allocated) before the race
+        warm = [srv.submit(Request("primary", "plant", 64, 64)) for _ in range(16)]
+        warm.append(srv.submit(Request("soft", "plant", 32, 32)))
+        assert all(r.event.wait(60) for r in warm)
         soft = srv.submit(Request("soft", "plant", 512, 512, light_scale=4.0))
         time.sleep(0.004)
         prim = srv.submit(Request("primary", "plant", 64, 64))
