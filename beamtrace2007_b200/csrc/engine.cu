@@ -1799,7 +1799,9 @@ struct RoundRunner {
     // the mode of this batch of rounds, from the counters of the last one
     const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
                       c->cfg.tail_records >= 0;
-    if (c->cfg.graph_rounds && !ktime) {
+    // (the legacy default stream, which the allocation-free entry point
+    // runs on, cannot be captured)
+    if (c->cfg.graph_rounds && !ktime && c->stream != nullptr) {
       const int e = graphBatch(tail);
       if (e) return e;
     } else {
