@@ -416,7 +416,7 @@ def batched_measure(g, s, N, lib, C, steps):
 
 
 def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: int = 200_000, reps: int = 1,
-                         seed: int = 2024, tune: bool = True):
+                         seed: int = 2024, tune: bool = True, plain_reps: int | None = None):
     """The batched-jobs workload: receiver/occluder pairs (icosphere or
     torus, meshes log-uniform between 100 and `max_tris` triangles, plus a
     ground quad), square resolutions from `sizes`, light scale U[0.25, 4],
@@ -427,9 +427,12 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
     job at 64x64 before the runs.  The warm-up is one small job (a pass of
     the whole mix can take tens of seconds); `heaviest`: the two longest
     jobs alone, with their triangle tests (the algorithm's work: the engine's
-    counters equal the reference's)."""
+    counters equal the reference's).  The batch is timed `reps` times and
+    the jobs one by one the first `plain_reps` of them (default: all);
+    medians of each."""
     from beamtrace2007_b200 import scenes
     from beamtrace2007_b200.autotune import tune_engine
+    plain_reps = reps if plain_reps is None else plain_reps
     from beamtrace2007_b200.renderer import GpuRenderer, PreparedScene, make_camera
     rng = np.random.default_rng(seed)
     specs = [(int(np.exp(rng.uniform(np.log(100), np.log(max_tris)))), int(rng.choice(list(sizes))),
@@ -464,6 +467,8 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
     for rep in range(reps):
         _, info = g.batch_soft(cams, lights, exact=True, scenes=ids, device_outputs=True)
         batch.append(info["ms_total"])
+        if rep >= plain_reps:
+            continue
         t = 0.0
         for k in range(len(cams)):
             _, i1 = g.batch_soft([cams[k]], [lights[k]], exact=True, scenes=[ids[k]], device_outputs=True)
@@ -474,7 +479,7 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
     pb, pp = float(np.median(batch)), float(np.median(plain))
     top = sorted(alone, key=lambda k: -alone[k][0])[:2]
     return {"jobs": len(jobs), "triangles": int(sum(ps.num_tris for _, ps, _, _ in jobs)), "pixels": int(px),
-            "sizes": list(sizes), "max_tris": max_tris, "reps": reps,
+            "sizes": list(sizes), "max_tris": max_tris, "reps": reps, "plain_reps": len(plain),
             "value": px / pb * 1e3, "unit": "px/s", "one_by_one_value": px / pp * 1e3, "ratio_vs_one_by_one": pp / pb,
             "ms_batch": pb, "ms_one_by_one": pp, "host_prep_s": prep_s, "autotuned": tuned,
             "heaviest": [{"job": k, "tris": jobs[k][1].num_tris, "res": cams[k].W, "light_scale": round(specs[k][2], 3),
@@ -639,7 +644,7 @@ def main():
         # the batched-jobs workload as configured (64 jobs of up to 200K
         # triangles at up to 512^2), one repetition; and a mix of small jobs
         # (32 jobs of <= 20K triangles at 64-128^2) with three
-        line["batched_jobs"] = batched_jobs_measure()
+        line["batched_jobs"] = batched_jobs_measure(reps=3, plain_reps=1)
         line["batched_jobs_small"] = batched_jobs_measure(n_jobs=32, max_tris=20_000, sizes=(64, 128), reps=3,
                                                           tune=False)
         line["visibility"] = visibility_measure()
