@@ -803,7 +803,12 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
   Stats st;
   st.clear();
   for (;;) {
-    if (__ldcv(&p.ctr->done)) break;
+    // Stop when the pass is done or every root is claimed (claims may
+    // overshoot).  rootNext moves while other warps claim, so lane 0 decides
+    // for its warp: the shuffles below need all 32 lanes.
+    int stop = 0;
+    if (lane == 0) stop = (__ldcv(&p.ctr->done) || __ldcv(&p.ctr->rootNext) >= p.numRoots) ? 1 : 0;
+    if (__shfl_sync(kFull, stop, 0)) break;
     int base = -1, fit = 0;
     if (lane == 0) {
       const unsigned long long res = (unsigned long long)p.reserve, cap = (unsigned long long)p.capacity;
@@ -1422,6 +1427,7 @@ struct bt_gpu_ctx {
     cudaGraphExec_t exec = nullptr;
     RoundParams p;
     int app = -1, mode = -1, grids[4] = {0, 0, 0, 0};
+    bool admit = true;
   } graphs[2];
   // serving (serve.cpp): a lane views its parent's scene pool and owns only
   // its engine buffers; the parent's scene lock is held shared while a lane
@@ -1702,16 +1708,16 @@ struct RoundRunner {
   // the same (a new frame with the same camera, light and buffers replays
   // the graph of the last one); otherwise captured again and the
   // executable graph updated in place.
-  int graphBatch(bool tail) {
+  int graphBatch(bool tail, bool admit) {
     auto& g = c->graphs[tail ? 1 : 0];
     RoundParams key = p;
     key.cur = 0;
     const int grids[4] = {gA, gT, gC, gF};
-    if (!g.exec || g.app != App || g.mode != mode || memcmp(grids, g.grids, sizeof grids) != 0 ||
+    if (!g.exec || g.app != App || g.mode != mode || g.admit != admit || memcmp(grids, g.grids, sizeof grids) != 0 ||
         memcmp(&key, &g.p, sizeof key) != 0) {
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       const int r0 = round, l0 = launches, t0 = tailRounds;
-      launchRounds(tail, false);
+      launchRounds(tail, admit, false);
       round = r0;
       launches = l0;
       tailRounds = t0;
@@ -1744,11 +1750,12 @@ struct RoundRunner {
       g.p = key;
       g.app = App;
       g.mode = mode;
+      g.admit = admit;
       memcpy(g.grids, grids, sizeof grids);
     }
     CK(cudaGraphLaunch(g.exec, c->stream));
     for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
-      launches += tail ? 2 : 4;
+      launches += tail ? 2 : (admit ? 4 : 3);
       if (tail) tailRounds++;
     }
     return BT_OK;
@@ -1757,7 +1764,9 @@ struct RoundRunner {
   // The launches of kRoundsPerCheck rounds on the engine's stream (full
   // rounds: admit, trace, clip; tail rounds: the fused kernel; then the
   // bookkeeping kernel), with the kernel_timing events when `events`.
-  void launchRounds(bool tail, bool events) {
+  // `admit`: some roots are not admitted yet (else the admit kernel, which
+  // would find none, is not launched).
+  void launchRounds(bool tail, bool admit, bool events) {
     const int n = p.numRoots;
     for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
       p.cur = round & 1;
@@ -1773,7 +1782,7 @@ struct RoundRunner {
         launches += 2;
         tailRounds++;
       } else {
-        admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
+        if (admit) admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
         if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
           traceKernel<App, false, kVoteFp64F<App>><<<gT, kThreads, 0, c->stream>>>(p);
@@ -1786,7 +1795,7 @@ struct RoundRunner {
           clipKernel<App, App == kAppSoft><<<gC, kThreads, 0, c->stream>>>(p);
         else
           clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
-        launches += 4;
+        launches += admit ? 4 : 3;
       }
       roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
     }
@@ -1801,11 +1810,12 @@ struct RoundRunner {
                       c->cfg.tail_records >= 0;
     // (the legacy default stream, which the allocation-free entry point
     // runs on, cannot be captured)
+    const bool admit = hc.rootNext < n;
     if (c->cfg.graph_rounds && !ktime && c->stream != nullptr) {
-      const int e = graphBatch(tail);
+      const int e = graphBatch(tail, admit);
       if (e) return e;
     } else {
-      launchRounds(tail, ktime);
+      launchRounds(tail, admit, ktime);
     }
     CK(cudaEventRecord(c->rev[1], c->stream));
     CK(cudaGetLastError());
