@@ -1587,6 +1587,10 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
 // once).  Roots abandoned over budget are retried in a further pass with a
 // 16x budget.
 constexpr int kRoundsPerCheck = 8;
+// The first batch of a pass is this many rounds: a pass whose queue then
+// holds at most half a record per root (long walks, few splits: point
+// shadows of a sparse scene) goes to tail rounds at once.
+constexpr int kFirstRounds = 2;
 
 // The FP64 band re-decision is compiled for soft shadows only; the other
 // applications map it to the float votes (their kernels are not built twice).
@@ -1703,7 +1707,7 @@ struct RoundRunner {
     return BT_OK;
   }
 
-  // One batch of kRoundsPerCheck rounds as one CUDA graph (graph_rounds):
+  // One batch of kRoundsPerCheck rounds (not the first) as one CUDA graph (graph_rounds):
   // the launches are captured once and replayed while their parameters stay
   // the same (a new frame with the same camera, light and buffers replays
   // the graph of the last one); otherwise captured again and the
@@ -1766,9 +1770,10 @@ struct RoundRunner {
   // bookkeeping kernel), with the kernel_timing events when `events`.
   // `admit`: some roots are not admitted yet (else the admit kernel, which
   // would find none, is not launched).
-  void launchRounds(bool tail, bool admit, bool events) {
+  int launchRounds(bool tail, bool admit, bool events) {
     const int n = p.numRoots;
-    for (int k = 0; k < kRoundsPerCheck; ++k, ++round) {
+    const int nr = round == 0 ? kFirstRounds : kRoundsPerCheck;
+    for (int k = 0; k < nr; ++k, ++round) {
       p.cur = round & 1;
       if (tail) {
         if (events) cudaEventRecord(c->kev[2 * k], c->stream);
@@ -1799,6 +1804,7 @@ struct RoundRunner {
       }
       roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);
     }
+    return nr;
   }
 
   // One batch of kRoundsPerCheck rounds, then the counters.
@@ -1806,16 +1812,18 @@ struct RoundRunner {
     const int n = p.numRoots;
     CK(cudaEventRecord(c->rev[0], c->stream));
     // the mode of this batch of rounds, from the counters of the last one
-    const bool tail = round > 0 && hc.rootNext >= n && int64_t(hc.count[round & 1]) < tailRecords &&
-                      c->cfg.tail_records >= 0;
+    const int64_t queued = hc.count[round & 1];
+    const bool tail = round > 0 && hc.rootNext >= n && queued < tailRecords && c->cfg.tail_records >= 0 &&
+                      (round > kFirstRounds || 2 * queued <= n);
     // (the legacy default stream, which the allocation-free entry point
     // runs on, cannot be captured)
     const bool admit = hc.rootNext < n;
-    if (c->cfg.graph_rounds && !ktime && c->stream != nullptr) {
+    int nr = kRoundsPerCheck;
+    if (c->cfg.graph_rounds && !ktime && c->stream != nullptr && round > 0) {
       const int e = graphBatch(tail, admit);
       if (e) return e;
     } else {
-      launchRounds(tail, admit, ktime);
+      nr = launchRounds(tail, admit, ktime);
     }
     CK(cudaEventRecord(c->rev[1], c->stream));
     CK(cudaGetLastError());
@@ -1825,9 +1833,9 @@ struct RoundRunner {
     cudaEventElapsedTime(&ms, c->rev[0], c->rev[1]);
     if (info) {
       info->ms_round += ms;
-      info->round_launches += 3 * kRoundsPerCheck;
+      info->round_launches += 3 * nr;
       if (ktime)
-        for (int k = 0; k < kRoundsPerCheck; ++k) {
+        for (int k = 0; k < nr; ++k) {
           float t = 0;
           CK(cudaEventElapsedTime(&t, c->kev[2 * k], c->kev[2 * k + 1]));
           info->ms_kernel_trace += t;
