@@ -14,7 +14,7 @@ from conftest import piece_keys, scene, to_f32
 
 pytestmark = pytest.mark.gpu
 
-VIS_TOL = 1e-4   # |vis - vis_fp64|
+VIS_TOL = 1e-4   # |vis - vis_fp64|, the soft-shadow parity bar
 E_REL = 1e-5     # |E_exact - E_fp64| relative to the image's largest E
 
 

@@ -197,3 +197,17 @@ def test_autotune_engine_settings(gpu):
         a = g1.soft_shadows(cam, s.light_array(), exact=True)
         b = g2.soft_shadows(cam, s.light_array(), exact=True)
     assert np.array_equal(a.vis, b.vis) and np.array_equal(a.E, b.E)
+
+
+@pytest.mark.gpu
+def test_soft_lane_cta_cap_same_results(gpu):
+    """soft_blocks_per_sm caps the soft lane's persistent CTAs per SM (room
+    for the visibility lanes); results stay bitwise those of the request
+    alone."""
+    from beamtrace2007_b200.serving import Request, Server
+    with Server({"plant": scene("plant")[0]}, memory_budget_gb=8.0, soft_blocks_per_sm=1) as srv:
+        reqs = [srv.submit(Request("soft", "plant", 96, 72, light_scale=s)) for s in (0.5, 2.0)]
+        reqs.append(srv.submit(Request("primary", "plant", 96, 72)))
+        for r in reqs:
+            assert r.event.wait(120) and r.error is None, r.error
+            assert _same(r, _alone(srv, r))
