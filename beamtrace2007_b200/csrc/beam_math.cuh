@@ -747,10 +747,12 @@ BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, in
 // The cheap beam-triangle tests: trivial cases, depth line, far plane
 // (BeamCtx::classifyTri, beam_core.h:374-409).  The current hit's plane
 // comes from the beam (hitA, hitC, hitN).  F64: the edge votes re-decide
-// band corners with the FP64 edge lines e64.
+// band corners with the FP64 edge lines e64.  Without `separation`, the
+// last test (the beam's side planes, case (b)) is left out: a clip, whose
+// triangle the trace step already classified, needs only the lines L.
 template <bool F64 = false>
 BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl,
-                        const Line64* e64 = nullptr) {
+                        const Line64* e64 = nullptr, bool separation = true) {
   nl = 0;
   bool allIn = true;
   for (int k = 0; k < 3; ++k)
@@ -763,7 +765,7 @@ BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* 
     if (!testLine(q, B, closerLine(q, ti, farA, q.farCq, q.P.n, -1), L, nl, allIn)) return kTriKeep;
   }
   if (allIn) return kTriAllIn;
-  if (separated(q, B, ti)) return kTriKeep;
+  if (separation && separated(q, B, ti)) return kTriKeep;
   return kTriClip;
 }
 

@@ -628,7 +628,7 @@ BT_CLIP int splitPass1(const SceneDev& s, const Query& q, const SubBeam& r, cons
     setupRef64(s, q, leaf.x + uint32_t(r.cursor), ti, e64);
   else
     setupRef(s, q, leaf.x + uint32_t(r.cursor), ti);
-  classifyTri<F64>(q, B, ti, L, nl, e64);
+  classifyTri<F64>(q, B, ti, L, nl, e64, false);  // the lines only: the trace step classified it
   ClipSink<Env> sink;
   sink.emitting = 0;
   sink.area = AreaSink{0.f, 0, 0};
