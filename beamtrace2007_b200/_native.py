@@ -82,7 +82,7 @@ class GpuConfig(C.Structure):
                 ("max_retries", C.c_int32), ("tail_records", C.c_int64),
                 ("eps_stats", C.c_int32), ("yield_pct", C.c_int32),
                 ("fuse_primary", C.c_int32), ("eps_fp64", C.c_int32),
-                ("graph_rounds", C.c_int32)]
+                ("graph_rounds", C.c_int32), ("trace_ctas", C.c_int32)]
 
 
 class SoftOpts(C.Structure):

@@ -846,12 +846,14 @@ __global__ void __launch_bounds__(kThreads) admitKernel(const __grid_constant__ 
 // record leaf by leaf until it finishes or a triangle needs a clip; idle
 // lanes are refilled at once (one atomic per warp, ballot/popc ranks).
 // Records needing a clip are compacted into the clip queue.
-// (At least 3 CTAs per SM: lets the compiler keep the lane's state in up to
-// 170 registers; at 4 CTAs it spills, which costs more than the warps gain.
-// The tail-round variant clips inline with its polygons in registers and
-// takes 2 CTAs per SM: tail rounds hold too few records to need more warps.)
-template <int App, bool Fused, int Mode = kVoteFloat>
-__global__ void __launch_bounds__(kThreads, Fused ? 2 : 3) traceKernel(const __grid_constant__ RoundParams p) {
+// (At least `Ctas` CTAs per SM.  3 lets the compiler keep the lane's state
+// in up to 170 registers; 4 caps it at 128 with a few spills and 16 warps
+// per SM, which pays on a scene that sits in L1/L2 and costs on a larger
+// one (trace_ctas).  The tail-round variant clips inline with its polygons
+// in registers and takes 2 CTAs per SM: tail rounds hold too few records to
+// need more warps.)
+template <int App, bool Fused, int Mode = kVoteFloat, int Ctas = 3>
+__global__ void __launch_bounds__(kThreads, Fused ? 2 : Ctas) traceKernel(const __grid_constant__ RoundParams p) {
   const int lane = laneId();
   const unsigned ltMask = (1u << lane) - 1u;
   const int nCur = min(p.ctr->count[p.cur], p.capacity);
@@ -1463,6 +1465,7 @@ void bt_gpu_config_default(bt_gpu_config* c) {
   c->fuse_primary = 0;
   c->eps_fp64 = 0;
   c->graph_rounds = 1;
+  c->trace_ctas = 0;
 }
 
 int bt_gpu_available(bt_gpu_info* info) {
@@ -1587,6 +1590,9 @@ void fillInfo(bt_gpu_ctx* c, const Counters& hc, bt_run_info* info) {
 // once).  Roots abandoned over budget are retried in a further pass with a
 // 16x budget.
 constexpr int kRoundsPerCheck = 8;
+// Scenes up to this many bytes on the device (kd nodes and boxes, leaf
+// references, triangle normals) take the 4-CTA round trace kernel.
+constexpr int64_t kWideSceneBytes = int64_t(16) << 20;
 // The first batch of a pass is this many rounds: a pass whose queue then
 // holds at most half a record per root (long walks, few splits: point
 // shadows of a sparse scene) goes to tail rounds at once.
@@ -1597,12 +1603,19 @@ constexpr int kFirstRounds = 2;
 template <int App>
 constexpr int kVoteFp64F = App == kAppSoft ? kVoteFp64 : kVoteFloat;
 
+// The resident scene pool's bytes on the device: kd nodes and boxes, leaf
+// references, triangle normals and planes.
+int64_t sceneDeviceBytes(const bt_gpu_ctx* c) {
+  return int64_t(c->s.numNodes) * (8 + 32 + 4) + c->numRefs * 64 + c->numTris * 32;
+}
+
 template <int App>
 struct RoundRunner {
   bt_gpu_ctx* c;
   bt_run_info* info;
   RoundParams p;
   int mode = kVoteFloat;
+  bool wide = false;  // the 4-CTA round trace kernel
   bool ktime = false;
   int gA = 0, gT = 0, gC = 0, gF = 0, yieldAt = INT_MAX;
   int64_t tailRecords = 0;
@@ -1644,8 +1657,13 @@ struct RoundRunner {
     // in FP64, eps_stats logs them, else the reference's float votes
     mode = (App == kAppSoft && c->cfg.eps_fp64) ? kVoteFp64 : (c->cfg.eps_stats ? kVoteLog : kVoteFloat);
     gA = gridFor(c, admitKernel<App>);
+    // 4 trace CTAs per SM on a scene small enough to stay in L1/L2
+    // (trace_ctas 0), or as configured
+    wide = mode == kVoteFloat &&
+           (c->cfg.trace_ctas == 4 || (c->cfg.trace_ctas == 0 && sceneDeviceBytes(c) <= kWideSceneBytes));
     gT = mode == kVoteFp64 ? gridFor(c, traceKernel<App, false, kVoteFp64F<App>>)
          : mode == kVoteLog ? gridFor(c, traceKernel<App, false, kVoteLog>)
+         : wide             ? gridFor(c, traceKernel<App, false, kVoteFloat, 4>)
                             : gridFor(c, traceKernel<App, false>);
     gC = mode == kVoteFp64 ? gridFor(c, clipKernel<App, App == kAppSoft>) : gridFor(c, clipKernel<App>);
     gF = mode == kVoteFp64 ? gridFor(c, traceKernel<App, true, kVoteFp64F<App>>)
@@ -1793,6 +1811,8 @@ struct RoundRunner {
           traceKernel<App, false, kVoteFp64F<App>><<<gT, kThreads, 0, c->stream>>>(p);
         else if (mode == kVoteLog)
           traceKernel<App, false, kVoteLog><<<gT, kThreads, 0, c->stream>>>(p);
+        else if (wide)
+          traceKernel<App, false, kVoteFloat, 4><<<gT, kThreads, 0, c->stream>>>(p);
         else
           traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
         if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
@@ -3000,9 +3020,7 @@ int64_t sceneTris(bt_gpu_ctx* c, int32_t scene) {
   return scene >= 0 && size_t(scene) < c->pool.size() ? c->pool[size_t(scene)].numTris : 0;
 }
 
-int64_t sceneBytes(const bt_gpu_ctx* c) {
-  return int64_t(c->s.numNodes) * (8 + 32 + 4) + c->numRefs * 64 + c->numTris * 32;
-}
+int64_t sceneBytes(const bt_gpu_ctx* c) { return sceneDeviceBytes(c); }
 
 int64_t laneBytes(const bt_gpu_ctx* c) {
   return 3 * int64_t(c->capacity) * int64_t(sizeof(SubBeam)) + int64_t(c->rootCap) * 68 + c->pixCap * 40 +

@@ -216,7 +216,7 @@ class GpuRenderer:
     def __init__(self, scene: PreparedScene, device: int = 0, budget: int = 2048, primary_budget: int = 4096,
                  capacity: int = 0, blocks_per_sm: int = 0, kernel_timing: bool = False,
                  tail_records: int = 0, eps_stats: bool = False, yield_pct: int = 0, fuse_primary: bool = False,
-                 eps_fp64: bool = False, graph_rounds: bool = True):
+                 eps_fp64: bool = False, graph_rounds: bool = True, trace_ctas: int = 0):
         self.scene = scene
         cfg = N.GpuConfig()
         N.lib().bt_gpu_config_default(C.byref(cfg))
@@ -232,6 +232,7 @@ class GpuRenderer:
         cfg.fuse_primary = int(fuse_primary)
         cfg.eps_fp64 = int(eps_fp64)
         cfg.graph_rounds = int(graph_rounds)
+        cfg.trace_ctas = int(trace_ctas)
         self.config = cfg
         sd, kd = scene.descs()
         h = C.c_void_p()
