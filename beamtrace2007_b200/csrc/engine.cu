@@ -1429,7 +1429,7 @@ struct bt_gpu_ctx {
     cudaGraphExec_t exec = nullptr;
     RoundParams p;
     int app = -1, mode = -1, grids[4] = {0, 0, 0, 0};
-    bool admit = true, events = false;
+    bool admit = true;
   } graphs[2];
   // serving (serve.cpp): a lane views its parent's scene pool and owns only
   // its engine buffers; the parent's scene lock is held shared while a lane
@@ -1735,11 +1735,11 @@ struct RoundRunner {
     RoundParams key = p;
     key.cur = 0;
     const int grids[4] = {gA, gT, gC, gF};
-    if (!g.exec || g.app != App || g.mode != mode || g.admit != admit || g.events != ktime ||
-        memcmp(grids, g.grids, sizeof grids) != 0 || memcmp(&key, &g.p, sizeof key) != 0) {
+    if (!g.exec || g.app != App || g.mode != mode || g.admit != admit || memcmp(grids, g.grids, sizeof grids) != 0 ||
+        memcmp(&key, &g.p, sizeof key) != 0) {
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       const int r0 = round, l0 = launches, t0 = tailRounds;
-      launchRounds(tail, admit, ktime);  // kernel_timing: event-record nodes around the trace kernels
+      launchRounds(tail, admit, false);
       round = r0;
       launches = l0;
       tailRounds = t0;
@@ -1773,7 +1773,6 @@ struct RoundRunner {
       g.app = App;
       g.mode = mode;
       g.admit = admit;
-      g.events = ktime;
       memcpy(g.grids, grids, sizeof grids);
     }
     CK(cudaGraphLaunch(g.exec, c->stream));
@@ -1795,19 +1794,19 @@ struct RoundRunner {
     for (int k = 0; k < nr; ++k, ++round) {
       p.cur = round & 1;
       if (tail) {
-        if (events) cudaEventRecordWithFlags(c->kev[2 * k], c->stream, cudaEventRecordExternal);
+        if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
           traceKernel<App, true, kVoteFp64F<App>><<<gF, kThreads, 0, c->stream>>>(p);
         else if (mode == kVoteLog)
           traceKernel<App, true, kVoteLog><<<gF, kThreads, 0, c->stream>>>(p);
         else
           traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
-        if (events) cudaEventRecordWithFlags(c->kev[2 * k + 1], c->stream, cudaEventRecordExternal);
+        if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         launches += 2;
         tailRounds++;
       } else {
         if (admit) admitKernel<App><<<gA, kThreads, 0, c->stream>>>(p);
-        if (events) cudaEventRecordWithFlags(c->kev[2 * k], c->stream, cudaEventRecordExternal);
+        if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
           traceKernel<App, false, kVoteFp64F<App>><<<gT, kThreads, 0, c->stream>>>(p);
         else if (mode == kVoteLog)
@@ -1816,7 +1815,7 @@ struct RoundRunner {
           traceKernel<App, false, kVoteFloat, 4><<<gT, kThreads, 0, c->stream>>>(p);
         else
           traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
-        if (events) cudaEventRecordWithFlags(c->kev[2 * k + 1], c->stream, cudaEventRecordExternal);
+        if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         if (mode == kVoteFp64)
           clipKernel<App, App == kAppSoft><<<gC, kThreads, 0, c->stream>>>(p);
         else
@@ -1836,11 +1835,11 @@ struct RoundRunner {
     const int64_t queued = hc.count[round & 1];
     const bool tail = round > 0 && hc.rootNext >= n && queued < tailRecords && c->cfg.tail_records >= 0 &&
                       (round > kFirstRounds || 2 * queued <= n);
-    const bool admit = hc.rootNext < n;
-    int nr = kRoundsPerCheck;
     // (the legacy default stream, which the allocation-free entry point
     // runs on, cannot be captured)
-    if (c->cfg.graph_rounds && c->stream != nullptr && round > 0) {
+    const bool admit = hc.rootNext < n;
+    int nr = kRoundsPerCheck;
+    if (c->cfg.graph_rounds && !ktime && c->stream != nullptr && round > 0) {
       const int e = graphBatch(tail, admit);
       if (e) return e;
     } else {

@@ -139,8 +139,7 @@ typedef struct {
   int32_t graph_rounds;     /* nonzero (default): each batch of rounds (the admit / trace / clip /
                                bookkeeping launches between two looks at the counters) is replayed as one
                                CUDA graph, captured again only when the launch parameters change (the
-                               executable graph updated in place; kernel_timing's events are nodes of
-                               the graph); same results */
+                               executable graph updated in place); same results.  Off with kernel_timing */
   int32_t trace_ctas;       /* CTAs per SM of the full-round trace kernel: 3 (up to 170 registers a
                                thread) or 4 (128, a few spills, more warps to hide latency); 0 = 4 for
                                scenes up to 16 MB on the device, else 3; same results */
