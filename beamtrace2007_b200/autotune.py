@@ -4,7 +4,9 @@ settings for a workload by timing a probe of it on the GPU.
 Two kinds of setting:
 
 * per context (`bt_gpu_config`): CTAs per SM of the persistent grids
-  (`blocks_per_sm`, i.e. warps per SM; 0 = as many as fit), the queue
+  (`blocks_per_sm`, i.e. warps per SM; 0 = as many as fit), the register
+  budget of the full-round trace kernel (`trace_ctas`: 3 or 4 CTAs per
+  SM, 0 = by scene size), the queue
   length below which rounds become fused tail rounds (`tail_records`), the
   share of exited trace warps at which the records still in flight are
   handed on to the next round (`yield_pct`), and the sub-beam queue
@@ -33,30 +35,37 @@ def _best(timings: dict):
 
 
 def tune_engine(scene, cam, light, exact: bool = True, blocks_per_sm=(0, 2), tail_records=(0, 30000, -1),
-                capacities=(0,), yield_pcts=(0,), budgets=None, reps: int = 2, device: int = 0):
+                capacities=(0,), yield_pcts=(0,), budgets=None, trace_ctas=None, reps: int = 2, device: int = 0):
     """Times `reps` soft-shadow frames (after one warm-up) for every
     combination of the candidate settings; returns (best settings as
     GpuRenderer keyword arguments, {settings tuple: best ms}).  `budgets`:
     candidate live sub-beam budgets per root (a root over it is retried with
-    16x; dense meshes under large lights prefer larger ones); None keeps the
+    16x; dense meshes under large lights prefer larger ones); `trace_ctas`:
+    candidate CTAs per SM of the full-round trace kernel.  Each given one
+    adds a field to the settings tuple (budget first); None keeps the
     default and the 4-tuple keys."""
     from .renderer import GpuRenderer
     timings = {}
-    for bps, tail, cap, yp, bud in itertools.product(blocks_per_sm, tail_records, capacities, yield_pcts,
-                                                     budgets or (None,)):
+    for bps, tail, cap, yp, bud, tc in itertools.product(blocks_per_sm, tail_records, capacities, yield_pcts,
+                                                         budgets or (None,), trace_ctas or (None,)):
         kw = {} if bud is None else {"budget": bud}
+        if tc is not None:
+            kw["trace_ctas"] = tc
         with GpuRenderer(scene, device=device, blocks_per_sm=bps, tail_records=tail, capacity=cap,
                          yield_pct=yp, **kw) as g:
             g.soft_shadows(cam, light, exact=exact)
             ms = []
             for _ in range(reps):
                 ms.append(g.soft_shadows(cam, light, exact=exact).info["ms_total"])
-        key = (bps, tail, cap, yp) if budgets is None else (bps, tail, cap, yp, bud)
+        key = (bps, tail, cap, yp) + (() if budgets is None else (bud,)) + (() if trace_ctas is None else (tc,))
         timings[key] = min(ms)
     best = _best(timings)
     out = {"blocks_per_sm": best[0], "tail_records": best[1], "capacity": best[2], "yield_pct": best[3]}
+    rest = list(best[4:])
     if budgets is not None:
-        out["budget"] = best[4]
+        out["budget"] = rest.pop(0)
+    if trace_ctas is not None:
+        out["trace_ctas"] = rest.pop(0)
     return out, timings
 
 

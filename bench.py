@@ -454,8 +454,8 @@ def batched_jobs_measure(n_jobs: int = 64, sizes=(64, 128, 256, 512), max_tris: 
         sd, ps, _, _ = jobs[h]
         v = sd.views[0]
         probe = make_camera(v.eye, v.target, v.fov, sd.up, 64, 64)
-        settings, timings = tune_engine(ps, probe, lights[h], budgets=(128, 512, 2048), blocks_per_sm=(0,),
-                                        tail_records=(0,), reps=1)
+        settings, timings = tune_engine(ps, probe, lights[h], budgets=(128, 512, 2048), trace_ctas=(3, 4),
+                                        blocks_per_sm=(0,), tail_records=(0,), reps=1)
         tuned = {"settings": settings, "probe": f"job {h} ({ps.num_tris} tris) at 64x64",
                  "ms": {str(k): round(t, 2) for k, t in timings.items()}}
     g = GpuRenderer(jobs[0][1], **settings)

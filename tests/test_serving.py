@@ -211,3 +211,23 @@ def test_soft_lane_cta_cap_same_results(gpu):
         for r in reqs:
             assert r.event.wait(120) and r.error is None, r.error
             assert _same(r, _alone(srv, r))
+
+
+@pytest.mark.gpu
+def test_autotune_trace_ctas(gpu):
+    """tune_engine with trace_ctas candidates times each and reports the
+    fastest; the frame is the same for 3 and 4 trace CTAs per SM."""
+    from beamtrace2007_b200.autotune import tune_engine
+    from beamtrace2007_b200.renderer import GpuRenderer, make_camera
+    s, ps = scene("plant")
+    v = s.views[0]
+    cam = make_camera(v.eye, v.target, v.fov, s.up, 96, 96)
+    best, timings = tune_engine(ps, cam, s.light_array(), blocks_per_sm=(0,), tail_records=(0,), trace_ctas=(3, 4),
+                                reps=1)
+    assert set(timings) == {(0, 0, 0, 0, 3), (0, 0, 0, 0, 4)}
+    assert best["trace_ctas"] == min(timings, key=timings.get)[4]
+    frames = []
+    for tc in (3, 4):
+        with GpuRenderer(ps, trace_ctas=tc) as g:
+            frames.append(g.soft_shadows(cam, s.light_array(), exact=True))
+    assert np.array_equal(frames[0].vis, frames[1].vis) and np.array_equal(frames[0].E, frames[1].E)
