@@ -726,6 +726,10 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
   }
 }
 
+// Each clipping thread's piece log (clipRecord), in shared memory rather
+// than the thread's local frame: 44.5 KB a CTA, 4 clip CTAs per SM.
+__shared__ PieceLog s_pieceLog[kThreads];
+
 // Clips one record of the clip queue (a triangle at its cursor needs it):
 // the pieces go to the next round's trace queue in consecutive slots (or,
 // in tail rounds, the first one back to the calling lane, `keep`).
@@ -752,7 +756,7 @@ __device__ __noinline__ bool clipRecord(const RoundParams& p, SubBeam* recp, Sta
   Line L[5];
   int nl = 0;
   bool commit = false;
-  PieceLog log;
+  PieceLog& log = s_pieceLog[threadIdx.x];  // shared memory: not in the thread's local frame
   Line64 e64[3];
   const int slots = splitPass1<SplitEnv<App>, F64>(p.s, q, rec, b, st, ti, L, nl, commit, &log, e64);
   if (slots < 0) {
