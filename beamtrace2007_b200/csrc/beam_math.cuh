@@ -751,7 +751,7 @@ BT_HD bool testLine(const Query& q, const Beam& B, const Line& line, Line* L, in
 // last test (the beam's side planes, case (b)) is left out: a clip, whose
 // triangle the trace step already classified, needs only the lines L.
 template <bool F64 = false>
-BT_COLD int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl,
+BT_CLIP int classifyTri(const Query& q, const Beam& B, const TriInfo& ti, Line* L, int& nl,
                         const Line64* e64 = nullptr, bool separation = true) {
   nl = 0;
   bool allIn = true;

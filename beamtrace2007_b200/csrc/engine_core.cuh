@@ -320,7 +320,7 @@ BT_HD V3 edgePlane(const V3* r, const uint32_t* T, int i, int j) {
   return T[i] < T[j] ? cross(r[i], r[j]) : neg(cross(r[j], r[i]));
 }
 
-BT_COLD void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
+BT_CLIP void setupRef(const SceneDev& s, const Query& q, uint32_t k, TriInfo& ti) {
   TriRec t = loadRef(s, k);
   triSetup(q, t.v0, t.v1, t.v2, t.n, t.vi, t.tri, ti);
 }
