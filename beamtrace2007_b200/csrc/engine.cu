@@ -726,9 +726,14 @@ __device__ __forceinline__ void flushStats(const RoundParams& p, const Stats& st
   }
 }
 
-// Each clipping thread's piece log (clipRecord), in shared memory rather
-// than the thread's local frame: 44.5 KB a CTA, 4 clip CTAs per SM.
-__shared__ PieceLog s_pieceLog[kThreads];
+// Each clipping thread's piece log (clipRecord), in dynamic shared memory
+// rather than the thread's local frame: kThreads logs of 10 pieces, 55.8 KB
+// a CTA, which still lets 4 clip CTAs share an SM (a log of 8 pieces was
+// 0.5 ms a plant frame slower, one of 6 1.5 ms: the clips it cannot hold
+// are clipped again).  The clip and fused trace kernels are launched with
+// kLogSmem bytes.
+extern __shared__ PieceLog s_pieceLog[];
+constexpr size_t kLogSmem = sizeof(PieceLog) * kThreads;
 
 // Clips one record of the clip queue (a triangle at its cursor needs it):
 // the pieces go to the next round's trace queue in consecutive slots (or,
@@ -1557,9 +1562,10 @@ int ensurePix(bt_gpu_ctx* c, int64_t n) {
 }
 
 template <class K>
-int gridFor(bt_gpu_ctx* c, K kernel) {
+int gridFor(bt_gpu_ctx* c, K kernel, size_t smem = 0) {
   int perSM = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, 0);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, smem);
   if (c->cfg.blocks_per_sm > 0) perSM = std::min(perSM, c->cfg.blocks_per_sm);
   return c->sms * std::max(1, perSM);
 }
@@ -1669,10 +1675,11 @@ struct RoundRunner {
          : mode == kVoteLog ? gridFor(c, traceKernel<App, false, kVoteLog>)
          : wide             ? gridFor(c, traceKernel<App, false, kVoteFloat, 4>)
                             : gridFor(c, traceKernel<App, false>);
-    gC = mode == kVoteFp64 ? gridFor(c, clipKernel<App, App == kAppSoft>) : gridFor(c, clipKernel<App>);
-    gF = mode == kVoteFp64 ? gridFor(c, traceKernel<App, true, kVoteFp64F<App>>)
-         : mode == kVoteLog ? gridFor(c, traceKernel<App, true, kVoteLog>)
-                            : gridFor(c, traceKernel<App, true>);
+    gC = mode == kVoteFp64 ? gridFor(c, clipKernel<App, App == kAppSoft>, kLogSmem)
+                           : gridFor(c, clipKernel<App>, kLogSmem);
+    gF = mode == kVoteFp64 ? gridFor(c, traceKernel<App, true, kVoteFp64F<App>>, kLogSmem)
+         : mode == kVoteLog ? gridFor(c, traceKernel<App, true, kVoteLog>, kLogSmem)
+                            : gridFor(c, traceKernel<App, true>, kLogSmem);
     // tail rounds: every root admitted and fewer queued records than this
     // (default: a sixth of the trace grid's lanes, about two warps' worth per SM -- the fused kernel clips
     // inside the divergent walk, which only pays once the queue no longer fills the GPU)
@@ -1800,11 +1807,11 @@ struct RoundRunner {
       if (tail) {
         if (events) cudaEventRecord(c->kev[2 * k], c->stream);
         if (mode == kVoteFp64)
-          traceKernel<App, true, kVoteFp64F<App>><<<gF, kThreads, 0, c->stream>>>(p);
+          traceKernel<App, true, kVoteFp64F<App>><<<gF, kThreads, kLogSmem, c->stream>>>(p);
         else if (mode == kVoteLog)
-          traceKernel<App, true, kVoteLog><<<gF, kThreads, 0, c->stream>>>(p);
+          traceKernel<App, true, kVoteLog><<<gF, kThreads, kLogSmem, c->stream>>>(p);
         else
-          traceKernel<App, true><<<gF, kThreads, 0, c->stream>>>(p);
+          traceKernel<App, true><<<gF, kThreads, kLogSmem, c->stream>>>(p);
         if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         launches += 2;
         tailRounds++;
@@ -1821,9 +1828,9 @@ struct RoundRunner {
           traceKernel<App, false><<<gT, kThreads, 0, c->stream>>>(p);
         if (events) cudaEventRecord(c->kev[2 * k + 1], c->stream);
         if (mode == kVoteFp64)
-          clipKernel<App, App == kAppSoft><<<gC, kThreads, 0, c->stream>>>(p);
+          clipKernel<App, App == kAppSoft><<<gC, kThreads, kLogSmem, c->stream>>>(p);
         else
-          clipKernel<App><<<gC, kThreads, 0, c->stream>>>(p);
+          clipKernel<App><<<gC, kThreads, kLogSmem, c->stream>>>(p);
         launches += admit ? 4 : 3;
       }
       roundEndKernel<<<1, 1, 0, c->stream>>>(c->dCtr, p.cur, n);

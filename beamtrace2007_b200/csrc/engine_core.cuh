@@ -578,8 +578,9 @@ struct EmitSink {
 
 // The pieces of pass 1 in push order, so that pass 2 can emit them without
 // clipping again (pieces have at most 5 corners; a clip with more than
-// kPieceLog pieces is replayed instead).
-constexpr int kPieceLog = 8;
+// kPieceLog pieces is replayed instead).  The engine keeps one per clipping
+// thread in shared memory, 436 bytes each.
+constexpr int kPieceLog = 10;
 struct PieceLog {
   int count;
   int8_t level[kPieceLog], n[kPieceLog], clean[kPieceLog];
