@@ -1794,9 +1794,10 @@ struct RoundRunner {
     return BT_OK;
   }
 
-  // The launches of kRoundsPerCheck rounds on the engine's stream (full
-  // rounds: admit, trace, clip; tail rounds: the fused kernel; then the
-  // bookkeeping kernel), with the kernel_timing events when `events`.
+  // The launches of one batch of rounds on the engine's stream
+  // (kFirstRounds at the start of a pass, else kRoundsPerCheck; full rounds:
+  // admit, trace, clip; tail rounds: the fused kernel; then the bookkeeping
+  // kernel), with the kernel_timing events when `events`; returns the rounds.
   // `admit`: some roots are not admitted yet (else the admit kernel, which
   // would find none, is not launched).
   int launchRounds(bool tail, bool admit, bool events) {
@@ -1838,7 +1839,7 @@ struct RoundRunner {
     return nr;
   }
 
-  // One batch of kRoundsPerCheck rounds, then the counters.
+  // One batch of rounds, then the counters.
   int batch() {
     const int n = p.numRoots;
     CK(cudaEventRecord(c->rev[0], c->stream));
